@@ -1,0 +1,373 @@
+"""Benchmark of the batched decode + AND-intersection path on B200.
+
+python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload zipf|pairs|skewed]
+
+One step = one batch of the workload's queries through the device pipeline
+(pack -> scan -> persistent probe -> scan -> scatter), with the compressed
+index resident in HBM. Prints ONE JSON line on rank 0.
+
+Workloads (seeded synthetic stand-ins for the reference's Baidu/GOV2 data):
+  zipf    10M docs, 100k terms, df_r = min(5M, 5M/r) (~60.4M postings), SegLRC
+          (256-entry segments, FRAC 0), 10,000 queries of 2-5 terms ~ df^0.5
+  pairs   1,000 pairs of 4,096 / 1,048,576 uniform docIDs over 2^23, ParaPFD
+          blocks of 128, FRAC 0.10
+  skewed  2^26 universe, clustered-run lists, HS-bucketed ParaPFD, 5,000 queries
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--workload", default="zipf", choices=["zipf", "pairs", "skewed"])
+    p.add_argument("--codec", default=None)
+    p.add_argument("--algo", default=None, help="search method for `value` (default: best measured)")
+    p.add_argument("--cpu-sample-s", type=float, default=15.0)
+    p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--scale", type=float, default=1.0, help="workload size factor (1.0 = the named config)")
+    return p.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# workloads
+
+def make_workload(name: str, scale: float):
+    from exclucene_b200 import synth
+
+    if name == "zipf":
+        nt = max(1000, int(100_000 * scale))
+        w = synth.zipf_corpus(ndocs=int(10_000_000 * max(scale, 0.01)), nterms=nt, cap=int(5_000_000 * scale),
+                              nq=max(100, int(10_000 * scale)), qmin=2, qmax=5)
+        return w, dict(codec="seglrc", block=256, frac=0.0), (
+            f"zipf corpus: {int(10_000_000 * max(scale, 0.01))} docs, {nt} terms, df_r=min(cap,cap/r), "
+            f"{w.nq} queries of 2-5 terms ~ df^0.5; SegLRC 256-entry segments, FRAC 0")
+    if name == "pairs":
+        npairs = max(10, int(1000 * scale))
+        w = synth.pairs(npairs=npairs)
+        return w, dict(codec="parapfd", block=128, frac=0.10), (
+            f"{npairs} pairs of 4096/1048576 uniform docIDs over 2^23; ParaPFD blocks of 128, FRAC 0.10")
+    if name == "skewed":
+        nq = max(100, int(5000 * scale))
+        w = synth.skewed(nq=nq, npool=32)
+        return w, dict(codec="hs_parapfd", block=128, frac=0.10, hs_kbits=16, hs_ubits=26), (
+            f"2^26 universe, 32 clustered long lists 1e6-2e7, {nq} short lists 1e3-1e4, 1-3 long per query; "
+            "HS top-16-bit buckets, ParaPFD blocks of 128, FRAC 0.10")
+    raise ValueError(name)
+
+
+def query_postings(w) -> int:
+    lens = np.diff(w.list_offsets).astype(np.int64)
+    return int(lens[w.terms.astype(np.int64)].sum())
+
+
+def algorithmic_bytes(w, arrays) -> int:
+    """Bytes one step must move at minimum (per query: the shortest list's
+    compressed bytes + for each longer list min(whole list, blocks hit by the
+    surviving probes + their metadata) + 4 bytes per result)."""
+    lists = arrays.lists
+    nseg_all = len(arrays.seg_head)
+    seg_rec = arrays.seg_rec
+    # words per segment
+    seg_words = np.zeros(nseg_all, dtype=np.int64)
+    for l in range(len(lists)):
+        s0, ns = int(lists[l]["seg_base"]), int(lists[l]["nseg"])
+        offs = seg_rec[s0:s0 + ns, 1].astype(np.int64)
+        end = offs[1:].tolist() + [None]
+        nxt = int(lists[l + 1]["word_base"]) - int(lists[l]["word_base"]) if l + 1 < len(lists) else None
+        if nxt is None:
+            nxt = int(offs[-1]) + 64
+        seg_words[s0:s0 + ns] = np.diff(np.append(offs, nxt))
+    codec_meta = {0: 12, 1: 8, 2: 12, 3: 28, 4: 28, 5: 12}
+    total = 0
+    lens = np.diff(w.list_offsets).astype(np.int64)
+    for q in range(w.nq):
+        ts = w.terms[w.term_offsets[q]:w.term_offsets[q + 1]]
+        if len(ts) == 0:
+            continue
+        order = sorted(ts.tolist(), key=lambda t: lens[t])
+        meta = codec_meta[int(lists[order[0]]["codec"])]
+        s0, ns = int(lists[order[0]]["seg_base"]), int(lists[order[0]]["nseg"])
+        total += 4 * int(seg_words[s0:s0 + ns].sum()) + meta * ns
+        keys = w.list(order[0])
+        for t in order[1:]:
+            if len(keys) == 0:
+                break
+            li = lists[t]
+            s0, ns = int(li["seg_base"]), int(li["nseg"])
+            meta = codec_meta[int(li["codec"])]
+            heads = arrays.seg_head[s0:s0 + ns]
+            segs = np.unique(np.clip(np.searchsorted(heads, keys, side="right") - 1, 0, ns - 1))
+            hit = 4 * int(seg_words[s0 + segs].sum()) + meta * len(segs)
+            whole = 4 * int(seg_words[s0:s0 + ns].sum()) + meta * ns
+            total += min(hit, whole)
+            keys = np.intersect1d(keys, w.list(t), assume_unique=True)
+        total += 4 * len(keys)
+    return total
+
+
+# ---------------------------------------------------------------------------
+# clocks
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = threading.Thread(target=self._run, daemon=True)
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if len(s) > 5 + i and
+                          s[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def peak_hbm():
+    try:
+        with open(MEASURED_PEAKS) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# CPU legs (oracle restatement of the reference path, all host threads)
+
+def cpu_run(w, seconds: float, threads: int):
+    import oracle
+
+    nq = w.nq
+    # grow the sample until it takes about `seconds`
+    n = max(1, min(nq, 64))
+    while True:
+        t, _ = oracle.run_queries(w.docs, w.list_offsets, w.terms[:int(w.term_offsets[n])],
+                                  w.term_offsets[:n + 1], threads)
+        if t >= seconds or n >= nq:
+            break
+        n = min(nq, max(n * 2, int(n * seconds / max(t, 1e-3) * 0.9)))
+    sub_terms = w.terms[:int(w.term_offsets[n])]
+    lens = np.diff(w.list_offsets).astype(np.int64)
+    postings = int(lens[sub_terms.astype(np.int64)].sum())
+    return t, n, postings
+
+
+def reference_arm(args, w, desc):
+    threads = os.cpu_count() or 1
+    vals = []
+    n = p = 0
+    for i in range(args.warmup + args.steps):
+        t, n, p = cpu_run(w, max(1.0, args.cpu_sample_s / max(args.steps, 1)), threads)
+        if i >= args.warmup:
+            vals.append(p / t)
+    v = float(np.median(vals))
+    sample = (f"first {n} of {w.nq} queries per step; exact galloping AND over the uncompressed lists "
+              f"(oracle port of the reference CPU path), {threads} threads")
+    line = {"metric": "postings/s", "value": v, "unit": "postings/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": desc},
+            "cpu_baseline": {"value": v, "unit": "postings/s", "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": "postings/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    w, params, desc = make_workload(args.workload, args.scale)
+    if args.codec:
+        params["codec"] = args.codec
+
+    if args.impl == "reference":
+        if rank == 0:
+            reference_arm(args, w, desc)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    import exclucene_b200 as ex
+
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    ix = ex.Index(w.docs, w.list_offsets, **params)
+    lens = np.diff(w.list_offsets).astype(np.int64)
+    shortest = sum(int(min(lens[w.terms[w.term_offsets[q]:w.term_offsets[q + 1]]], default=0)) for q in range(w.nq))
+    ctx = ex.Context(local, max_queries=max(w.nq, 1024), max_keys=max(1 << 20, 2 * shortest))
+    ctx.upload(ix)
+    sizes = ix.sizes()
+    arrays = ix.export()
+    stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+
+    d_terms = torch.from_numpy(w.terms.astype(np.int32)).to(dev)
+    d_toff = torch.from_numpy(w.term_offsets.astype(np.int32)).to(dev)
+    cap = max(1, shortest)
+    d_offs = torch.zeros(w.nq + 1, dtype=torch.int32, device=dev)
+    d_docs = torch.zeros(cap, dtype=torch.int32, device=dev)
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.int32, device=dev)  # > L2 (126 MB)
+    torch.cuda.synchronize()
+
+    def step(algo):
+        ctx.intersect_device(ix, d_terms.data_ptr(), d_toff.data_ptr(), w.nq, algo, d_offs.data_ptr(),
+                             d_docs.data_ptr(), cap)
+
+    def measure(algo, k, warm):
+        for _ in range(warm):
+            step(algo)
+        ctx.check()
+        tot, probe = [], []
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        for _ in range(k):
+            flush.zero_()
+            torch.cuda.synchronize()
+            step(algo)
+            st = ctx.stats()
+            tot.append(st.total_ms)
+            probe.append(st.probe_ms)
+        torch.cuda.synchronize()
+        ctx.check()
+        if world > 1:
+            dist.barrier()
+        return float(np.mean(tot)), float(np.mean(probe)), st
+
+    postings = query_postings(w)
+    algos = [args.algo] if args.algo else ["bsearch", "hashseg", "auto"]
+    per_algo = {}
+    with ClockSampler(local) as clk:
+        for a in algos:
+            ms, pms, st = measure(a, args.steps, args.warmup)
+            per_algo[a] = (ms, pms, st)
+    clocks = clk.summary()
+    best = min(per_algo, key=lambda a: per_algo[a][0]) if not args.algo else args.algo
+    ms, pms, st = per_algo[best]
+    if world > 1:
+        t = torch.tensor([ms, pms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, pms = float(t[0]), float(t[1])
+    value = world * postings / (ms / 1e3)
+
+    # checksum of the last device result (traceability)
+    offs_h = d_offs.cpu().numpy().astype(np.uint32)
+    docs_h = d_docs[: int(offs_h[-1])].cpu().numpy().astype(np.uint32)
+    cs = ex.checksum(offs_h, docs_h)
+
+    # end to end through the public host API: H2D of the queries, D2H of the results
+    h_off = np.zeros(w.nq + 1, dtype=np.uint32)
+    h_docs = np.zeros(cap, dtype=np.uint32)
+    for _ in range(args.warmup):
+        b = ctx.submit(ix, w.terms, w.term_offsets, best)
+        b.wait_into(h_off, h_docs)
+        b.free()
+    e2e_t = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        b = ctx.submit(ix, w.terms, w.term_offsets, best)
+        tot = b.wait_into(h_off, h_docs)
+        e2e_t.append(time.perf_counter() - t0)
+        b.free()
+    e2e_s = float(np.mean(e2e_t))
+    if world > 1:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t[0])
+    h2d = w.terms.nbytes + w.term_offsets.nbytes
+    d2h = h_off.nbytes + 4 * tot
+
+    peak, peak_kind = peak_hbm()
+    algo_bytes = algorithmic_bytes(w, arrays)
+    achieved = algo_bytes / (pms / 1e3) / 1e9
+    line = {
+        "metric": "postings/s", "value": value, "unit": "postings/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": desc, "codec": params["codec"], "algo": best, "queries_per_step": w.nq,
+                   "postings_per_step": postings, "index_device_bytes": int(sizes.device_bytes),
+                   "index_postings": int(sizes.postings), "l2": "flushed (512 MB write) between timed steps"},
+        "queries_per_s": world * w.nq / (ms / 1e3),
+        "per_algo_ms": {a: round(per_algo[a][0], 4) for a in per_algo},
+        "per_algo_postings_per_s": {a: world * postings / (per_algo[a][0] / 1e3) for a in per_algo},
+        "stats": {"tiles": int(st.tiles), "keys": int(st.keys), "probes": int(st.probes),
+                  "fallbacks": int(st.fallbacks), "probe_ms": pms, "pack_ms": st.pack_ms,
+                  "compact_ms": st.compact_ms},
+        "checksum": list(cs),
+        "roofline": {"bound": "hbm", "kernel": "k_probe", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None, "algorithmic_bytes": algo_bytes,
+                     "peak_kind": peak_kind},
+        "e2e": {"value": world * postings / e2e_s, "unit": "postings/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_s * 1e3},
+        "gpu_launches": 5 * (args.steps),
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        t, n, p = cpu_run(w, args.cpu_sample_s, threads)
+        line["cpu_baseline"] = {"value": p / t, "unit": "postings/s", "cores": threads, "kind": "port",
+                                "sample": f"first {n} of {w.nq} queries; exact galloping AND over uncompressed "
+                                          f"lists (oracle), {t:.1f} s"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

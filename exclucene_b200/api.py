@@ -1,0 +1,350 @@
+"""ctypes binding of libexcl_gpu.so (C ABI in include/excl_gpu.h).
+
+Mirrors the reference's entry points for this path: the ParaPFD codec calls
+(encodeArray/decodeArray, Compressed/include/ParaPFor.h:15-16), the index
+build of the X_Compression/X_Generator tools, and the batched conjunctive
+query pipeline (CPUPreprocess -> kernels -> results, ParaPFD_Intersection.cu).
+There is no CPU fallback: every call goes to the compiled library, and a
+missing library raises at import time.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "libexcl_gpu.so")
+
+if not os.path.exists(_LIB_PATH):
+    raise ImportError(f"{_LIB_PATH} is not built; run `python -m exclucene_b200.build`")
+_lib = C.CDLL(_LIB_PATH)
+
+u32p = C.POINTER(C.c_uint32)
+u64p = C.POINTER(C.c_uint64)
+
+OK, E_INVALID, E_CUDA, E_CAPACITY, E_FORMAT, E_TIMEOUT, E_DEVICE_FLAG, E_NOMEM = range(8)
+STATUS_NAMES = ["OK", "INVALID", "CUDA", "CAPACITY", "FORMAT", "TIMEOUT", "DEVICE_FLAG", "NOMEM"]
+
+CODEC_PARAPFD, CODEC_LRC, CODEC_LRCSEG, CODEC_SEGLRC, CODEC_HS_SEGLRC, CODEC_HS_PARAPFD = range(6)
+CODEC_NAMES = {"parapfd": 0, "lrc": 1, "lrcseg": 2, "seglrc": 3, "hs_seglrc": 4, "hs_parapfd": 5}
+ALGO_AUTO, ALGO_BSEARCH, ALGO_HASHSEG, ALGO_LEARNED = range(4)
+ALGO_NAMES = {"auto": 0, "bsearch": 1, "hashseg": 2, "learned": 3}
+
+
+class ExclError(RuntimeError):
+    def __init__(self, status: int, msg: str = ""):
+        self.status = status
+        name = STATUS_NAMES[status] if 0 <= status < len(STATUS_NAMES) else str(status)
+        super().__init__(f"EXCL_E_{name}: {msg}")
+
+
+class BuildParams(C.Structure):
+    _fields_ = [("codec", C.c_uint32), ("codecs", C.POINTER(C.c_uint8)), ("block", C.c_uint32),
+                ("frac", C.c_float), ("hs_bucket", C.c_uint32), ("hs_kbits", C.c_uint32),
+                ("hs_ubits", C.c_uint32), ("threads", C.c_uint32)]
+
+
+class ListInfo(C.Structure):
+    _fields_ = [("word_base", C.c_uint64), ("n", C.c_uint32), ("seg_base", C.c_uint32), ("nseg", C.c_uint32),
+                ("codec", C.c_uint32), ("log2_block", C.c_uint32), ("first_doc", C.c_uint32),
+                ("last_doc", C.c_uint32), ("reg", C.c_uint32 * 4), ("dir_shift", C.c_uint32),
+                ("dir_base", C.c_uint32), ("ndir", C.c_uint32), ("tile_base", C.c_uint32),
+                ("ntiles", C.c_uint32), ("model", C.c_uint32)]
+
+
+class IndexSizes(C.Structure):
+    _fields_ = [("nlists", C.c_uint32), ("nsegs", C.c_uint64), ("nwords", C.c_uint64), ("ndir", C.c_uint64),
+                ("ntilemap", C.c_uint64), ("postings", C.c_uint64), ("device_bytes", C.c_uint64)]
+
+
+class CtxConfig(C.Structure):
+    _fields_ = [("max_queries", C.c_uint32), ("max_terms", C.c_uint32), ("max_keys", C.c_uint64),
+                ("warps_per_cta", C.c_uint32), ("ctas_per_sm", C.c_uint32)]
+
+
+class BatchStats(C.Structure):
+    _fields_ = [("pack_ms", C.c_float), ("probe_ms", C.c_float), ("compact_ms", C.c_float),
+                ("total_ms", C.c_float), ("tiles", C.c_uint64), ("keys", C.c_uint64), ("probes", C.c_uint64),
+                ("fallbacks", C.c_uint64)]
+
+
+def _sig(name, res, *args):
+    f = getattr(_lib, name)
+    f.restype = res
+    f.argtypes = list(args)
+    return f
+
+
+_encode = _sig("excl_parapfd_encode", C.c_int, u32p, C.c_uint32, C.c_float, u32p, C.c_size_t, C.POINTER(C.c_size_t))
+_decode = _sig("excl_parapfd_decode", C.c_int, u32p, C.c_size_t, C.c_uint32, u32p, C.POINTER(C.c_size_t))
+_set_frac = _sig("excl_set_frac", None, C.c_float)
+_encodeArray = _sig("encodeArray", C.c_uint32, u32p, u32p, C.c_uint32)
+_decodeArray = _sig("decodeArray", C.c_uint32, u32p, u32p, C.c_uint32)
+_build = _sig("excl_index_build", C.c_int, u32p, u64p, C.c_uint32, C.POINTER(BuildParams), C.POINTER(C.c_void_p))
+_ifree = _sig("excl_index_free", C.c_int, C.c_void_p)
+_isizes = _sig("excl_index_sizes_get", C.c_int, C.c_void_p, C.POINTER(IndexSizes))
+_iexport = _sig("excl_index_export", C.c_int, C.c_void_p, C.POINTER(ListInfo), u32p, u32p, u32p, u32p, u32p)
+_ctx_create = _sig("excl_ctx_create", C.c_int, C.c_int, C.POINTER(CtxConfig), C.POINTER(C.c_void_p))
+_ctx_destroy = _sig("excl_ctx_destroy", C.c_int, C.c_void_p)
+_last_error = _sig("excl_last_error", C.c_char_p, C.c_void_p)
+_ctx_stream = _sig("excl_ctx_stream", C.c_void_p, C.c_void_p)
+_upload = _sig("excl_index_upload", C.c_int, C.c_void_p, C.c_void_p)
+_dec_dev = _sig("excl_decode_lists_device", C.c_int, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p)
+_dec_host = _sig("excl_decode_lists", C.c_int, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, u32p, C.c_size_t)
+_submit = _sig("excl_submit", C.c_int, C.c_void_p, C.c_void_p, u32p, u32p, C.c_uint32, C.c_uint32,
+               C.POINTER(C.c_void_p))
+_wait = _sig("excl_wait", C.c_int, C.c_void_p, u32p, u32p, C.c_size_t, C.c_int, u64p)
+_bfree = _sig("excl_batch_free", C.c_int, C.c_void_p)
+_isect_dev = _sig("excl_intersect_device", C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
+                  C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint64)
+_check = _sig("excl_ctx_check", C.c_int, C.c_void_p)
+_stats = _sig("excl_last_stats", C.c_int, C.c_void_p, C.POINTER(BatchStats))
+_checksum = _sig("excl_checksum", C.c_int, C.c_uint32, u32p, u32p, C.POINTER(C.c_uint64 * 3))
+
+EXPORTED = ["excl_parapfd_encode", "excl_parapfd_decode", "excl_set_frac", "encodeArray", "decodeArray",
+            "excl_index_build", "excl_index_free", "excl_index_sizes_get", "excl_index_export", "excl_ctx_create",
+            "excl_ctx_destroy", "excl_last_error", "excl_ctx_stream", "excl_index_upload",
+            "excl_decode_lists_device", "excl_decode_lists", "excl_submit", "excl_wait", "excl_batch_free",
+            "excl_intersect_device", "excl_ctx_check", "excl_last_stats", "excl_checksum"]
+
+
+def _p32(a: np.ndarray):
+    return a.ctypes.data_as(u32p)
+
+
+def _u32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.uint32)
+
+
+def _check_status(st: int, ctx=None, what: str = "") -> None:
+    if st != OK:
+        msg = what
+        if ctx is not None and ctx._h:
+            msg += ": " + _last_error(ctx._h).decode(errors="replace")
+        raise ExclError(st, msg)
+
+
+# ---------------------------------------------------------------------------
+# Codec calls
+
+def parapfd_encode(values, frac: float = 0.0) -> np.ndarray:
+    v = _u32(values)
+    cap = 3 * len(v) + 8
+    out = np.zeros(cap, dtype=np.uint32)
+    w = C.c_size_t(0)
+    _check_status(_encode(_p32(v), len(v), frac, _p32(out), cap, C.byref(w)), what="parapfd_encode")
+    return out[: w.value].copy()
+
+
+def parapfd_decode(words, n: int) -> tuple[np.ndarray, int]:
+    w = _u32(words)
+    out = np.zeros(max(n, 1), dtype=np.uint32)
+    used = C.c_size_t(0)
+    _check_status(_decode(_p32(w), len(w), n, _p32(out), C.byref(used)), what="parapfd_decode")
+    return out[:n], used.value
+
+
+def encode_array_compat(values, frac: float = 0.0) -> np.ndarray:
+    """Reference-signature shim: encodeArray(in, out, n) with a process-wide FRAC."""
+    v = _u32(values)
+    out = np.zeros(3 * len(v) + 8, dtype=np.uint32)
+    _set_frac(frac)
+    w = _encodeArray(_p32(v), _p32(out), len(v))
+    return out[:w].copy()
+
+
+# ---------------------------------------------------------------------------
+# Index
+
+@dataclass
+class IndexArrays:
+    lists: np.ndarray      # structured view of excl_list_info
+    words: np.ndarray
+    seg_head: np.ndarray
+    seg_rec: np.ndarray    # (nseg, 4) start, off, aux, count
+    seg_reg: np.ndarray    # (nseg, 4) raw a, b, L, R
+    dir: np.ndarray
+
+
+class Index:
+    """A built index (host image); upload it with Context.upload."""
+
+    def __init__(self, docs, list_offsets, codec="parapfd", block: int = 256, frac: float = 0.0,
+                 hs_bucket: int = 256, hs_kbits: int = 0, hs_ubits: int = 32, codecs=None, threads: int = 0):
+        self._h = None
+        docs = _u32(docs)
+        loff = np.ascontiguousarray(list_offsets, dtype=np.uint64)
+        self.nlists = len(loff) - 1
+        p = BuildParams()
+        p.codec = CODEC_NAMES[codec] if isinstance(codec, str) else int(codec)
+        self._codecs = None
+        if codecs is not None:
+            self._codecs = np.ascontiguousarray(codecs, dtype=np.uint8)
+            p.codecs = self._codecs.ctypes.data_as(C.POINTER(C.c_uint8))
+        p.block = block
+        p.frac = frac
+        p.hs_bucket = hs_bucket
+        p.hs_kbits = hs_kbits
+        p.hs_ubits = hs_ubits
+        p.threads = threads
+        h = C.c_void_p()
+        _check_status(_build(_p32(docs), loff.ctypes.data_as(u64p), self.nlists, C.byref(p), C.byref(h)),
+                      what="excl_index_build")
+        self._h = h
+        self.list_lengths = np.diff(loff).astype(np.uint64)
+
+    @classmethod
+    def from_handle(cls, h: C.c_void_p, nlists: int, lengths) -> "Index":
+        self = cls.__new__(cls)
+        self._h = h
+        self.nlists = nlists
+        self._codecs = None
+        self.list_lengths = np.asarray(lengths, dtype=np.uint64)
+        return self
+
+    def sizes(self) -> IndexSizes:
+        s = IndexSizes()
+        _check_status(_isizes(self._h, C.byref(s)))
+        return s
+
+    def export(self) -> IndexArrays:
+        s = self.sizes()
+        lists = (ListInfo * s.nlists)()
+        words = np.zeros(s.nwords, dtype=np.uint32)
+        head = np.zeros(s.nsegs, dtype=np.uint32)
+        rec = np.zeros((s.nsegs, 4), dtype=np.uint32)
+        reg = np.zeros((s.nsegs, 4), dtype=np.uint32)
+        d = np.zeros(max(s.ndir, 1), dtype=np.uint32)
+        _check_status(_iexport(self._h, lists, _p32(words), _p32(head), _p32(rec), _p32(reg), _p32(d)))
+        arr = np.ctypeslib.as_array(lists).copy() if s.nlists else np.zeros(0)
+        return IndexArrays(arr, words, head, rec, reg, d[: s.ndir])
+
+    def close(self) -> None:
+        if self._h:
+            _ifree(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------------------
+# Context
+
+class Context:
+    def __init__(self, device: int = 0, max_queries: int = 65536, max_keys: int = 1 << 26, warps_per_cta: int = 0,
+                 ctas_per_sm: int = 0):
+        self._h = None
+        cfg = CtxConfig(max_queries, 32, max_keys, warps_per_cta, ctas_per_sm)
+        h = C.c_void_p()
+        st = _ctx_create(device, C.byref(cfg), C.byref(h))
+        _check_status(st, what="excl_ctx_create")
+        self._h = h
+        self.device = device
+
+    @property
+    def stream(self) -> int:
+        return _ctx_stream(self._h) or 0
+
+    def last_error(self) -> str:
+        return _last_error(self._h).decode(errors="replace")
+
+    def upload(self, ix: Index) -> None:
+        _check_status(_upload(self._h, ix._h), self, "excl_index_upload")
+
+    def decode_lists(self, ix: Index, l0: int = 0, l1: int | None = None) -> np.ndarray:
+        l1 = ix.nlists if l1 is None else l1
+        n = int(ix.list_lengths[l0:l1].sum())
+        out = np.zeros(max(n, 1), dtype=np.uint32)
+        _check_status(_dec_host(self._h, ix._h, l0, l1, _p32(out), n), self, "excl_decode_lists")
+        return out[:n]
+
+    def decode_lists_device(self, ix: Index, l0: int, l1: int, d_out_ptr: int) -> None:
+        _check_status(_dec_dev(self._h, ix._h, l0, l1, C.c_void_p(d_out_ptr)), self, "excl_decode_lists_device")
+
+    def submit(self, ix: Index, terms, term_offsets, algo="auto"):
+        t = _u32(terms)
+        o = _u32(term_offsets)
+        nq = len(o) - 1
+        a = ALGO_NAMES[algo] if isinstance(algo, str) else int(algo)
+        b = C.c_void_p()
+        if len(t) == 0:
+            t = np.zeros(1, dtype=np.uint32)
+        _check_status(_submit(self._h, ix._h, _p32(t), _p32(o), nq, a, C.byref(b)), self, "excl_submit")
+        return Batch(self, b, nq)
+
+    def intersect(self, ix: Index, terms, term_offsets, algo="auto") -> tuple[np.ndarray, np.ndarray]:
+        """Runs one batch and returns (offsets[nq+1], docids) — each query's docIDs sorted."""
+        b = self.submit(ix, terms, term_offsets, algo)
+        try:
+            return b.wait()
+        finally:
+            b.free()
+
+    def intersect_device(self, ix: Index, d_terms: int, d_toff: int, nq: int, algo, d_offsets: int, d_docids: int,
+                         cap: int) -> None:
+        a = ALGO_NAMES[algo] if isinstance(algo, str) else int(algo)
+        _check_status(_isect_dev(self._h, ix._h, C.c_void_p(d_terms), C.c_void_p(d_toff), nq, a,
+                                 C.c_void_p(d_offsets), C.c_void_p(d_docids), cap), self, "excl_intersect_device")
+
+    def check(self) -> None:
+        _check_status(_check(self._h), self, "excl_ctx_check")
+
+    def stats(self) -> BatchStats:
+        s = BatchStats()
+        _check_status(_stats(self._h, C.byref(s)), self, "excl_last_stats")
+        return s
+
+    def close(self) -> None:
+        if self._h:
+            _ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    def __init__(self, ctx: Context, h: C.c_void_p, nq: int):
+        self.ctx, self._h, self.nq = ctx, h, nq
+
+    def wait(self, timeout_ms: int = -1) -> tuple[np.ndarray, np.ndarray]:
+        offs = np.zeros(self.nq + 1, dtype=np.uint32)
+        tot = C.c_uint64(0)
+        _check_status(_wait(self._h, _p32(offs), None, 0, timeout_ms, C.byref(tot)), self.ctx, "excl_wait")
+        docs = np.zeros(max(int(tot.value), 1), dtype=np.uint32)
+        _check_status(_wait(self._h, _p32(offs), _p32(docs), len(docs), timeout_ms, C.byref(tot)), self.ctx,
+                      "excl_wait")
+        return offs, docs[: int(tot.value)]
+
+    def wait_into(self, offsets: np.ndarray, docids: np.ndarray, timeout_ms: int = -1) -> int:
+        tot = C.c_uint64(0)
+        _check_status(_wait(self._h, _p32(offsets), _p32(docids), len(docids), timeout_ms, C.byref(tot)),
+                      self.ctx, "excl_wait")
+        return int(tot.value)
+
+    def free(self) -> None:
+        if self._h:
+            _bfree(self._h)
+            self._h = None
+
+
+def checksum(offsets, docids) -> tuple[int, int, int]:
+    o = _u32(offsets)
+    d = _u32(docids) if len(docids) else np.zeros(1, dtype=np.uint32)
+    cs = (C.c_uint64 * 3)()
+    _check_status(_checksum(len(o) - 1, _p32(o), _p32(d), C.byref(cs)))
+    return int(cs[0]), int(cs[1]), int(cs[2])
+
+
+def library_path() -> str:
+    return _LIB_PATH

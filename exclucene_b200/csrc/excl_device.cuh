@@ -1,0 +1,336 @@
+// Device helpers shared by the kernels: bit extraction from LSB-first packed
+// ParaPFD sections, block headers, per-codec value reconstruction, the
+// warp-cooperative block decode and the per-lane probe of one longer list.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "excl_internal.h"
+
+namespace excl {
+
+// Learned position model (two-stage): root MLP 1->32->32->1 on the normalized
+// key routes to one of `nleaves` linear leaves; each leaf stores the exact
+// rank error window of its keys, measured with this same inference code.
+constexpr int kHidden = 32;
+constexpr int kRootParams = kHidden + kHidden + kHidden * kHidden + kHidden + kHidden + 1;  // 1153
+constexpr int kRootStride = 1156;
+
+struct ModelHdr {
+    float kmin, kscale;    // x = (key - kmin) * kscale in [0, 1]
+    uint32_t nleaves;      // leaves of this model
+    uint32_t leaf_base;    // first leaf in the leaf array
+    uint32_t n;            // postings of the list
+    uint32_t max_window;   // leaves with a wider window fall back to the directory search
+    uint32_t pad[2];
+};
+
+struct alignas(16) Leaf {
+    float a, b;     // rank ~ a * x + b (x normalized key)
+    int32_t elo;    // rank >= pred + elo for every key of the leaf (elo <= 0)
+    int32_t ehi;    // rank <= pred + ehi
+};
+
+struct ModelView {
+    const float *root = nullptr;      // kRootStride floats per model
+    const ModelHdr *hdr = nullptr;
+    const Leaf *leaves = nullptr;
+};
+
+struct DevIndexView {
+    const ListDesc *lists;
+    const uint32_t *words;
+    const uint32_t *seg_head;
+    const SegRec *seg_rec;
+    const SegReg *seg_reg;
+    const uint32_t *dir;
+    const uint64_t *tilemap;
+    const uint64_t *post_base;
+    ModelView models;
+};
+
+enum : uint32_t {
+    kErrTerms = 1u,      // a query has more than kMaxTerms terms
+    kErrScanSpin = 2u,   // a look-back wait gave up
+    kErrTermId = 4u,     // a term id is out of range
+    kErrCapacity = 8u,   // results or tiles exceed a buffer
+    kErrModel = 16u,     // learned model inconsistency
+};
+
+__device__ __forceinline__ uint32_t ldg(const uint32_t *p) { return __ldg(p); }
+
+// `bits` (0..31) bits starting at bit `bitpos` of the packed array `w`.
+// Reads two words; the index keeps kWordPad zero words after the last block.
+__device__ __forceinline__ uint32_t get_bits(const uint32_t *w, uint32_t bitpos, uint32_t bits) {
+    const uint32_t i = bitpos >> 5;
+    const uint32_t lo = ldg(w + i), hi = ldg(w + i + 1);
+    return __funnelshift_r(lo, hi, bitpos & 31u) & ((1u << bits) - 1u);
+}
+
+struct BlkHdr {
+    uint32_t lb, eb, hb, en;
+};
+
+// ParaPFor.cpp:121-125 descriptor fields.
+__device__ __forceinline__ BlkHdr blk_hdr(uint32_t d) {
+    BlkHdr h;
+    h.lb = (d >> 26) & 31u;
+    h.eb = (d >> 21) & 31u;
+    h.hb = (d >> 16) & 31u;
+    h.en = d & 0xffffu;
+    return h;
+}
+
+__device__ __forceinline__ uint32_t words_for(uint32_t n, uint32_t bits) { return (n * bits + 31u) >> 5; }
+
+// Predicted values of the regression codecs, with the reference's arithmetic:
+// LRC (LRC_Decompression_kernel.cu:254): int((float)i * slope) + icpt;
+// LRCSeg/SegLRC/HS (SegLRC_Decompression_kernel.cu:252): (int)(i * a + b) as
+// one fused multiply-add.
+__device__ __forceinline__ uint32_t pred_lrc(uint32_t i, float slope, int32_t icpt) {
+    return (uint32_t)__float2int_rz(__fmul_rn(__int2float_rn((int)i), slope)) + (uint32_t)icpt;
+}
+__device__ __forceinline__ uint32_t pred_fma(uint32_t i, float a, float b) {
+    return (uint32_t)__float2int_rz(__fmaf_rn(__uint2float_rn(i), a, b));
+}
+
+// Per-segment reconstruction parameters of a residual-coded segment:
+// value(t) = low(t) + pred(idx0 + t) + base.
+struct ResidParams {
+    float a, b;
+    uint32_t idx0;   // index fed to the predictor for t = 0
+    uint32_t base;   // added after the prediction (LRC: the intercept)
+    bool lrc;
+};
+
+__device__ __forceinline__ ResidParams resid_params(const ListDesc &L, const SegRec &rec, const SegReg &reg) {
+    ResidParams p;
+    if (L.codec == EXCL_CODEC_LRC) {
+        p.a = __uint_as_float(L.reg[0]);
+        p.b = 0.0f;
+        p.idx0 = rec.start;
+        p.base = L.reg[1];
+        p.lrc = true;
+    } else if (L.codec == EXCL_CODEC_LRCSEG) {
+        p.a = __uint_as_float(L.reg[0]);
+        p.b = __uint_as_float(L.reg[1]);
+        p.idx0 = rec.start;
+        p.base = rec.aux;
+        p.lrc = false;
+    } else {
+        p.a = reg.a;
+        p.b = reg.b;
+        p.idx0 = 0;
+        p.base = rec.aux;
+        p.lrc = false;
+    }
+    return p;
+}
+
+__device__ __forceinline__ uint32_t resid_value(const ResidParams &p, uint32_t t, uint32_t low) {
+    const uint32_t i = p.idx0 + t;
+    return low + (p.lrc ? pred_lrc(i, p.a, (int32_t)p.base) : pred_fma(i, p.a, p.b) + p.base);
+}
+
+// Low bits of element t of a block plus its exception high bits, by binary
+// search over the sorted exception positions (random access).
+__device__ __forceinline__ uint32_t block_value_ra(const uint32_t *blk, const BlkHdr &h, uint32_t count, uint32_t t) {
+    uint32_t v = get_bits(blk + 1, t * h.lb, h.lb);
+    if (h.en) {
+        const uint32_t *pb = blk + 1 + words_for(count, h.lb);
+        uint32_t lo = 0, hi = h.en;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (get_bits(pb, mid * h.eb, h.eb) < t) lo = mid + 1;
+            else hi = mid;
+        }
+        if (lo < h.en && get_bits(pb, lo * h.eb, h.eb) == t) {
+            const uint32_t *hp = pb + words_for(h.en, h.eb);
+            v |= get_bits(hp, lo * h.hb, h.hb) << h.lb;
+        }
+    }
+    return v;
+}
+
+// Warp-cooperative decode of elements [e0, e0 + kc) (kc <= 256) of one
+// segment into buf[0 .. kc). Lane l owns elements l*vpl .. l*vpl+vpl-1 so its
+// bits are contiguous; exceptions are patched through `buf`; d-gap codecs
+// replace element 0 by the segment head and take a warp inclusive scan
+// (ParaPFD_Decompression_kernel.cu:205-263), residual codecs add the
+// regression prediction and base (SegLRC_Decompression_kernel.cu:249-252).
+__device__ __forceinline__ void warp_decode(const DevIndexView &ix, const ListDesc &L, uint32_t sg, uint32_t e0,
+                                            uint32_t kc, uint32_t *buf, uint32_t lane) {
+    const SegRec rec = ix.seg_rec[sg];
+    const uint32_t *blk = ix.words + L.word_base + rec.off;
+    const BlkHdr h = blk_hdr(ldg(blk));
+    const uint32_t vpl = (kc + 31u) >> 5;
+    const uint32_t el = lane * vpl;
+    uint32_t v[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const uint32_t e = el + j;
+        v[j] = (j < (int)vpl && e < kc) ? get_bits(blk + 1, (e0 + e) * h.lb, h.lb) : 0u;
+    }
+    if (h.en) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+            if (j < (int)vpl && el + j < kc) buf[el + j] = v[j];
+        __syncwarp();
+        const uint32_t *pb = blk + 1 + words_for(rec.count, h.lb);
+        const uint32_t *hp = pb + words_for(h.en, h.eb);
+        for (uint32_t x = lane; x < h.en; x += 32) {
+            const uint32_t p = get_bits(pb, x * h.eb, h.eb);
+            if (p >= e0 && p < e0 + kc) buf[p - e0] |= get_bits(hp, x * h.hb, h.hb) << h.lb;
+        }
+        __syncwarp();
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+            if (j < (int)vpl && el + j < kc) v[j] = buf[el + j];
+        __syncwarp();
+    }
+    if (codec_is_dgap(L.codec)) {
+        if (lane == 0 && e0 == 0) v[0] = ix.seg_head[sg];
+        uint32_t run = 0;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            run += v[j];
+            v[j] = run;
+        }
+        uint32_t incl = run;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= (uint32_t)o) incl += t;
+        }
+        const uint32_t excl = incl - run;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) v[j] += excl;
+    } else {
+        const ResidParams rp = resid_params(L, rec, ix.seg_reg[sg]);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) v[j] = resid_value(rp, e0 + el + j, v[j]);
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+        if (j < (int)vpl && el + j < kc) buf[el + j] = v[j];
+    __syncwarp();
+}
+
+// Last segment in [lo, hi) whose head <= key, or -1.
+__device__ __forceinline__ int last_head_le(const uint32_t *head, uint32_t lo, uint32_t hi, uint32_t key) {
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (ldg(head + mid) <= key) lo = mid + 1;
+        else hi = mid;
+    }
+    return (int)lo - 1;
+}
+
+// Serial search of `key` (head <= key) in a d-gap segment, starting at the
+// segment head or at its median (ParaPFD_Intersection_kernel.cu:383-447:
+// median halves the walk; exceptions tracked with a cursor).
+__device__ __forceinline__ bool dgap_find(const uint32_t *blk, uint32_t count, uint32_t head, uint32_t median,
+                                          uint32_t key) {
+    if (key == head || key == median) return true;
+    const BlkHdr h = blk_hdr(ldg(blk));
+    uint32_t from, end, v;
+    if (key > median) {
+        from = count >> 1;
+        end = count;
+        v = median;
+    } else {
+        from = 0;
+        end = count >> 1;
+        v = head;
+    }
+    const uint32_t *lows = blk + 1;
+    const uint32_t *pb = lows + words_for(count, h.lb);
+    const uint32_t *hp = pb + words_for(h.en, h.eb);
+    uint32_t x = 0, xp = 0xffffffffu;
+    if (h.en) {
+        uint32_t lo = 0, hi = h.en;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (get_bits(pb, mid * h.eb, h.eb) <= from) lo = mid + 1;
+            else hi = mid;
+        }
+        x = lo;
+        xp = x < h.en ? get_bits(pb, x * h.eb, h.eb) : 0xffffffffu;
+    }
+    // stream the low bits with a 64-bit window
+    uint32_t bit = (from + 1) * h.lb;
+    uint32_t wi = bit >> 5;
+    uint64_t win = ((uint64_t)ldg(lows + wi + 1) << 32) | ldg(lows + wi);
+    uint32_t sh = bit & 31u;
+    const uint32_t mask = (1u << h.lb) - 1u;
+    for (uint32_t i = from + 1; i < end; ++i) {
+        uint32_t g = (uint32_t)(win >> sh) & mask;
+        sh += h.lb;
+        if (sh >= 32) {
+            sh -= 32;
+            ++wi;
+            win = (win >> 32) | ((uint64_t)ldg(lows + wi + 1) << 32);
+        }
+        if (i == xp) {
+            g |= get_bits(hp, x * h.hb, h.hb) << h.lb;
+            ++x;
+            xp = x < h.en ? get_bits(pb, x * h.eb, h.eb) : 0xffffffffu;
+        }
+        v += g;
+        if (v >= key) return v == key;
+    }
+    return false;
+}
+
+// Binary search for `key` over elements [t0, t1] of a residual-coded segment.
+__device__ __forceinline__ bool resid_find(const uint32_t *blk, const BlkHdr &h, const ResidParams &rp, uint32_t count,
+                                           int t0, int t1, uint32_t key) {
+    while (t0 <= t1) {
+        const int mid = (t0 + t1) >> 1;
+        const uint32_t v = resid_value(rp, (uint32_t)mid, block_value_ra(blk, h, count, (uint32_t)mid));
+        if (v == key) return true;
+        if (v < key) t0 = mid + 1;
+        else t1 = mid - 1;
+    }
+    return false;
+}
+
+// Learned model inference (root MLP + leaf) -> predicted rank and the leaf.
+// Every operation is an explicit round-to-nearest intrinsic so that the error
+// bounds measured at build time hold bit for bit at query time.
+__device__ __forceinline__ float model_root(const float *W, float x) {
+    const float *w1 = W, *b1 = W + kHidden, *w2 = W + 2 * kHidden, *b2 = w2 + kHidden * kHidden,
+                *w3 = b2 + kHidden, *b3 = w3 + kHidden;
+    float h1[kHidden];
+#pragma unroll
+    for (int i = 0; i < kHidden; ++i) h1[i] = fmaxf(__fmaf_rn(w1[i], x, b1[i]), 0.0f);
+    float out = b3[0];
+#pragma unroll 4
+    for (int o = 0; o < kHidden; ++o) {
+        float acc = b2[o];
+        const float *row = w2 + o * kHidden;
+#pragma unroll
+        for (int i = 0; i < kHidden; ++i) acc = __fmaf_rn(row[i], h1[i], acc);
+        out = __fmaf_rn(w3[o], fmaxf(acc, 0.0f), out);
+    }
+    return out;
+}
+
+__device__ __forceinline__ uint32_t model_leaf_of(float root_out, uint32_t nleaves) {
+    const float f = __fmul_rn(root_out, (float)nleaves);
+    int li = __float2int_rd(f);
+    li = li < 0 ? 0 : (li >= (int)nleaves ? (int)nleaves - 1 : li);
+    return (uint32_t)li;
+}
+
+__device__ __forceinline__ float model_norm(const ModelHdr &m, uint32_t key) {
+    return __fmul_rn(__fsub_rn(__uint2float_rn(key), m.kmin), m.kscale);
+}
+
+__device__ __forceinline__ int model_pred_rank(const Leaf &lf, float x) {
+    const float r = __fmaf_rn(lf.a, x, lf.b);
+    // clamp before the conversion so the result is defined
+    const float rc = fminf(fmaxf(r, -1.0e9f), 1.0e9f);
+    return __float2int_rd(rc);
+}
+
+}  // namespace excl

@@ -1,0 +1,92 @@
+// Internal layout shared by the host builder (codec.cpp) and the device
+// kernels (*.cu). Not part of the C ABI.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/excl_gpu.h"
+
+namespace excl {
+
+constexpr uint32_t kNoModel = 0xffffffffu;
+constexpr uint32_t kMaxTerms = 32;    // terms per query on the device
+constexpr uint32_t kTileKeys = 256;   // keys per tile (one shortest-list segment or a 256-slice of an HS bucket)
+constexpr uint32_t kWordPad = 8;      // zero words after the last block: 64/128-bit window reads stay in bounds
+
+// Device-resident description of one posting list (80 bytes, 16-byte aligned
+// so a warp reads it with 128-bit loads).
+struct alignas(16) ListDesc {
+    uint64_t word_base;   // first word of the list's blocks in the words[] array
+    uint32_t n;           // postings
+    uint32_t seg_base;    // first segment of the list in the per-segment arrays
+    uint32_t nseg;        // segments (fixed blocks, or non-empty HS blocks)
+    uint32_t codec;       // excl_codec
+    uint32_t log2_block;  // fixed block size = 1 << log2_block; 0 = variable (HS)
+    uint32_t first_doc;
+    uint32_t last_doc;
+    uint32_t reg[4];      // list-level regression raw bits (LRC: slope, icpt, range, 0; others a, b, L, R)
+    uint32_t dir_shift;   // bucket = docID >> dir_shift
+    uint32_t dir_base;    // first directory entry (ndir + 1 entries)
+    uint32_t ndir;        // buckets
+    uint32_t tile_base;   // variable lists: first tilemap entry
+    uint32_t ntiles;      // tiles when this list is the shortest of a query
+    uint32_t model;       // learned model slot or kNoModel
+    uint32_t pad;
+};
+static_assert(sizeof(ListDesc) == 80, "ListDesc layout");
+
+// Per-segment record: start element, word offset within the list, aux
+// (ParaPFD: docID at the segment middle = segMedian; residual codecs: base).
+struct alignas(16) SegRec {
+    uint32_t start;
+    uint32_t off;
+    uint32_t aux;
+    uint32_t count;
+};
+
+struct alignas(16) SegReg {
+    float a;
+    float b;
+    uint32_t L;
+    uint32_t R;
+};
+
+#ifdef __CUDACC__
+#define EXCL_HD __host__ __device__ __forceinline__
+#else
+#define EXCL_HD inline
+#endif
+
+EXCL_HD bool codec_is_hs(uint32_t c) { return c == EXCL_CODEC_HS_SEGLRC || c == EXCL_CODEC_HS_PARAPFD; }
+EXCL_HD bool codec_is_dgap(uint32_t c) { return c == EXCL_CODEC_PARAPFD || c == EXCL_CODEC_HS_PARAPFD; }
+
+struct DeviceIndex;  // runtime.cu
+struct ModelSet;     // learned.cu
+
+// Host image of a built index.
+struct HostIndex {
+    uint32_t nlists = 0;
+    uint64_t postings = 0;
+    std::vector<ListDesc> lists;
+    std::vector<uint32_t> words;
+    std::vector<uint32_t> seg_head;
+    std::vector<SegRec> seg_rec;
+    std::vector<SegReg> seg_reg;
+    std::vector<uint32_t> dir;
+    std::vector<uint64_t> tilemap;   // (segment within list << 32) | first element within segment
+    DeviceIndex *dev = nullptr;
+    ModelSet *models = nullptr;
+};
+
+// codec.cpp
+uint32_t pfd_encode_block(const uint32_t *in, uint32_t n, float frac, uint32_t *out, int *err);
+uint32_t pfd_decode_block(const uint32_t *in, uint32_t n, uint32_t *out);
+uint32_t pfd_block_words(const uint32_t *in, uint32_t n);
+int build_index(const uint32_t *docs, const uint64_t *loff, uint32_t nlists, const excl_build_params &p,
+                HostIndex &ix, std::string &err);
+
+}  // namespace excl
+
+struct excl_index : excl::HostIndex {};

@@ -1,0 +1,36 @@
+// Launch wrappers of kernels.cu and the per-batch device view.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "excl_device.cuh"
+
+namespace excl {
+
+struct BatchView {
+    uint32_t nq;
+    const uint32_t *qterms;      // nq * kMaxTerms list ids, ascending length
+    const uint32_t *qnterms;     // terms per query
+    const uint32_t *tile_prefix; // nq + 1, exclusive prefix of tiles per query
+    uint32_t *tile_counter;      // work-queue head (zeroed by k_pack)
+    uint32_t *tile_count;        // survivors per tile
+    uint32_t *scratch;           // max_tiles * kTileKeys survivor slots
+    uint32_t max_tiles;
+    uint32_t *err;               // error flag bits
+    uint64_t *stats;             // [probes, fallbacks] or null
+};
+
+int launch_decode(const DevIndexView &ix, uint32_t l0, uint32_t l1, uint64_t out_base0, uint32_t *out, uint32_t seg0,
+                  uint32_t nsegs, int nsm, cudaStream_t st);
+int launch_pack(const ListDesc *lists, uint32_t nlists, const uint32_t *terms, const uint32_t *toff, uint32_t nq,
+                const BatchView &b, uint32_t *ntiles, cudaStream_t st);
+uint32_t scan_blocks_for(uint64_t n);
+int launch_scan(const uint32_t *in, uint32_t *out, const uint32_t *n_dev, uint32_t n_host, uint64_t max_n,
+                uint64_t *state, uint32_t *ticket, uint32_t *err, cudaStream_t st);
+int launch_probe(const DevIndexView &ix, const BatchView &b, int algo, int warps, int ctas_per_sm, int nsm,
+                 cudaStream_t st);
+int launch_scatter(const BatchView &b, const uint32_t *tile_out, uint32_t *offsets, uint32_t *docids, uint64_t cap,
+                   int nsm, cudaStream_t st);
+
+}  // namespace excl

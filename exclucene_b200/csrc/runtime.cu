@@ -1,0 +1,579 @@
+// C ABI of libexcl_gpu.so: codec calls, index build/upload, contexts, the
+// batched query pipeline and its host-buffer submit/wait form.
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "excl_device.cuh"
+#include "kernels.h"
+#include "runtime.h"
+
+using namespace excl;
+
+// ---------------------------------------------------------------------------
+// Codec calls.
+
+extern "C" int excl_parapfd_encode(const uint32_t *in, uint32_t n, float frac, uint32_t *out, size_t cap,
+                                   size_t *words) {
+    if ((!in && n) || !out || !words) return EXCL_E_INVALID;
+    std::vector<uint32_t> tmp((size_t)n * 3 + 8);
+    int err = 0;
+    const uint32_t w = pfd_encode_block(in, n, frac, tmp.data(), &err);
+    if (err) return err;
+    if (w > cap) return EXCL_E_CAPACITY;
+    std::memcpy(out, tmp.data(), (size_t)w * 4);
+    *words = w;
+    return EXCL_OK;
+}
+
+extern "C" int excl_parapfd_decode(const uint32_t *in, size_t nwords, uint32_t n, uint32_t *out, size_t *consumed) {
+    if (!in || !out || !consumed || nwords == 0) return EXCL_E_INVALID;
+    const uint32_t need = pfd_block_words(in, n);
+    if (need > nwords) return EXCL_E_FORMAT;
+    *consumed = pfd_decode_block(in, n, out);
+    return EXCL_OK;
+}
+
+static float g_frac = 0.0f;
+extern "C" void excl_set_frac(float frac) { g_frac = frac; }
+
+extern "C" uint32_t encodeArray(const uint32_t *in, uint32_t *out, uint32_t n) {
+    int err = 0;
+    std::vector<uint32_t> tmp((size_t)n * 3 + 8);
+    const uint32_t w = pfd_encode_block(in, n, g_frac, tmp.data(), &err);
+    if (err) return 0;
+    std::memcpy(out, tmp.data(), (size_t)w * 4);
+    return w;
+}
+
+extern "C" uint32_t decodeArray(const uint32_t *in, uint32_t *out, uint32_t n) { return pfd_decode_block(in, n, out); }
+
+// ---------------------------------------------------------------------------
+// Index build / export.
+
+extern "C" int excl_index_build(const uint32_t *docs, const uint64_t *list_offsets, uint32_t nlists,
+                                const excl_build_params *params, excl_index **out) {
+    if (!params || !out) return EXCL_E_INVALID;
+    excl_index *ix = new (std::nothrow) excl_index();
+    if (!ix) return EXCL_E_NOMEM;
+    std::string err;
+    int st;
+    try {
+        st = build_index(docs, list_offsets, nlists, *params, *ix, err);
+    } catch (const std::bad_alloc &) {
+        st = EXCL_E_NOMEM;
+    }
+    if (st) {
+        std::fprintf(stderr, "excl_index_build: %s\n", err.c_str());
+        delete ix;
+        return st;
+    }
+    *out = ix;
+    return EXCL_OK;
+}
+
+extern "C" int excl_index_sizes_get(const excl_index *ix, excl_index_sizes *s) {
+    if (!ix || !s) return EXCL_E_INVALID;
+    s->nlists = ix->nlists;
+    s->nsegs = ix->seg_head.size();
+    s->nwords = ix->words.size();
+    s->ndir = ix->dir.size();
+    s->ntilemap = ix->tilemap.size();
+    s->postings = ix->postings;
+    s->device_bytes = ix->dev ? ix->dev->bytes : 0;
+    return EXCL_OK;
+}
+
+extern "C" int excl_index_export(const excl_index *ix, excl_list_info *lists, uint32_t *words, uint32_t *seg_head,
+                                 uint32_t *seg_rec, uint32_t *seg_reg, uint32_t *dir) {
+    if (!ix) return EXCL_E_INVALID;
+    if (lists)
+        for (uint32_t l = 0; l < ix->nlists; ++l) {
+            const ListDesc &d = ix->lists[l];
+            excl_list_info &o = lists[l];
+            o.word_base = d.word_base;
+            o.n = d.n;
+            o.seg_base = d.seg_base;
+            o.nseg = d.nseg;
+            o.codec = d.codec;
+            o.log2_block = d.log2_block;
+            o.first_doc = d.first_doc;
+            o.last_doc = d.last_doc;
+            std::memcpy(o.reg, d.reg, sizeof(o.reg));
+            o.dir_shift = d.dir_shift;
+            o.dir_base = d.dir_base;
+            o.ndir = d.ndir;
+            o.tile_base = d.tile_base;
+            o.ntiles = d.ntiles;
+            o.model = d.model;
+        }
+    if (words) std::memcpy(words, ix->words.data(), ix->words.size() * 4);
+    if (seg_head) std::memcpy(seg_head, ix->seg_head.data(), ix->seg_head.size() * 4);
+    if (seg_rec) std::memcpy(seg_rec, ix->seg_rec.data(), ix->seg_rec.size() * sizeof(SegRec));
+    if (seg_reg) std::memcpy(seg_reg, ix->seg_reg.data(), ix->seg_reg.size() * sizeof(SegReg));
+    if (dir) std::memcpy(dir, ix->dir.data(), ix->dir.size() * 4);
+    return EXCL_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Context.
+
+namespace excl {
+
+void ctx_error(excl_ctx *ctx, const char *fmt, ...) {
+    if (!ctx) return;
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    std::lock_guard<std::mutex> g(ctx->mu);
+    ctx->last_error = buf;
+}
+
+int cuda_status(excl_ctx *ctx, cudaError_t e, const char *what) {
+    if (e == cudaSuccess) return EXCL_OK;
+    ctx_error(ctx, "%s: %s", what, cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? EXCL_E_NOMEM : EXCL_E_CUDA;
+}
+
+template <typename T>
+static int dalloc(excl_ctx *ctx, T **p, size_t count, const char *what) {
+    *p = nullptr;
+    if (count == 0) count = 1;
+    return cuda_status(ctx, cudaMalloc((void **)p, count * sizeof(T)), what);
+}
+
+void DeviceIndex::release() {
+    cudaFree(lists);
+    cudaFree(words);
+    cudaFree(seg_head);
+    cudaFree(seg_rec);
+    cudaFree(seg_reg);
+    cudaFree(dir);
+    cudaFree(tilemap);
+    cudaFree(post_base);
+    lists = nullptr;
+    words = seg_head = dir = nullptr;
+    seg_rec = nullptr;
+    seg_reg = nullptr;
+    tilemap = post_base = nullptr;
+}
+
+DevIndexView DeviceIndex::view(const ModelView &mv) const {
+    DevIndexView v;
+    v.lists = lists;
+    v.words = words;
+    v.seg_head = seg_head;
+    v.seg_rec = seg_rec;
+    v.seg_reg = seg_reg;
+    v.dir = dir;
+    v.tilemap = tilemap;
+    v.post_base = post_base;
+    v.models = mv;
+    return v;
+}
+
+int ctx_alloc_batch(excl_ctx *ctx) {
+    const excl_ctx_config &c = ctx->cfg;
+    ctx->max_tiles = (uint32_t)std::min<uint64_t>(0xffffffffull, c.max_keys / kTileKeys + c.max_queries + 1);
+    int st = 0;
+    st |= dalloc(ctx, &ctx->d_terms, (size_t)c.max_queries * kMaxTerms, "alloc terms");
+    st |= dalloc(ctx, &ctx->d_toff, (size_t)c.max_queries + 1, "alloc term offsets");
+    st |= dalloc(ctx, &ctx->d_qterms, (size_t)c.max_queries * kMaxTerms, "alloc qterms");
+    st |= dalloc(ctx, &ctx->d_qnterms, (size_t)c.max_queries, "alloc qnterms");
+    st |= dalloc(ctx, &ctx->d_ntiles, (size_t)c.max_queries + 1, "alloc ntiles");
+    st |= dalloc(ctx, &ctx->d_tile_prefix, (size_t)c.max_queries + 2, "alloc tile prefix");
+    st |= dalloc(ctx, &ctx->d_tile_count, (size_t)ctx->max_tiles + 1, "alloc tile count");
+    st |= dalloc(ctx, &ctx->d_tile_out, (size_t)ctx->max_tiles + 2, "alloc tile out");
+    st |= dalloc(ctx, &ctx->d_scratch, (size_t)ctx->max_tiles * kTileKeys, "alloc scratch");
+    st |= dalloc(ctx, &ctx->d_misc, 16, "alloc misc");
+    st |= dalloc(ctx, &ctx->d_stats, 4, "alloc stats");
+    const uint32_t nsb = std::max(scan_blocks_for(c.max_queries + 1), scan_blocks_for(ctx->max_tiles + 1));
+    st |= dalloc(ctx, &ctx->d_scan_state, nsb, "alloc scan state");
+    st |= dalloc(ctx, &ctx->d_offsets, (size_t)c.max_queries + 1, "alloc offsets");
+    ctx->docids_cap = (uint64_t)ctx->max_tiles * kTileKeys;
+    st |= dalloc(ctx, &ctx->d_docids, ctx->docids_cap, "alloc docids");
+    st |= cuda_status(ctx, cudaMallocHost((void **)&ctx->h_terms, (size_t)c.max_queries * kMaxTerms * 4), "pinned");
+    st |= cuda_status(ctx, cudaMallocHost((void **)&ctx->h_toff, ((size_t)c.max_queries + 1) * 4), "pinned");
+    st |= cuda_status(ctx, cudaMallocHost((void **)&ctx->h_offsets, ((size_t)c.max_queries + 1) * 4), "pinned");
+    if (st) return EXCL_E_NOMEM;
+    cudaMemsetAsync(ctx->d_misc, 0, 16 * 4, ctx->stream);
+    cudaMemsetAsync(ctx->d_stats, 0, 4 * 8, ctx->stream);
+    return cuda_status(ctx, cudaStreamSynchronize(ctx->stream), "ctx init");
+}
+
+// Runs the whole device pipeline for nq queries whose terms are in device memory.
+int run_pipeline(excl_ctx *ctx, excl_index *ix, const uint32_t *d_terms, const uint32_t *d_toff, uint32_t nq,
+                 uint32_t algo, uint32_t *d_offsets, uint32_t *d_docids, uint64_t cap) {
+    if (!ix->dev) {
+        ctx_error(ctx, "index not uploaded");
+        return EXCL_E_INVALID;
+    }
+    if (nq > ctx->cfg.max_queries) {
+        ctx_error(ctx, "batch of %u queries exceeds max_queries %u", nq, ctx->cfg.max_queries);
+        return EXCL_E_CAPACITY;
+    }
+    if (algo > EXCL_ALGO_LEARNED) {
+        ctx_error(ctx, "unknown algo %u", algo);
+        return EXCL_E_INVALID;
+    }
+    cudaStream_t st = ctx->stream;
+    BatchView b{};
+    b.nq = nq;
+    b.qterms = ctx->d_qterms;
+    b.qnterms = ctx->d_qnterms;
+    b.tile_prefix = ctx->d_tile_prefix;
+    b.tile_counter = ctx->d_misc + kMiscTileCounter;
+    b.tile_count = ctx->d_tile_count;
+    b.scratch = ctx->d_scratch;
+    b.max_tiles = ctx->max_tiles;
+    b.err = ctx->d_misc + kMiscErr;
+    b.stats = ctx->collect_stats ? ctx->d_stats : nullptr;
+    const DevIndexView ixv = ix->dev->view(ix->models ? model_view(ix->models) : ModelView{});
+    if (ctx->collect_stats) cudaMemsetAsync(ctx->d_stats, 0, 3 * 8, st);
+    cudaEventRecord(ctx->ev[0], st);
+    int e = 0;
+    e |= launch_pack(ix->dev->lists, ix->nlists, d_terms, d_toff, nq, b, ctx->d_ntiles, st);
+    e |= launch_scan(ctx->d_ntiles, ctx->d_tile_prefix, nullptr, nq, ctx->cfg.max_queries, ctx->d_scan_state,
+                     ctx->d_misc + kMiscTicket0, b.err, st);
+    cudaEventRecord(ctx->ev[1], st);
+    e |= launch_probe(ixv, b, (int)algo, ctx->warps, ctx->ctas_per_sm, ctx->nsm, st);
+    cudaEventRecord(ctx->ev[2], st);
+    e |= launch_scan(ctx->d_tile_count, ctx->d_tile_out, ctx->d_tile_prefix + nq, 0, ctx->max_tiles,
+                     ctx->d_scan_state, ctx->d_misc + kMiscTicket1, b.err, st);
+    e |= launch_scatter(b, ctx->d_tile_out, d_offsets, d_docids, cap, ctx->nsm, st);
+    cudaEventRecord(ctx->ev[3], st);
+    if (e) return cuda_status(ctx, (cudaError_t)e, "launch");
+    ctx->last_nq = nq;
+    return EXCL_OK;
+}
+
+int read_device_flags(excl_ctx *ctx) {
+    uint32_t f = 0;
+    cudaError_t e = cudaMemcpy(&f, ctx->d_misc + kMiscErr, 4, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_status(ctx, e, "read error flag");
+    if (f) {
+        cudaMemset(ctx->d_misc + kMiscErr, 0, 4);
+        ctx_error(ctx, "device error flags 0x%x (%s%s%s%s%s)", f, (f & kErrTerms) ? "too many terms " : "",
+                  (f & kErrScanSpin) ? "scan wait expired " : "", (f & kErrTermId) ? "term id out of range " : "",
+                  (f & kErrCapacity) ? "result capacity " : "", (f & kErrModel) ? "model " : "");
+        if (f & kErrCapacity) return EXCL_E_CAPACITY;
+        if (f & (kErrTermId | kErrTerms)) return EXCL_E_INVALID;
+        return EXCL_E_DEVICE_FLAG;
+    }
+    return EXCL_OK;
+}
+
+}  // namespace excl
+
+extern "C" int excl_ctx_create(int device, const excl_ctx_config *cfg, excl_ctx **out) {
+    if (!out) return EXCL_E_INVALID;
+    *out = nullptr;
+    excl_ctx *ctx = new (std::nothrow) excl_ctx();
+    if (!ctx) return EXCL_E_NOMEM;
+    ctx->device = device;
+    excl_ctx_config c{};
+    if (cfg) c = *cfg;
+    if (c.max_queries == 0) c.max_queries = 65536;
+    if (c.max_terms == 0 || c.max_terms > kMaxTerms) c.max_terms = kMaxTerms;
+    if (c.max_keys == 0) c.max_keys = 1ull << 26;
+    ctx->cfg = c;
+    ctx->warps = c.warps_per_cta ? (int)c.warps_per_cta : 8;
+    ctx->ctas_per_sm = c.ctas_per_sm ? (int)c.ctas_per_sm : 4;
+    int st = cuda_status(ctx, cudaSetDevice(device), "cudaSetDevice");
+    if (!st) st = cuda_status(ctx, cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, device), "attr");
+    if (!st) st = cuda_status(ctx, cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking), "stream");
+    for (int i = 0; i < 4 && !st; ++i) st = cuda_status(ctx, cudaEventCreate(&ctx->ev[i]), "event");
+    if (!st) st = ctx_alloc_batch(ctx);
+    if (st) {
+        std::fprintf(stderr, "excl_ctx_create: %s\n", ctx->last_error.c_str());
+        excl_ctx_destroy(ctx);
+        return st;
+    }
+    *out = ctx;
+    return EXCL_OK;
+}
+
+extern "C" int excl_ctx_destroy(excl_ctx *ctx) {
+    if (!ctx) return EXCL_E_INVALID;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    uint32_t *bufs[] = {ctx->d_terms,      ctx->d_toff,     ctx->d_qterms, ctx->d_qnterms, ctx->d_ntiles,
+                        ctx->d_tile_prefix, ctx->d_tile_count, ctx->d_tile_out, ctx->d_scratch, ctx->d_misc,
+                        ctx->d_offsets,    ctx->d_docids};
+    for (uint32_t *p : bufs) cudaFree(p);
+    cudaFree(ctx->d_stats);
+    cudaFree(ctx->d_scan_state);
+    cudaFreeHost(ctx->h_terms);
+    cudaFreeHost(ctx->h_toff);
+    cudaFreeHost(ctx->h_offsets);
+    for (auto &e : ctx->ev)
+        if (e) cudaEventDestroy(e);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return EXCL_OK;
+}
+
+extern "C" const char *excl_last_error(const excl_ctx *ctx) { return ctx ? ctx->last_error.c_str() : "null context"; }
+
+extern "C" void *excl_ctx_stream(excl_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+extern "C" int excl_index_upload(excl_ctx *ctx, excl_index *ix) {
+    if (!ctx || !ix) return EXCL_E_INVALID;
+    cudaSetDevice(ctx->device);
+    if (ix->dev) {
+        ix->dev->release();
+        delete ix->dev;
+        ix->dev = nullptr;
+    }
+    DeviceIndex *d = new (std::nothrow) DeviceIndex();
+    if (!d) return EXCL_E_NOMEM;
+    std::vector<uint64_t> pb(ix->nlists + 1, 0);
+    for (uint32_t l = 0; l < ix->nlists; ++l) pb[l + 1] = pb[l] + ix->lists[l].n;
+    int st = 0;
+    st |= dalloc(ctx, &d->lists, ix->lists.size(), "index lists");
+    st |= dalloc(ctx, &d->words, ix->words.size(), "index words");
+    st |= dalloc(ctx, &d->seg_head, ix->seg_head.size(), "index heads");
+    st |= dalloc(ctx, &d->seg_rec, ix->seg_rec.size(), "index recs");
+    st |= dalloc(ctx, &d->seg_reg, ix->seg_reg.size(), "index regs");
+    st |= dalloc(ctx, &d->dir, ix->dir.size(), "index dir");
+    st |= dalloc(ctx, &d->tilemap, ix->tilemap.size(), "index tilemap");
+    st |= dalloc(ctx, &d->post_base, pb.size(), "index post base");
+    if (st) {
+        d->release();
+        delete d;
+        return EXCL_E_NOMEM;
+    }
+    auto up = [&](void *dst, const void *src, size_t bytes) {
+        if (bytes && !st) st = cuda_status(ctx, cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice), "index upload");
+    };
+    up(d->lists, ix->lists.data(), ix->lists.size() * sizeof(ListDesc));
+    up(d->words, ix->words.data(), ix->words.size() * 4);
+    up(d->seg_head, ix->seg_head.data(), ix->seg_head.size() * 4);
+    up(d->seg_rec, ix->seg_rec.data(), ix->seg_rec.size() * sizeof(SegRec));
+    up(d->seg_reg, ix->seg_reg.data(), ix->seg_reg.size() * sizeof(SegReg));
+    up(d->dir, ix->dir.data(), ix->dir.size() * 4);
+    up(d->tilemap, ix->tilemap.data(), ix->tilemap.size() * 8);
+    up(d->post_base, pb.data(), pb.size() * 8);
+    if (st) {
+        d->release();
+        delete d;
+        return st;
+    }
+    d->bytes = ix->lists.size() * sizeof(ListDesc) + ix->words.size() * 4 + ix->seg_head.size() * 4 +
+               ix->seg_rec.size() * sizeof(SegRec) + ix->seg_reg.size() * sizeof(SegReg) + ix->dir.size() * 4 +
+               ix->tilemap.size() * 8 + pb.size() * 8;
+    d->device = ctx->device;
+    ix->dev = d;
+    if (ix->models) st = models_upload(ctx, ix);
+    return st;
+}
+
+extern "C" int excl_index_free(excl_index *ix) {
+    if (!ix) return EXCL_E_INVALID;
+    if (ix->dev) {
+        cudaSetDevice(ix->dev->device);
+        ix->dev->release();
+        delete ix->dev;
+    }
+    if (ix->models) models_free(ix->models);
+    delete ix;
+    return EXCL_OK;
+}
+
+extern "C" int excl_decode_lists_device(excl_ctx *ctx, excl_index *ix, uint32_t l0, uint32_t l1, uint32_t *d_out) {
+    if (!ctx || !ix || !d_out || l0 >= l1 || l1 > ix->nlists) return EXCL_E_INVALID;
+    if (!ix->dev) {
+        ctx_error(ctx, "index not uploaded");
+        return EXCL_E_INVALID;
+    }
+    cudaSetDevice(ctx->device);
+    uint64_t base0 = 0;
+    for (uint32_t l = 0; l < l0; ++l) base0 += ix->lists[l].n;
+    const uint32_t seg0 = ix->lists[l0].seg_base;
+    const uint32_t seg1 = ix->lists[l1 - 1].seg_base + ix->lists[l1 - 1].nseg;
+    const int e = launch_decode(ix->dev->view(ModelView{}), l0, l1, base0, d_out, seg0, seg1 - seg0, ctx->nsm,
+                                ctx->stream);
+    return cuda_status(ctx, (cudaError_t)e, "decode launch");
+}
+
+extern "C" int excl_decode_lists(excl_ctx *ctx, excl_index *ix, uint32_t l0, uint32_t l1, uint32_t *out, size_t cap) {
+    if (!ctx || !ix || !out || l0 >= l1 || l1 > ix->nlists) return EXCL_E_INVALID;
+    uint64_t n = 0;
+    for (uint32_t l = l0; l < l1; ++l) n += ix->lists[l].n;
+    if (n > cap) return EXCL_E_CAPACITY;
+    cudaSetDevice(ctx->device);
+    uint32_t *d = nullptr;
+    int st = dalloc(ctx, &d, n, "decode buffer");
+    if (st) return st;
+    st = excl_decode_lists_device(ctx, ix, l0, l1, d);
+    if (!st) st = cuda_status(ctx, cudaMemcpyAsync(out, d, n * 4, cudaMemcpyDeviceToHost, ctx->stream), "decode d2h");
+    if (!st) st = cuda_status(ctx, cudaStreamSynchronize(ctx->stream), "decode sync");
+    cudaFree(d);
+    return st;
+}
+
+// ---------------------------------------------------------------------------
+// Batches.
+
+extern "C" int excl_intersect_device(excl_ctx *ctx, excl_index *ix, const uint32_t *d_terms,
+                                     const uint32_t *d_term_offsets, uint32_t nq, uint32_t algo, uint32_t *d_offsets,
+                                     uint32_t *d_docids, uint64_t cap) {
+    if (!ctx || !ix || !d_term_offsets || !d_offsets || (!d_docids && cap)) return EXCL_E_INVALID;
+    cudaSetDevice(ctx->device);
+    return run_pipeline(ctx, ix, d_terms, d_term_offsets, nq, algo, d_offsets, d_docids, cap);
+}
+
+extern "C" int excl_ctx_check(excl_ctx *ctx) {
+    if (!ctx) return EXCL_E_INVALID;
+    cudaSetDevice(ctx->device);
+    int st = cuda_status(ctx, cudaStreamSynchronize(ctx->stream), "stream sync");
+    if (st) return st;
+    return read_device_flags(ctx);
+}
+
+struct excl_batch {
+    excl_ctx *ctx;
+    uint32_t nq;
+    cudaEvent_t done;
+    bool waited;
+};
+
+extern "C" int excl_submit(excl_ctx *ctx, excl_index *ix, const uint32_t *terms, const uint32_t *term_offsets,
+                           uint32_t nq, uint32_t algo, excl_batch **ticket) {
+    if (!ctx || !ix || !term_offsets || !ticket) return EXCL_E_INVALID;
+    *ticket = nullptr;
+    if (nq > ctx->cfg.max_queries) {
+        ctx_error(ctx, "batch of %u queries exceeds max_queries %u", nq, ctx->cfg.max_queries);
+        return EXCL_E_CAPACITY;
+    }
+    const uint32_t nterms = term_offsets[nq] - term_offsets[0];
+    if (nterms > (uint64_t)ctx->cfg.max_queries * kMaxTerms) return EXCL_E_CAPACITY;
+    for (uint32_t q = 0; q < nq; ++q) {
+        if (term_offsets[q + 1] < term_offsets[q]) return EXCL_E_INVALID;
+        if (term_offsets[q + 1] - term_offsets[q] > kMaxTerms) {
+            ctx_error(ctx, "query %u has more than %u terms", q, kMaxTerms);
+            return EXCL_E_CAPACITY;
+        }
+    }
+    for (uint32_t i = 0; i < nterms; ++i)
+        if (terms[term_offsets[0] + i] >= ix->nlists) {
+            ctx_error(ctx, "term id %u out of range", terms[term_offsets[0] + i]);
+            return EXCL_E_INVALID;
+        }
+    cudaSetDevice(ctx->device);
+    // wait for the previous batch to release the shared buffers
+    cudaStreamSynchronize(ctx->stream);
+    std::memcpy(ctx->h_terms, terms + term_offsets[0], (size_t)nterms * 4);
+    for (uint32_t q = 0; q <= nq; ++q) ctx->h_toff[q] = term_offsets[q] - term_offsets[0];
+    cudaStream_t st = ctx->stream;
+    int s = cuda_status(ctx, cudaMemcpyAsync(ctx->d_terms, ctx->h_terms, (size_t)nterms * 4, cudaMemcpyHostToDevice, st),
+                        "h2d terms");
+    if (!s)
+        s = cuda_status(ctx, cudaMemcpyAsync(ctx->d_toff, ctx->h_toff, ((size_t)nq + 1) * 4, cudaMemcpyHostToDevice, st),
+                        "h2d offsets");
+    if (!s) s = run_pipeline(ctx, ix, ctx->d_terms, ctx->d_toff, nq, algo, ctx->d_offsets, ctx->d_docids, ctx->docids_cap);
+    if (!s)
+        s = cuda_status(ctx, cudaMemcpyAsync(ctx->h_offsets, ctx->d_offsets, ((size_t)nq + 1) * 4,
+                                             cudaMemcpyDeviceToHost, st),
+                        "d2h offsets");
+    if (s) return s;
+    excl_batch *b = new (std::nothrow) excl_batch{ctx, nq, nullptr, false};
+    if (!b) return EXCL_E_NOMEM;
+    s = cuda_status(ctx, cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming), "event");
+    if (!s) s = cuda_status(ctx, cudaEventRecord(b->done, st), "record");
+    if (s) {
+        delete b;
+        return s;
+    }
+    *ticket = b;
+    return EXCL_OK;
+}
+
+extern "C" int excl_wait(excl_batch *b, uint32_t *offsets, uint32_t *docids, size_t cap, int timeout_ms,
+                         uint64_t *total) {
+    if (!b) return EXCL_E_INVALID;
+    excl_ctx *ctx = b->ctx;
+    cudaSetDevice(ctx->device);
+    const auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+        const cudaError_t q = cudaEventQuery(b->done);
+        if (q == cudaSuccess) break;
+        if (q != cudaErrorNotReady) return cuda_status(ctx, q, "batch");
+        if (timeout_ms >= 0 &&
+            std::chrono::steady_clock::now() - t0 > std::chrono::milliseconds(timeout_ms))
+            return EXCL_E_TIMEOUT;
+        std::this_thread::sleep_for(std::chrono::microseconds(20));
+    }
+    int s = read_device_flags(ctx);
+    if (s) return s;
+    const uint32_t tot = ctx->h_offsets[b->nq];
+    if (total) *total = tot;
+    if (offsets) std::memcpy(offsets, ctx->h_offsets, ((size_t)b->nq + 1) * 4);
+    if (docids) {
+        if (tot > cap) {
+            ctx_error(ctx, "result buffer holds %zu docIDs, batch produced %u", cap, tot);
+            return EXCL_E_CAPACITY;
+        }
+        s = cuda_status(ctx, cudaMemcpyAsync(docids, ctx->d_docids, (size_t)tot * 4, cudaMemcpyDeviceToHost, ctx->stream),
+                        "d2h docids");
+        if (!s) s = cuda_status(ctx, cudaStreamSynchronize(ctx->stream), "sync");
+    }
+    b->waited = true;
+    return s;
+}
+
+extern "C" int excl_batch_free(excl_batch *b) {
+    if (!b) return EXCL_E_INVALID;
+    if (b->done) cudaEventDestroy(b->done);
+    delete b;
+    return EXCL_OK;
+}
+
+extern "C" int excl_last_stats(excl_ctx *ctx, excl_batch_stats *stt) {
+    if (!ctx || !stt) return EXCL_E_INVALID;
+    cudaSetDevice(ctx->device);
+    int s = cuda_status(ctx, cudaStreamSynchronize(ctx->stream), "sync");
+    if (s) return s;
+    std::memset(stt, 0, sizeof *stt);
+    cudaEventElapsedTime(&stt->pack_ms, ctx->ev[0], ctx->ev[1]);
+    cudaEventElapsedTime(&stt->probe_ms, ctx->ev[1], ctx->ev[2]);
+    cudaEventElapsedTime(&stt->compact_ms, ctx->ev[2], ctx->ev[3]);
+    cudaEventElapsedTime(&stt->total_ms, ctx->ev[0], ctx->ev[3]);
+    uint32_t T = 0;
+    cudaMemcpy(&T, ctx->d_tile_prefix + ctx->last_nq, 4, cudaMemcpyDeviceToHost);
+    stt->tiles = T;
+    uint64_t hs[3] = {0, 0, 0};
+    if (ctx->collect_stats) cudaMemcpy(hs, ctx->d_stats, 24, cudaMemcpyDeviceToHost);
+    stt->probes = hs[0];
+    stt->fallbacks = hs[1];
+    stt->keys = hs[2];
+    return EXCL_OK;
+}
+
+extern "C" int excl_checksum(uint32_t nq, const uint32_t *offsets, const uint32_t *docids, uint64_t cs[3]) {
+    if (!offsets || !cs) return EXCL_E_INVALID;
+    cs[0] = cs[1] = cs[2] = 0;
+    for (uint32_t q = 0; q < nq; ++q) {
+        const uint32_t n = offsets[q + 1] - offsets[q];
+        if (!n) {
+            ++cs[0];
+            continue;
+        }
+        const uint32_t *r = docids + offsets[q];
+        cs[1] += n;
+        cs[2] ^= r[0];
+        cs[2] ^= r[n - 1];
+        cs[2] ^= r[n / 2];
+    }
+    return EXCL_OK;
+}

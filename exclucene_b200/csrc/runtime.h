@@ -1,0 +1,65 @@
+// Host-side state of a context and of a device-resident index.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <mutex>
+#include <string>
+
+#include "excl_device.cuh"
+
+namespace excl {
+
+struct DeviceIndex {
+    ListDesc *lists = nullptr;
+    uint32_t *words = nullptr;
+    uint32_t *seg_head = nullptr;
+    SegRec *seg_rec = nullptr;
+    SegReg *seg_reg = nullptr;
+    uint32_t *dir = nullptr;
+    uint64_t *tilemap = nullptr;
+    uint64_t *post_base = nullptr;
+    size_t bytes = 0;
+    int device = 0;
+    void release();
+    DevIndexView view(const ModelView &mv) const;
+};
+
+// slots of ctx->d_misc
+enum { kMiscErr = 0, kMiscTileCounter = 1, kMiscTicket0 = 2, kMiscTicket1 = 3 };
+
+}  // namespace excl
+
+struct excl_ctx {
+    int device = 0;
+    int nsm = 148;
+    int warps = 8;
+    int ctas_per_sm = 4;
+    bool collect_stats = true;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    excl_ctx_config cfg{};
+    std::mutex mu;
+    std::string last_error;
+    uint32_t max_tiles = 0;
+    uint32_t last_nq = 0;
+    uint32_t *d_terms = nullptr, *d_toff = nullptr;
+    uint32_t *d_qterms = nullptr, *d_qnterms = nullptr, *d_ntiles = nullptr, *d_tile_prefix = nullptr;
+    uint32_t *d_tile_count = nullptr, *d_tile_out = nullptr, *d_scratch = nullptr, *d_misc = nullptr;
+    uint64_t *d_stats = nullptr, *d_scan_state = nullptr;
+    uint32_t *d_offsets = nullptr, *d_docids = nullptr;
+    uint64_t docids_cap = 0;
+    uint32_t *h_terms = nullptr, *h_toff = nullptr, *h_offsets = nullptr;
+};
+
+namespace excl {
+void ctx_error(excl_ctx *ctx, const char *fmt, ...);
+int cuda_status(excl_ctx *ctx, cudaError_t e, const char *what);
+int read_device_flags(excl_ctx *ctx);
+int run_pipeline(excl_ctx *ctx, excl_index *ix, const uint32_t *d_terms, const uint32_t *d_toff, uint32_t nq,
+                 uint32_t algo, uint32_t *d_offsets, uint32_t *d_docids, uint64_t cap);
+
+// learned.cu
+ModelView model_view(const ModelSet *m);
+int models_upload(excl_ctx *ctx, excl_index *ix);
+void models_free(ModelSet *m);
+}  // namespace excl

@@ -1,0 +1,185 @@
+/*
+ * excl_gpu.h — C ABI of libexcl_gpu.so, the B200 (sm_100a) implementation of
+ * ExCLucene's batched decode + conjunctive (AND) intersection of compressed
+ * posting lists in the ParaPFD, LRC, LRCSeg, SegLRC and hash-segmentation (HS)
+ * formats.
+ *
+ * Plain C types only: pointers, sizes, integer status codes. Every call returns
+ * an excl_status; nothing aborts the caller. Reference paths below are relative
+ * to the ExCLucene source tree.
+ */
+#ifndef EXCL_GPU_H_
+#define EXCL_GPU_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. Replace the reference's exit()-on-error paths:
+ * CUDA_SAFE_CALL (ParaPFD_Intersection_kernel.cu:8-15) and the capacity checks
+ * of CPUPreprocess (ParaPFD_Intersection.cu:204-212). */
+typedef enum {
+    EXCL_OK = 0,
+    EXCL_E_INVALID = 1,     /* bad argument (null pointer, unknown term id, ...) */
+    EXCL_E_CUDA = 2,        /* a CUDA runtime call failed */
+    EXCL_E_CAPACITY = 3,    /* a batch or buffer exceeds its capacity */
+    EXCL_E_FORMAT = 4,      /* data not representable in / not valid for the format */
+    EXCL_E_TIMEOUT = 5,     /* excl_wait timed out; the batch is still in flight */
+    EXCL_E_DEVICE_FLAG = 6, /* a kernel raised its error flag (bounded wait expired, bad index) */
+    EXCL_E_NOMEM = 7        /* host or device allocation failed */
+} excl_status;
+
+/* List formats (one codec per list). Block bytes are the reference ParaPFD
+ * layout (ParaPFor.cpp:75-113); see excl_build_params for the segmentation. */
+typedef enum {
+    EXCL_CODEC_PARAPFD = 0,   /* d-gaps, ParaPFD blocks (ParaPFD_Compression/main.cpp:163-189) */
+    EXCL_CODEC_LRC = 1,       /* list regression, int intercept (LRC_Generator.cu:155-287) */
+    EXCL_CODEC_LRCSEG = 2,    /* list regression + per-segment base (LRCSeg_Generator*.cu) */
+    EXCL_CODEC_SEGLRC = 3,    /* per-segment regression + base (SegLRC_Generator.cu:94-436) */
+    EXCL_CODEC_HS_SEGLRC = 4, /* hash buckets, per-bucket regression + base (HS_SegLRC_Generator.cu) */
+    EXCL_CODEC_HS_PARAPFD = 5 /* hash buckets, d-gap ParaPFD blocks inside each bucket */
+} excl_codec;
+
+/* Search method for locating a probe in a longer list. */
+typedef enum {
+    EXCL_ALGO_AUTO = 0,     /* learned where a model exists, else hash directory */
+    EXCL_ALGO_BSEARCH = 1,  /* binary search over segment heads (cuda_binarySearch_kernel.cu:167-296) */
+    EXCL_ALGO_HASHSEG = 2,  /* top-bits bucket directory (cuda_hashSegment_kernel.cu:170-314) */
+    EXCL_ALGO_LEARNED = 3   /* two-stage learned position model with exact error window */
+} excl_algo;
+
+/* ---------------------------------------------------------------------------
+ * Codec calls — replace `uint32_t encodeArray(const uint32_t*, uint32_t*, uint32_t)`
+ * and `decodeArray` (Compressed/include/ParaPFor.h:15-16). Reentrant; FRAC is an
+ * argument instead of the global `float FRAC` (ParaPFor.cpp:38). Byte-identical
+ * blocks. `cap` is the capacity of `out` in words. */
+int excl_parapfd_encode(const uint32_t *in, uint32_t n, float frac, uint32_t *out, size_t cap, size_t *words);
+int excl_parapfd_decode(const uint32_t *in, size_t nwords, uint32_t n, uint32_t *out, size_t *consumed);
+
+/* Compatibility shims with the reference's exact signatures (ParaPFor.h:15-16);
+ * they use the process-wide FRAC set by excl_set_frac (default 0.0). Return 0
+ * where the reference would write an unrepresentable block. */
+void excl_set_frac(float frac);
+uint32_t encodeArray(const uint32_t *in, uint32_t *out, uint32_t n);
+uint32_t decodeArray(const uint32_t *in, uint32_t *out, uint32_t n);
+
+/* ---------------------------------------------------------------------------
+ * Index build (host). Replaces the offline encoders X_Compression / X_Generator
+ * (e.g. ParaPFD_Compression/main.cpp:81-232, SegLRC_Generator.cu:94-436,
+ * HS_SegLRC_Generator.cu:503-594) that wrote the .ind1, .ind2, .segHead, .segOffset,
+ * .segMedian, .segNum, .regression_info and .HashSeg files. Input: sorted, duplicate-free docID lists in CSR form. */
+typedef struct {
+    uint32_t codec;        /* excl_codec used for every list unless `codecs` is set */
+    const uint8_t *codecs; /* optional per-list codec (nlists entries) or NULL */
+    uint32_t block;        /* segment size for fixed-block codecs: 128 or 256 (reference: 256) */
+    float frac;            /* ParaPFD exception fraction (reference sweep 0..0.64) */
+    uint32_t hs_bucket;    /* HS: expected bucket size (reference kExceptedBucketSize = 256), used when hs_kbits = 0 */
+    uint32_t hs_kbits;     /* HS: fixed number of top bits of a hs_ubits-bit universe (0 = derive from length) */
+    uint32_t hs_ubits;     /* HS: universe bits for hs_kbits */
+    uint32_t threads;      /* host threads for the build (0 = all cores) */
+} excl_build_params;
+
+typedef struct excl_index excl_index;
+
+int excl_index_build(const uint32_t *docs, const uint64_t *list_offsets, uint32_t nlists,
+                     const excl_build_params *params, excl_index **out);
+int excl_index_free(excl_index *ix);
+
+/* Sizes and host arrays of a built index (for checkers and the file writers).
+ * Layout per list: see excl_list_info. Per segment: head, rec {start, word
+ * offset, aux (ParaPFD: median docID; residual codecs: base)}, reg {a, b, L, R}. */
+typedef struct {
+    uint64_t word_base;
+    uint32_t n, seg_base, nseg, codec, log2_block, first_doc, last_doc;
+    uint32_t reg[4];      /* list regression raw bits: LRC {slope, icpt, range, 0}; LRCSeg/SegLRC {a, b, L, R} */
+    uint32_t dir_shift, dir_base, ndir;
+    uint32_t tile_base, ntiles;
+    uint32_t model;       /* learned model slot or 0xffffffff */
+} excl_list_info;
+
+typedef struct {
+    uint32_t nlists;
+    uint64_t nsegs, nwords, ndir, ntilemap, postings;
+    uint64_t device_bytes; /* bytes the resident image takes in HBM */
+} excl_index_sizes;
+
+int excl_index_sizes_get(const excl_index *ix, excl_index_sizes *s);
+int excl_index_export(const excl_index *ix, excl_list_info *lists, uint32_t *words, uint32_t *seg_head,
+                      uint32_t *seg_rec /* 4 u32 per segment */, uint32_t *seg_reg /* 4 u32 per segment */,
+                      uint32_t *dir);
+
+/* ---------------------------------------------------------------------------
+ * Context and device residency. One context per device; its own streams. */
+typedef struct excl_ctx excl_ctx;
+
+typedef struct {
+    uint32_t max_queries;    /* per batch (reference: 16380-word constant image, ParaPFD_Intersection_kernel.cu:134) */
+    uint32_t max_terms;      /* per query, <= 32 (reference MAX_QUERY_LEN 80, of which 8 are used by the workloads) */
+    uint64_t max_keys;       /* per batch, sum of shortest-list lengths (reference baseSize) */
+    uint32_t warps_per_cta;  /* probe kernel launch shape (0 = autotuned/default) */
+    uint32_t ctas_per_sm;
+} excl_ctx_config;
+
+int excl_ctx_create(int device, const excl_ctx_config *cfg, excl_ctx **out);
+int excl_ctx_destroy(excl_ctx *ctx);
+const char *excl_last_error(const excl_ctx *ctx);
+void *excl_ctx_stream(excl_ctx *ctx); /* the cudaStream_t all of this context's work runs on */
+
+/* Uploads the index image once; it stays resident (reference: allocateResource,
+ * ParaPFD_Intersection.cu:76-123, copies the whole .ind2 once). The caller may
+ * free its host arrays afterwards; the library owns the device copies. */
+int excl_index_upload(excl_ctx *ctx, excl_index *ix);
+
+/* Decode lists [l0, l1) on the device into `d_out` (device pointer, list-major,
+ * concatenated). Replaces the X_Decompression kernels (ParaPFD_Decompression_kernel.cu:117-272,
+ * LRC_Decompression_kernel.cu:122-258, SegLRC_Decompression_kernel.cu:124-256,
+ * HS_SegLRC_Decompression_kernel.cu:139-). Asynchronous on the context stream. */
+int excl_decode_lists_device(excl_ctx *ctx, excl_index *ix, uint32_t l0, uint32_t l1, uint32_t *d_out);
+/* Host convenience: decode to a host buffer (synchronous). */
+int excl_decode_lists(excl_ctx *ctx, excl_index *ix, uint32_t l0, uint32_t l1, uint32_t *out, size_t cap);
+
+/* ---------------------------------------------------------------------------
+ * Batched conjunctive queries. Replaces the per-batch pipeline
+ * CPUPreprocess -> htodTransfer -> kernelInvoke -> dtohTransfer
+ * (ParaPFD_Intersection.cu:126-309; same skeleton in LRC/LRCSeg/SegLRC/HS).
+ * Query q's terms are terms[term_offsets[q] .. term_offsets[q+1]).
+ * Results: offsets[nq+1] (exclusive prefix of per-query counts) and the
+ * concatenated per-query docIDs, each query sorted ascending. The output is
+ * identical whatever the batching. */
+typedef struct excl_batch excl_batch;
+
+int excl_submit(excl_ctx *ctx, excl_index *ix, const uint32_t *terms, const uint32_t *term_offsets, uint32_t nq,
+                uint32_t algo, excl_batch **ticket);
+int excl_wait(excl_batch *ticket, uint32_t *offsets, uint32_t *docids, size_t cap, int timeout_ms, uint64_t *total);
+int excl_batch_free(excl_batch *ticket);
+
+/* All-device variant: queries and outputs already in device memory; no host
+ * synchronisation. d_offsets has nq+1 entries; d_docids capacity `cap`.
+ * Writes the total to d_offsets[nq]; a total above cap raises EXCL_E_CAPACITY
+ * on the next excl_ctx_check. */
+int excl_intersect_device(excl_ctx *ctx, excl_index *ix, const uint32_t *d_terms, const uint32_t *d_term_offsets,
+                          uint32_t nq, uint32_t algo, uint32_t *d_offsets, uint32_t *d_docids, uint64_t cap);
+/* Synchronises the context stream and reports device-side error flags. */
+int excl_ctx_check(excl_ctx *ctx);
+
+/* Per-kernel timing of the last excl_intersect_device / excl_wait (ms, CUDA events). */
+typedef struct {
+    float pack_ms, probe_ms, compact_ms, total_ms;
+    uint64_t tiles;     /* (query, tile) work items */
+    uint64_t keys;      /* shortest-list docIDs decoded */
+    uint64_t probes;    /* (key, longer list) probes */
+    uint64_t fallbacks; /* learned probes that fell back to the directory search */
+} excl_batch_stats;
+int excl_last_stats(excl_ctx *ctx, excl_batch_stats *st);
+
+/* Checksum triple of the reference (ParaPFD_Intersection.cu:378-403): empty
+ * queries, total results, XOR of first/middle/last result per query. */
+int excl_checksum(uint32_t nq, const uint32_t *offsets, const uint32_t *docids, uint64_t cs[3]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EXCL_GPU_H_ */

@@ -1,0 +1,303 @@
+"""CPU ORACLE — test infrastructure only.
+
+ctypes wrapper of oracle/liboracle.so (oracle.c: a plain-C restatement of the
+reference's ParaPFD codec, list formats, regression arithmetic, hash-segment
+partition, exact intersection and checksum), and of the reference's own code
+compiled from its sources into oracle/_ref/ (ParaPFor.cpp; the generators'
+getRegressionInfo). Only tests/, __graft_entry__.smoke() and bench.py's CPU
+baseline legs use this package, and only as the checker.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+REF_CODEC = os.path.join(HERE, "_ref", "libparapfor_ref.so")
+REF_FIT = os.path.join(HERE, "_ref", "libfit_ref.so")
+
+
+def build(ref: bool | None = None) -> None:
+    """make -C oracle (and the reference builds when the reference tree exists)."""
+    subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
+    if ref is None:
+        ref = os.path.isdir("/root/reference/src/gpu")
+    if ref:
+        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+
+
+if not os.path.exists(LIB):
+    build(ref=False)
+_lib = C.CDLL(LIB)
+
+u32p = C.POINTER(C.c_uint32)
+i32p = C.POINTER(C.c_int32)
+u64p = C.POINTER(C.c_uint64)
+
+
+def _f(lib, name, res, *args):
+    fn = getattr(lib, name)
+    fn.restype = res
+    fn.argtypes = list(args)
+    return fn
+
+
+_enc_block = _f(_lib, "or_parapfd_encode_block", C.c_uint32, u32p, C.c_uint32, C.c_float, u32p, C.POINTER(C.c_int))
+_dec_block = _f(_lib, "or_parapfd_decode_block", C.c_uint32, u32p, C.c_uint32, u32p)
+_fit_seg = _f(_lib, "or_fit_seg", None, u32p, C.c_uint32, C.POINTER(C.c_float), C.POINTER(C.c_float), u32p, u32p)
+_fit_lrc = _f(_lib, "or_fit_lrc", None, u32p, C.c_uint32, C.POINTER(C.c_float), i32p, C.POINTER(C.c_float))
+_enc_pfd = _f(_lib, "or_encode_parapfd_list", C.c_int64, u32p, C.c_uint32, C.c_uint32, C.c_float, u32p, u32p, u32p,
+              u32p)
+_enc_pfd_segs = _f(_lib, "or_encode_parapfd_segs", C.c_int64, u32p, C.c_uint32, C.c_uint32, u32p, C.c_float, u32p,
+                   u32p, u32p, u32p)
+_enc_res = _f(_lib, "or_encode_residual_list", C.c_int64, C.c_int, u32p, C.c_uint32, C.c_uint32, u32p, C.c_float,
+              u32p, u32p, u32p, u32p, i32p, u32p)
+_hs = _f(_lib, "or_hs_partition", C.c_uint32, u32p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, u32p, u32p)
+_dec_list = _f(_lib, "or_decode_list", C.c_int, C.c_int, u32p, C.c_uint32, C.c_uint32, u32p, u32p, u32p, u32p, i32p,
+               u32p, u32p)
+_isect = _f(_lib, "or_intersect", C.c_uint64, C.c_uint32, C.POINTER(u32p), u64p, u32p)
+_cs = _f(_lib, "or_checksum", None, C.c_uint32, u64p, u32p, u64p)
+_runq = _f(_lib, "or_run_queries", C.c_double, u32p, u64p, u32p, u64p, C.c_uint32, C.c_uint32, C.c_uint64, u64p)
+
+
+def _u32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.uint32)
+
+
+def _p(a: np.ndarray, t=u32p):
+    return a.ctypes.data_as(t)
+
+
+def encode_block(values, frac: float = 0.0) -> np.ndarray:
+    v = _u32(values)
+    out = np.zeros(3 * len(v) + 8, dtype=np.uint32)
+    err = C.c_int(0)
+    w = _enc_block(_p(v), len(v), frac, _p(out), C.byref(err))
+    if err.value:
+        raise ValueError("block not representable in ParaPFD")
+    return out[:w].copy()
+
+
+def decode_block(words, n: int) -> tuple[np.ndarray, int]:
+    w = np.zeros(len(words) + 4, dtype=np.uint32)
+    w[: len(words)] = words
+    out = np.zeros(max(n, 1), dtype=np.uint32)
+    used = _dec_block(_p(w), n, _p(out))
+    return out[:n], int(used)
+
+
+def fit_seg(y) -> tuple[float, float, int, int]:
+    y = _u32(y)
+    a, b = C.c_float(), C.c_float()
+    L, R = C.c_uint32(), C.c_uint32()
+    _fit_seg(_p(y), len(y), C.byref(a), C.byref(b), C.byref(L), C.byref(R))
+    return a.value, b.value, L.value, R.value
+
+
+def fit_seg_raw(y) -> np.ndarray:
+    a, b, L, R = fit_seg(y)
+    return np.array([np.float32(a).view(np.uint32), np.float32(b).view(np.uint32), L, R], dtype=np.uint32)
+
+
+def fit_lrc_raw(y) -> np.ndarray:
+    y = _u32(y)
+    s, r = C.c_float(), C.c_float()
+    i = C.c_int32()
+    _fit_lrc(_p(y), len(y), C.byref(s), C.byref(i), C.byref(r))
+    return np.array([np.float32(s.value).view(np.uint32), np.int32(i.value).view(np.uint32),
+                     np.float32(r.value).view(np.uint32)], dtype=np.uint32)
+
+
+def hs_partition(docs, bucket: int = 256, kbits: int = 0, ubits: int = 32) -> tuple[int, np.ndarray]:
+    d = _u32(docs)
+    nb_max = (int(d[-1]) >> max(0, ubits - kbits)) + 2 if kbits else len(d) * 2 + 4
+    bnd = np.zeros(nb_max + 2, dtype=np.uint32)
+    sh = C.c_uint32()
+    nb = _hs(_p(d), len(d), bucket, kbits, ubits, C.byref(sh), _p(bnd))
+    return int(sh.value), bnd[: nb + 1].copy()
+
+
+CODECS = {"parapfd": 0, "lrc": 1, "lrcseg": 2, "seglrc": 3, "hs_seglrc": 4, "hs_parapfd": 5}
+
+
+def segment_starts(docs, codec: int, block: int, bucket: int = 256, kbits: int = 0, ubits: int = 32):
+    """Segment start elements of a list, as the formats cut it: fixed blocks, or
+    the non-empty buckets (HS_SegLRC) / blocks inside buckets (HS_ParaPFD).
+    Returns (starts, shift, bucket->first segment table or None)."""
+    n = len(docs)
+    if codec not in (4, 5):
+        return np.arange(0, n, block, dtype=np.uint32), None, None
+    shift, bnd = hs_partition(docs, bucket, kbits, ubits)
+    starts, first = [], []
+    for b in range(len(bnd) - 1):
+        first.append(len(starts))
+        lo, hi = int(bnd[b]), int(bnd[b + 1])
+        step = block if codec == 5 else max(hi - lo, 1)
+        for k in range(lo, hi, step):
+            starts.append(k)
+    first.append(len(starts))
+    return np.array(starts, dtype=np.uint32), shift, np.array(first, dtype=np.uint32)
+
+
+def encode_list(docs, codec: int, block: int = 256, frac: float = 0.0, bucket: int = 256, kbits: int = 0,
+                ubits: int = 32) -> dict:
+    """Oracle encoding of one list in the given codec: blocks and metadata."""
+    d = _u32(docs)
+    n = len(d)
+    starts, shift, first = segment_starts(d, codec, block, bucket, kbits, ubits)
+    ns = len(starts)
+    words = np.zeros(3 * n + 8 * ns + 8, dtype=np.uint32)
+    off = np.zeros(ns, dtype=np.uint32)
+    head = np.zeros(ns, dtype=np.uint32)
+    aux = np.zeros(ns, dtype=np.uint32)
+    reg = np.zeros((ns, 4), dtype=np.uint32)
+    base = np.zeros(ns, dtype=np.int32)
+    listreg = np.zeros(4, dtype=np.uint32)
+    if codec in (0, 5):
+        if codec == 0:
+            w = _enc_pfd(_p(d), n, block, frac, _p(words), _p(off), _p(head), _p(aux))
+        else:
+            w = _enc_pfd_segs(_p(d), n, ns, _p(starts), frac, _p(words), _p(off), _p(head), _p(aux))
+    else:
+        ocodec = 4 if codec == 4 else codec
+        w = _enc_res(ocodec, _p(d), n, ns, _p(starts), frac, _p(words), _p(off), _p(head), _p(reg),
+                     _p(base, i32p), _p(listreg))
+        aux = base.view(np.uint32)
+    if w < 0:
+        raise ValueError("list not representable in this format")
+    counts = np.diff(np.append(starts, n)).astype(np.uint32)
+    return dict(words=words[:w].copy(), off=off, head=head, aux=aux, reg=reg, listreg=listreg, starts=starts,
+                counts=counts, shift=shift, first=first)
+
+
+def decode_list(enc: dict, codec: int, n: int) -> np.ndarray:
+    words = np.zeros(len(enc["words"]) + 8, dtype=np.uint32)
+    words[: len(enc["words"])] = enc["words"]
+    out = np.zeros(max(n, 1), dtype=np.uint32)
+    ocodec = {0: 0, 5: 0, 1: 1, 2: 2, 3: 3, 4: 3}[codec]
+    reg = np.ascontiguousarray(enc["reg"].reshape(-1), dtype=np.uint32)
+    base = np.ascontiguousarray(enc["aux"]).view(np.int32)
+    _dec_list(ocodec, _p(words), n, len(enc["starts"]), _p(_u32(enc["starts"])), _p(_u32(enc["off"])),
+              _p(_u32(enc["head"])), _p(reg), _p(np.ascontiguousarray(base), i32p), _p(_u32(enc["listreg"])),
+              _p(out))
+    return out[:n]
+
+
+def intersect(lists) -> np.ndarray:
+    arrs = [_u32(a) for a in lists]
+    if not arrs:
+        return np.zeros(0, dtype=np.uint32)
+    ptrs = (u32p * len(arrs))(*[_p(a) if len(a) else _p(np.zeros(1, np.uint32)) for a in arrs])
+    lens = np.array([len(a) for a in arrs], dtype=np.uint64)
+    out = np.zeros(max(1, min(len(a) for a in arrs)), dtype=np.uint32)
+    r = _isect(len(arrs), ptrs, _p(lens, u64p), _p(out))
+    return out[:r].copy()
+
+
+def run_queries(docs, list_offsets, terms, term_offsets, threads: int = 1) -> tuple[float, np.ndarray]:
+    """Exact AND of every query on `threads` host threads; (seconds, counts)."""
+    d = _u32(docs)
+    lo = np.ascontiguousarray(list_offsets, dtype=np.uint64)
+    t = _u32(terms) if len(terms) else np.zeros(1, np.uint32)
+    to = np.ascontiguousarray(term_offsets, dtype=np.uint64)
+    nq = len(to) - 1
+    counts = np.zeros(max(nq, 1), dtype=np.uint64)
+    maxl = int(np.diff(lo).max()) if len(lo) > 1 else 1
+    secs = _runq(_p(d), _p(lo, u64p), _p(t), _p(to, u64p), nq, threads, maxl, _p(counts, u64p))
+    return float(secs), counts[:nq]
+
+
+def answer(docs, list_offsets, terms, term_offsets) -> tuple[np.ndarray, np.ndarray]:
+    """Expected (offsets[nq+1], docids) of a batch."""
+    lo = np.asarray(list_offsets, dtype=np.uint64)
+    to = np.asarray(term_offsets, dtype=np.uint64)
+    res, offs = [], [0]
+    for q in range(len(to) - 1):
+        ts = terms[int(to[q]):int(to[q + 1])]
+        if len(ts) == 0:
+            r = np.zeros(0, dtype=np.uint32)
+        else:
+            r = intersect([docs[int(lo[t]):int(lo[t + 1])] for t in ts])
+        res.append(r)
+        offs.append(offs[-1] + len(r))
+    return np.array(offs, dtype=np.uint64), (np.concatenate(res) if res else np.zeros(0, np.uint32))
+
+
+def checksum(offsets, docids) -> tuple[int, int, int]:
+    o = np.ascontiguousarray(offsets, dtype=np.uint64)
+    d = _u32(docids) if len(docids) else np.zeros(1, np.uint32)
+    cs = np.zeros(3, dtype=np.uint64)
+    _cs(len(o) - 1, _p(o, u64p), _p(d), _p(cs, u64p))
+    return int(cs[0]), int(cs[1]), int(cs[2])
+
+
+# ---------------------------------------------------------------------------
+# The reference's own code (built from its sources; absent off this machine
+# unless oracle/_ref travelled with the tree).
+
+def have_ref_codec() -> bool:
+    return os.path.exists(REF_CODEC)
+
+
+def have_ref_fit() -> bool:
+    return os.path.exists(REF_FIT)
+
+
+_ref_codec = None
+_ref_fit = None
+
+
+def _rc():
+    global _ref_codec
+    if _ref_codec is None:
+        lib = C.CDLL(REF_CODEC)
+        _f(lib, "ref_set_frac", None, C.c_float)
+        _f(lib, "ref_encode", C.c_uint32, u32p, u32p, C.c_uint32)
+        _f(lib, "ref_decode", C.c_uint32, u32p, u32p, C.c_uint32)
+        _ref_codec = lib
+    return _ref_codec
+
+
+def ref_encode(values, frac: float) -> np.ndarray:
+    v = _u32(values)
+    out = np.zeros(3 * len(v) + 16, dtype=np.uint32)
+    lib = _rc()
+    lib.ref_set_frac(frac)
+    w = lib.ref_encode(_p(v), _p(out), len(v))
+    return out[:w].copy()
+
+
+def ref_decode(words, n: int) -> tuple[np.ndarray, int]:
+    w = np.zeros(len(words) + 4, dtype=np.uint32)
+    w[: len(words)] = words
+    out = np.zeros(max(n, 1) + 2, dtype=np.uint32)
+    used = _rc().ref_decode(_p(w), _p(out), n)
+    return out[:n].copy(), int(used)
+
+
+def _rf():
+    global _ref_fit
+    if _ref_fit is None:
+        lib = C.CDLL(REF_FIT)
+        _f(lib, "ref_fit_seglrc", None, u32p, C.c_uint32, u32p)
+        _f(lib, "ref_fit_lrc", None, u32p, C.c_uint32, u32p)
+        _ref_fit = lib
+    return _ref_fit
+
+
+def ref_fit_seg_raw(y) -> np.ndarray:
+    y = _u32(y)
+    out = np.zeros(4, dtype=np.uint32)
+    _rf().ref_fit_seglrc(_p(y), len(y), _p(out))
+    return out
+
+
+def ref_fit_lrc_raw(y) -> np.ndarray:
+    y = _u32(y)
+    out = np.zeros(3, dtype=np.uint32)
+    _rf().ref_fit_lrc(_p(y), len(y), _p(out))
+    return out

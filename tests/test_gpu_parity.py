@@ -1,0 +1,115 @@
+"""GPU parity: device decode and batched AND intersection of every format and
+search method against the CPU oracle, bit for bit, through the C ABI."""
+import numpy as np
+import pytest
+
+import exclucene_b200 as ex
+import oracle
+from exclucene_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+FORMATS = ["parapfd", "lrc", "lrcseg", "seglrc", "hs_seglrc", "hs_parapfd"]
+ALGOS = ["bsearch", "hashseg", "auto"]
+
+
+def _index(w, codec, block=256, frac=0.0, ubits=24):
+    kb = 10 if codec == "hs_parapfd" else 0
+    return ex.Index(w.docs, w.list_offsets, codec=codec, block=block, frac=frac, hs_bucket=256, hs_kbits=kb,
+                    hs_ubits=ubits)
+
+
+@pytest.fixture(scope="module")
+def corpus():
+    # Zipf-frequency corpus in the shape of the multi-term workload, scaled down
+    return synth.zipf_corpus(seed=77, ndocs=1 << 20, nterms=3000, cap=200_000, nq=3000, qmin=1, qmax=6)
+
+
+@pytest.fixture(scope="module")
+def expected(corpus):
+    return oracle.answer(corpus.docs, corpus.list_offsets, corpus.terms, corpus.term_offsets)
+
+
+@pytest.mark.parametrize("codec", FORMATS)
+@pytest.mark.parametrize("block,frac", [(256, 0.0), (128, 0.1)])
+def test_decode_matches_source_lists(gpu_ctx, corpus, codec, block, frac):
+    ix = _index(corpus, codec, block, frac)
+    gpu_ctx.upload(ix)
+    got = gpu_ctx.decode_lists(ix)
+    assert np.array_equal(got, corpus.docs)
+    # a sub-range of lists
+    l0, l1 = 17, 401
+    got = gpu_ctx.decode_lists(ix, l0, l1)
+    assert np.array_equal(got, corpus.docs[corpus.list_offsets[l0]:corpus.list_offsets[l1]])
+    ix.close()
+
+
+@pytest.mark.parametrize("codec", FORMATS)
+@pytest.mark.parametrize("algo", ALGOS)
+def test_intersection_matches_oracle(gpu_ctx, corpus, expected, codec, algo):
+    ix = _index(corpus, codec, 128 if codec == "parapfd" else 256, 0.1 if codec == "parapfd" else 0.0)
+    gpu_ctx.upload(ix)
+    offs, docs = gpu_ctx.intersect(ix, corpus.terms, corpus.term_offsets, algo=algo)
+    eoffs, edocs = expected
+    assert np.array_equal(offs.astype(np.uint64), eoffs)
+    assert np.array_equal(docs, edocs)
+    assert ex.checksum(offs, docs) == oracle.checksum(eoffs, edocs)
+    ix.close()
+
+
+def test_edge_case_queries(gpu_ctx):
+    lists = [np.array([5], np.uint32),                               # 0 single posting
+             np.arange(0, 3000, 3, dtype=np.uint32),                   # 1
+             np.arange(1, 3000, 3, dtype=np.uint32),                   # 2 disjoint from 1
+             np.arange(0, 600000, 2, dtype=np.uint32),                 # 3 long
+             np.array([0, 4294967295 - 7], np.uint32),                 # 4 extremes
+             np.arange(2 ** 31 - 1000, 2 ** 31 + 1000, 7, dtype=np.uint32),  # 5 around 2^31
+             np.arange(0, 256, dtype=np.uint32),                       # 6 exactly one block
+             np.arange(0, 257, dtype=np.uint32)]                       # 7 one block + 1
+    docs = np.concatenate(lists)
+    loff = np.concatenate([[0], np.cumsum([len(x) for x in lists])]).astype(np.uint64)
+    queries = [[], [0], [1], [1, 2], [1, 3], [3, 1], [3, 3], [0, 3, 1], [4, 4], [4, 3], [5], [5, 5, 5],
+               [6, 7], [7, 6, 1, 3], list(range(8)), [3] * 32, [1, 3, 6, 7, 3, 1]]
+    terms = np.array([t for q in queries for t in q], np.uint32)
+    toff = np.concatenate([[0], np.cumsum([len(q) for q in queries])]).astype(np.uint32)
+    eoffs, edocs = oracle.answer(docs, loff, terms, toff)
+    for codec in FORMATS:
+        if codec == "lrc":
+            continue  # docIDs near 2^32 are beyond LRC's int arithmetic
+        ix = ex.Index(docs, loff, codec=codec, block=256, hs_bucket=64, hs_kbits=12 if codec == "hs_parapfd" else 0,
+                      hs_ubits=32)
+        gpu_ctx.upload(ix)
+        for algo in ALGOS:
+            offs, got = gpu_ctx.intersect(ix, terms, toff, algo=algo)
+            assert np.array_equal(offs.astype(np.uint64), eoffs), (codec, algo)
+            assert np.array_equal(got, edocs), (codec, algo)
+        ix.close()
+
+
+def test_invalid_batches_raise(gpu_ctx, corpus):
+    ix = _index(corpus, "parapfd")
+    gpu_ctx.upload(ix)
+    with pytest.raises(ex.ExclError):
+        gpu_ctx.intersect(ix, np.array([corpus.nlists + 5], np.uint32), np.array([0, 1], np.uint32))
+    with pytest.raises(ex.ExclError):
+        gpu_ctx.intersect(ix, np.zeros(33, np.uint32), np.array([0, 33], np.uint32))
+    # the context stays usable
+    offs, docs = gpu_ctx.intersect(ix, corpus.terms[:10], corpus.term_offsets[:4] - corpus.term_offsets[0])
+    eo, ed = oracle.answer(corpus.docs, corpus.list_offsets, corpus.terms[:10], corpus.term_offsets[:4])
+    assert np.array_equal(docs, ed)
+    ix.close()
+
+
+def test_batching_does_not_change_results(gpu_ctx, corpus, expected):
+    ix = _index(corpus, "seglrc")
+    gpu_ctx.upload(ix)
+    eoffs, edocs = expected
+    toff = corpus.term_offsets
+    for q0, q1 in [(0, 1), (5, 6), (100, 357), (1000, 3000)]:
+        t = corpus.terms[toff[q0]:toff[q1]]
+        o = (toff[q0:q1 + 1] - toff[q0]).astype(np.uint32)
+        offs, docs = gpu_ctx.intersect(ix, t, o)
+        exp = edocs[eoffs[q0]:eoffs[q1]]
+        assert np.array_equal(docs, exp)
+        assert np.array_equal(offs.astype(np.uint64), eoffs[q0:q1 + 1] - eoffs[q0])
+    ix.close()
