@@ -425,8 +425,22 @@ static void build_list(const uint32_t *docs, uint32_t n, uint32_t codec, const e
     if (d.log2_block) {
         d.ntiles = ns;
     } else {
-        for (uint32_t s = 0; s < ns; ++s)
-            for (uint32_t k = 0; k < cnt[s]; k += kTileKeys) o.tiles.push_back(((uint64_t)s << 32) | k);
+        // Variable segments: a segment larger than a tile is cut into 256-slices;
+        // consecutive small segments are grouped while they fit in one tile.
+        uint32_t s = 0;
+        while (s < ns) {
+            if (cnt[s] >= kTileKeys) {
+                if (cnt[s] > kTileMaxE0) return fail(o, EXCL_E_FORMAT, "hash bucket larger than 2^24 postings");
+                for (uint32_t k = 0; k < cnt[s]; k += kTileKeys) o.tiles.push_back(tile_pack(s, k, 1));
+                ++s;
+                continue;
+            }
+            uint32_t keys = 0, g = 0;
+            while (s + g < ns && g < kTileMaxSegs && cnt[s + g] < kTileKeys && keys + cnt[s + g] <= kTileKeys)
+                keys += cnt[s + g++];
+            o.tiles.push_back(tile_pack(s, 0, g));
+            s += g;
+        }
         d.ntiles = (uint32_t)o.tiles.size();
     }
 }
@@ -437,8 +451,8 @@ int build_index(const uint32_t *docs, const uint64_t *loff, uint32_t nlists, con
         err = "null input or no lists";
         return EXCL_E_INVALID;
     }
-    if (p.block == 0 || p.block > kTileKeys || (p.block & (p.block - 1))) {
-        err = "block must be a power of two <= 256";
+    if (p.block < kMinBlock || p.block > kTileKeys || (p.block & (p.block - 1))) {
+        err = "block must be a power of two in [32, 256]";
         return EXCL_E_INVALID;
     }
     for (uint32_t l = 0; l < nlists; ++l) {

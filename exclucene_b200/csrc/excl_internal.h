@@ -14,6 +14,15 @@ constexpr uint32_t kNoModel = 0xffffffffu;
 constexpr uint32_t kMaxTerms = 32;    // terms per query on the device
 constexpr uint32_t kTileKeys = 256;   // keys per tile (one shortest-list segment or a 256-slice of an HS bucket)
 constexpr uint32_t kWordPad = 8;      // zero words after the last block: 64/128-bit window reads stay in bounds
+constexpr uint32_t kMinBlock = 32;    // smallest fixed block (bounds tiles per key for buffer sizing)
+
+// Tile map entry of a variable-segment (HS) list: first segment of the tile
+// (within the list), first element within that segment, number of segments.
+constexpr uint32_t kTileMaxE0 = (1u << 24) - 1;
+constexpr uint32_t kTileMaxSegs = 255;
+inline constexpr uint64_t tile_pack(uint32_t seg, uint32_t e0, uint32_t nseg) {
+    return ((uint64_t)seg << 32) | ((uint64_t)e0 << 8) | nseg;
+}
 
 // Device-resident description of one posting list (80 bytes, 16-byte aligned
 // so a warp reads it with 128-bit loads).

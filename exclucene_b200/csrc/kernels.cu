@@ -66,8 +66,8 @@ __global__ void __launch_bounds__(kDecodeWarps * 32) k_decode_lists(DevIndexView
 
 __global__ void k_pack(const ListDesc *__restrict__ lists, uint32_t nlists, const uint32_t *__restrict__ terms,
                        const uint32_t *__restrict__ toff, uint32_t nq, uint32_t *__restrict__ qterms,
-                       uint32_t *__restrict__ qnterms, uint32_t *__restrict__ ntiles, uint32_t *__restrict__ tile_counter,
-                       uint32_t *__restrict__ err) {
+                       uint32_t *__restrict__ qnterms, uint32_t *__restrict__ ntiles, uint32_t *__restrict__ nkeys,
+                       uint32_t *__restrict__ tile_counter, uint32_t *__restrict__ err) {
     const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q == 0) *tile_counter = 0u;
     if (q >= nq) return;
@@ -103,6 +103,7 @@ __global__ void k_pack(const ListDesc *__restrict__ lists, uint32_t nlists, cons
     for (uint32_t i = 0; i < k; ++i) dst[i] = id[i];
     qnterms[q] = k;
     ntiles[q] = k ? lists[id[0]].ntiles : 0u;
+    nkeys[q] = k ? len[0] : 0u;
 }
 
 // ---------------------------------------------------------------------------
@@ -340,18 +341,25 @@ __global__ void __launch_bounds__(WARPS * 32) k_probe(DevIndexView ix, BatchView
         __syncwarp();
         if (lane < 5) reinterpret_cast<uint4 *>(&L)[lane] = reinterpret_cast<const uint4 *>(ix.lists + qt[0])[lane];
         __syncwarp();
-        uint32_t sg, e0, kc;
+        // decode the tile's keys: one fixed segment, or 1..255 consecutive
+        // variable segments / one 256-slice of a large segment
+        uint32_t kc = 0, first_elem;
         if (L.log2_block) {
-            sg = L.seg_base + ti;
-            e0 = 0;
+            const uint32_t sg = L.seg_base + ti;
             kc = ix.seg_rec[sg].count;
+            first_elem = ti << L.log2_block;
+            warp_decode(ix, L, sg, 0, kc, keys, lane);
         } else {
             const uint64_t tm = ix.tilemap[L.tile_base + ti];
-            sg = L.seg_base + (uint32_t)(tm >> 32);
-            e0 = (uint32_t)tm;
-            kc = min(kTileKeys, ix.seg_rec[sg].count - e0);
+            const uint32_t sg0 = L.seg_base + (uint32_t)(tm >> 32);
+            const uint32_t e0 = (uint32_t)(tm >> 8) & kTileMaxE0, ns = (uint32_t)tm & 0xffu;
+            first_elem = ix.seg_rec[sg0].start + e0;
+            for (uint32_t g = 0; g < ns; ++g) {
+                const uint32_t c = min(kTileKeys - kc, ix.seg_rec[sg0 + g].count - (g ? 0u : e0));
+                warp_decode(ix, L, sg0 + g, g ? 0u : e0, c, keys + kc, lane);
+                kc += c;
+            }
         }
-        warp_decode(ix, L, sg, e0, kc, keys, lane);
         nkeys += kc;
         uint32_t alive = kc;
         for (uint32_t j = 1; j < k && alive; ++j) {
@@ -374,9 +382,19 @@ __global__ void __launch_bounds__(WARPS * 32) k_probe(DevIndexView ix, BatchView
             __syncwarp();
             alive = nout;
         }
-        uint32_t *dst = b.scratch + (size_t)t * kTileKeys;
+        // survivors go to the tile's key-indexed slot (its keys' positions in
+        // the batch's concatenated shortest lists)
+        const uint64_t slot = (uint64_t)b.key_base[q] + first_elem;
+        if (slot + kc > b.max_keys) {
+            if (lane == 0) atomicOr(b.err, kErrCapacity);
+            alive = 0;
+        }
+        uint32_t *dst = b.scratch + slot;
         for (uint32_t i = lane; i < alive; i += 32) dst[i] = keys[i];
-        if (lane == 0) b.tile_count[t] = alive;
+        if (lane == 0) {
+            b.tile_count[t] = alive;
+            b.tile_slot[t] = (uint32_t)slot;
+        }
         __syncwarp();
     }
     if (b.stats) {
@@ -407,7 +425,7 @@ __global__ void k_scatter(BatchView b, const uint32_t *__restrict__ tile_out, ui
     for (uint32_t t = gw; t < T; t += nw) {
         const uint32_t c = b.tile_count[t];
         const uint64_t o = tile_out[t];
-        const uint32_t *src = b.scratch + (size_t)t * kTileKeys;
+        const uint32_t *src = b.scratch + b.tile_slot[t];
         for (uint32_t i = lane; i < c; i += 32)
             if (o + i < cap) docids[o + i] = src[i];
     }
@@ -431,10 +449,10 @@ int launch_decode(const DevIndexView &ix, uint32_t l0, uint32_t l1, uint64_t out
 }
 
 int launch_pack(const ListDesc *lists, uint32_t nlists, const uint32_t *terms, const uint32_t *toff, uint32_t nq,
-                const BatchView &b, uint32_t *ntiles, cudaStream_t st) {
+                const BatchView &b, uint32_t *ntiles, uint32_t *nkeys, cudaStream_t st) {
     const uint32_t blocks = std::max(1u, (nq + 127) / 128);
     k_pack<<<blocks, 128, 0, st>>>(lists, nlists, terms, toff, nq, const_cast<uint32_t *>(b.qterms),
-                                    const_cast<uint32_t *>(b.qnterms), ntiles, b.tile_counter, b.err);
+                                    const_cast<uint32_t *>(b.qnterms), ntiles, nkeys, b.tile_counter, b.err);
     return (int)cudaGetLastError();
 }
 

@@ -14,9 +14,12 @@ struct BatchView {
     const uint32_t *qnterms;     // terms per query
     const uint32_t *tile_prefix; // nq + 1, exclusive prefix of tiles per query
     uint32_t *tile_counter;      // work-queue head (zeroed by k_pack)
+    const uint32_t *key_base;    // nq + 1, exclusive prefix of shortest-list lengths
     uint32_t *tile_count;        // survivors per tile
-    uint32_t *scratch;           // max_tiles * kTileKeys survivor slots
+    uint32_t *tile_slot;         // scratch position of each tile's survivors
+    uint32_t *scratch;           // max_keys survivor slots, indexed by key position
     uint32_t max_tiles;
+    uint64_t max_keys;
     uint32_t *err;               // error flag bits
     uint64_t *stats;             // [probes, fallbacks] or null
 };
@@ -24,7 +27,7 @@ struct BatchView {
 int launch_decode(const DevIndexView &ix, uint32_t l0, uint32_t l1, uint64_t out_base0, uint32_t *out, uint32_t seg0,
                   uint32_t nsegs, int nsm, cudaStream_t st);
 int launch_pack(const ListDesc *lists, uint32_t nlists, const uint32_t *terms, const uint32_t *toff, uint32_t nq,
-                const BatchView &b, uint32_t *ntiles, cudaStream_t st);
+                const BatchView &b, uint32_t *ntiles, uint32_t *nkeys, cudaStream_t st);
 uint32_t scan_blocks_for(uint64_t n);
 int launch_scan(const uint32_t *in, uint32_t *out, const uint32_t *n_dev, uint32_t n_host, uint64_t max_n,
                 uint64_t *state, uint32_t *ticket, uint32_t *err, cudaStream_t st);

@@ -184,23 +184,28 @@ DevIndexView DeviceIndex::view(const ModelView &mv) const {
 
 int ctx_alloc_batch(excl_ctx *ctx) {
     const excl_ctx_config &c = ctx->cfg;
-    ctx->max_tiles = (uint32_t)std::min<uint64_t>(0xffffffffull, c.max_keys / kTileKeys + c.max_queries + 1);
+    // Tiles hold >= kMinBlock keys except where consecutive HS segments are
+    // grouped (>= 128 keys on average) or a list ends, so this bounds them.
+    ctx->max_tiles = (uint32_t)std::min<uint64_t>(0xfffffff0ull, c.max_keys / kMinBlock + c.max_queries + 1);
     int st = 0;
     st |= dalloc(ctx, &ctx->d_terms, (size_t)c.max_queries * kMaxTerms, "alloc terms");
     st |= dalloc(ctx, &ctx->d_toff, (size_t)c.max_queries + 1, "alloc term offsets");
     st |= dalloc(ctx, &ctx->d_qterms, (size_t)c.max_queries * kMaxTerms, "alloc qterms");
     st |= dalloc(ctx, &ctx->d_qnterms, (size_t)c.max_queries, "alloc qnterms");
     st |= dalloc(ctx, &ctx->d_ntiles, (size_t)c.max_queries + 1, "alloc ntiles");
+    st |= dalloc(ctx, &ctx->d_nkeys, (size_t)c.max_queries + 1, "alloc nkeys");
     st |= dalloc(ctx, &ctx->d_tile_prefix, (size_t)c.max_queries + 2, "alloc tile prefix");
+    st |= dalloc(ctx, &ctx->d_key_base, (size_t)c.max_queries + 2, "alloc key base");
     st |= dalloc(ctx, &ctx->d_tile_count, (size_t)ctx->max_tiles + 1, "alloc tile count");
+    st |= dalloc(ctx, &ctx->d_tile_slot, (size_t)ctx->max_tiles + 1, "alloc tile slot");
     st |= dalloc(ctx, &ctx->d_tile_out, (size_t)ctx->max_tiles + 2, "alloc tile out");
-    st |= dalloc(ctx, &ctx->d_scratch, (size_t)ctx->max_tiles * kTileKeys, "alloc scratch");
+    st |= dalloc(ctx, &ctx->d_scratch, (size_t)c.max_keys, "alloc scratch");
     st |= dalloc(ctx, &ctx->d_misc, 16, "alloc misc");
     st |= dalloc(ctx, &ctx->d_stats, 4, "alloc stats");
     const uint32_t nsb = std::max(scan_blocks_for(c.max_queries + 1), scan_blocks_for(ctx->max_tiles + 1));
     st |= dalloc(ctx, &ctx->d_scan_state, nsb, "alloc scan state");
     st |= dalloc(ctx, &ctx->d_offsets, (size_t)c.max_queries + 1, "alloc offsets");
-    ctx->docids_cap = (uint64_t)ctx->max_tiles * kTileKeys;
+    ctx->docids_cap = c.max_keys;
     st |= dalloc(ctx, &ctx->d_docids, ctx->docids_cap, "alloc docids");
     st |= cuda_status(ctx, cudaMallocHost((void **)&ctx->h_terms, (size_t)c.max_queries * kMaxTerms * 4), "pinned");
     st |= cuda_status(ctx, cudaMallocHost((void **)&ctx->h_toff, ((size_t)c.max_queries + 1) * 4), "pinned");
@@ -233,17 +238,22 @@ int run_pipeline(excl_ctx *ctx, excl_index *ix, const uint32_t *d_terms, const u
     b.qnterms = ctx->d_qnterms;
     b.tile_prefix = ctx->d_tile_prefix;
     b.tile_counter = ctx->d_misc + kMiscTileCounter;
+    b.key_base = ctx->d_key_base;
     b.tile_count = ctx->d_tile_count;
+    b.tile_slot = ctx->d_tile_slot;
     b.scratch = ctx->d_scratch;
     b.max_tiles = ctx->max_tiles;
+    b.max_keys = ctx->cfg.max_keys;
     b.err = ctx->d_misc + kMiscErr;
     b.stats = ctx->collect_stats ? ctx->d_stats : nullptr;
     const DevIndexView ixv = ix->dev->view(ix->models ? model_view(ix->models) : ModelView{});
     if (ctx->collect_stats) cudaMemsetAsync(ctx->d_stats, 0, 3 * 8, st);
     cudaEventRecord(ctx->ev[0], st);
     int e = 0;
-    e |= launch_pack(ix->dev->lists, ix->nlists, d_terms, d_toff, nq, b, ctx->d_ntiles, st);
+    e |= launch_pack(ix->dev->lists, ix->nlists, d_terms, d_toff, nq, b, ctx->d_ntiles, ctx->d_nkeys, st);
     e |= launch_scan(ctx->d_ntiles, ctx->d_tile_prefix, nullptr, nq, ctx->cfg.max_queries, ctx->d_scan_state,
+                     ctx->d_misc + kMiscTicket0, b.err, st);
+    e |= launch_scan(ctx->d_nkeys, ctx->d_key_base, nullptr, nq, ctx->cfg.max_queries, ctx->d_scan_state,
                      ctx->d_misc + kMiscTicket0, b.err, st);
     cudaEventRecord(ctx->ev[1], st);
     e |= launch_probe(ixv, b, (int)algo, ctx->warps, ctx->ctas_per_sm, ctx->nsm, st);
@@ -309,6 +319,7 @@ extern "C" int excl_ctx_destroy(excl_ctx *ctx) {
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     uint32_t *bufs[] = {ctx->d_terms,      ctx->d_toff,     ctx->d_qterms, ctx->d_qnterms, ctx->d_ntiles,
                         ctx->d_tile_prefix, ctx->d_tile_count, ctx->d_tile_out, ctx->d_scratch, ctx->d_misc,
+                        ctx->d_nkeys,      ctx->d_key_base, ctx->d_tile_slot,
                         ctx->d_offsets,    ctx->d_docids};
     for (uint32_t *p : bufs) cudaFree(p);
     cudaFree(ctx->d_stats);

@@ -45,6 +45,7 @@ struct excl_ctx {
     uint32_t *d_terms = nullptr, *d_toff = nullptr;
     uint32_t *d_qterms = nullptr, *d_qnterms = nullptr, *d_ntiles = nullptr, *d_tile_prefix = nullptr;
     uint32_t *d_tile_count = nullptr, *d_tile_out = nullptr, *d_scratch = nullptr, *d_misc = nullptr;
+    uint32_t *d_nkeys = nullptr, *d_key_base = nullptr, *d_tile_slot = nullptr;
     uint64_t *d_stats = nullptr, *d_scan_state = nullptr;
     uint32_t *d_offsets = nullptr, *d_docids = nullptr;
     uint64_t docids_cap = 0;

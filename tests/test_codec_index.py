@@ -106,6 +106,14 @@ def test_index_build_uniform_wide_universe(cname, codec):
     _compare_index(w, cname, codec, 256, 0.0, 12 if codec == 5 else 0, 31)
 
 
+def test_index_rejects_unrepresentable_gap():
+    """A d-gap >= 2^31 needs b = 32, which the descriptor's 5-bit lb field cannot
+    hold (ParaPFor.cpp:107 stores lb << 26 and :122 reads it back modulo 32)."""
+    with pytest.raises(ex.ExclError) as e:
+        ex.Index(np.array([0, 2 ** 32 - 8], np.uint32), np.array([0, 2], np.uint64), codec="parapfd")
+    assert e.value.status == api.E_FORMAT
+
+
 def test_index_rejects_bad_input():
     docs = np.array([5, 3, 9], np.uint32)
     with pytest.raises(ex.ExclError):

@@ -62,7 +62,7 @@ def test_edge_case_queries(gpu_ctx):
              np.arange(0, 3000, 3, dtype=np.uint32),                   # 1
              np.arange(1, 3000, 3, dtype=np.uint32),                   # 2 disjoint from 1
              np.arange(0, 600000, 2, dtype=np.uint32),                 # 3 long
-             np.array([0, 4294967295 - 7], np.uint32),                 # 4 extremes
+             np.array([0, 2 ** 31 - 1, 2 ** 32 - 8], np.uint32),       # 4 extremes (gaps < 2^31)
              np.arange(2 ** 31 - 1000, 2 ** 31 + 1000, 7, dtype=np.uint32),  # 5 around 2^31
              np.arange(0, 256, dtype=np.uint32),                       # 6 exactly one block
              np.arange(0, 257, dtype=np.uint32)]                       # 7 one block + 1
