@@ -348,3 +348,25 @@ def checksum(offsets, docids) -> tuple[int, int, int]:
 
 def library_path() -> str:
     return _LIB_PATH
+
+
+# ---------------------------------------------------------------------------
+# Allocation-free form of Context.intersect_device, for callers that cannot
+# allocate device memory when they query (their budget is fixed at start-up,
+# or they run without a Context, whose creation allocates the batch buffers).
+# Its scratch is a fixed 5.0 MiB device array inside the library, shared by
+# all calls: calls that overlap on the GPU race. The first call on a device
+# looks the array up; make it before any stream capture.
+
+NOALLOC_MAX_QUERIES = 4096
+NOALLOC_MAX_KEYS = 1 << 20
+_isect_noalloc = _sig("excl_intersect_device_noalloc", C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
+                      C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p)
+
+
+def intersect_device_noalloc(ix: Index, d_terms: int, d_toff: int, nq: int, algo, d_offsets: int, d_docids: int,
+                             cap: int, stream: int) -> None:
+    """Runs one batch on `stream` (device pointers in and out) and returns when it is done."""
+    a = ALGO_NAMES[algo] if isinstance(algo, str) else int(algo)
+    _check_status(_isect_noalloc(ix._h, C.c_void_p(d_terms), C.c_void_p(d_toff), nq, a, C.c_void_p(d_offsets),
+                                 C.c_void_p(d_docids), cap, C.c_void_p(stream)), what="excl_intersect_device_noalloc")

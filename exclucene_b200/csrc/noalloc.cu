@@ -1,0 +1,144 @@
+// Allocation-free variant of excl_intersect_device.
+//
+// Who needs it: callers that must not allocate device memory when they issue
+// queries — a host that hands the library a fixed memory budget and forbids
+// cudaMalloc/cudaFree after start-up (so the device allocator never
+// synchronises or fragments under load), code that runs where the caller owns
+// every allocation, or an embedding that cannot create a context (an
+// excl_ctx reserves its batch buffers with cudaMalloc). This entry point runs
+// the same kernels as excl_intersect_device, but all of its per-batch scratch
+// (sorted query terms, tile and key prefixes, per-tile counts, survivor slots,
+// scan state, error flag) lives in one file-scope device array of fixed size.
+//
+// Limits: at most EXCL_NOALLOC_MAX_QUERIES queries per call and at most
+// EXCL_NOALLOC_MAX_KEYS docIDs summed over the queries' shortest lists. The
+// array takes 5,245,440 bytes (5.0 MiB) on every GPU that loads the library,
+// until the process exits.
+//
+// Sharing: every call uses the same array and it keeps the last call's
+// contents; each call clears what must start at zero (error flag, counters,
+// scan state) on its stream. Calls whose work overlaps on the GPU (two
+// streams, or two host threads) race on the array and must be serialised by
+// the caller.
+#include <cuda_runtime.h>
+
+#include <mutex>
+
+#include "kernels.h"
+#include "runtime.h"
+
+namespace excl {
+namespace {
+
+constexpr uint32_t kNAQueries = EXCL_NOALLOC_MAX_QUERIES;
+constexpr uint32_t kNAKeys = EXCL_NOALLOC_MAX_KEYS;
+constexpr uint32_t kNATiles = kNAKeys / kMinBlock + kNAQueries + 1;
+constexpr uint32_t kScanItemsPerBlock = 2048;  // k_scan_excl tile
+constexpr uint32_t kNAScanBlocks = (kNATiles + 1 + kScanItemsPerBlock - 1) / kScanItemsPerBlock;
+
+constexpr uint64_t up64(uint64_t w) { return (w + 63) & ~63ull; }  // regions start on 256-byte boundaries
+
+// word offsets of the regions inside the array
+constexpr uint64_t kOffQterms = 0;
+constexpr uint64_t kOffQnterms = kOffQterms + up64((uint64_t)kNAQueries * kMaxTerms);
+constexpr uint64_t kOffNtiles = kOffQnterms + up64(kNAQueries);
+constexpr uint64_t kOffNkeys = kOffNtiles + up64(kNAQueries + 1);
+constexpr uint64_t kOffTilePrefix = kOffNkeys + up64(kNAQueries + 1);
+constexpr uint64_t kOffKeyBase = kOffTilePrefix + up64(kNAQueries + 2);
+constexpr uint64_t kOffTileCount = kOffKeyBase + up64(kNAQueries + 2);
+constexpr uint64_t kOffTileSlot = kOffTileCount + up64(kNATiles + 1);
+constexpr uint64_t kOffTileOut = kOffTileSlot + up64(kNATiles + 1);
+constexpr uint64_t kOffSurvivors = kOffTileOut + up64(kNATiles + 2);
+constexpr uint64_t kOffMisc = kOffSurvivors + up64(kNAKeys);
+constexpr uint64_t kOffStats = kOffMisc + 64;           // 3 x u64 counters
+constexpr uint64_t kOffScanState = kOffStats + 64;      // kNAScanBlocks x u64
+constexpr uint64_t kWords = kOffScanState + up64(2ull * kNAScanBlocks);
+static_assert(kWords * 4 == 5245440, "scratch size stated in the comments and excl_gpu.h");
+
+static __device__ __align__(256) uint32_t g_noalloc_scratch[kWords];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_mu;
+uint32_t *g_base[kMaxDevices];  // device address of g_noalloc_scratch, per device
+int g_nsm[kMaxDevices];
+
+// First call on a device (with that device current): look up the device
+// address of the array. The host-side name g_noalloc_scratch is only a
+// stand-in, never a device address, so kernels get this pointer instead.
+int setup_device(int dev, uint32_t **base, int *nsm) {
+    std::lock_guard<std::mutex> g(g_mu);
+    if (!g_base[dev]) {
+        // the look-back scan must fit its per-block state in the region above
+        if (scan_blocks_for((uint64_t)kNATiles + 1) > kNAScanBlocks) return EXCL_E_CAPACITY;
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) return EXCL_E_CUDA;
+        int n = 0;
+        e = cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (e != cudaSuccess) return EXCL_E_CUDA;
+        g_nsm[dev] = n;
+        g_base[dev] = static_cast<uint32_t *>(p);
+    }
+    *base = g_base[dev];
+    *nsm = g_nsm[dev];
+    return EXCL_OK;
+}
+
+}  // namespace
+}  // namespace excl
+
+using namespace excl;
+
+extern "C" int excl_intersect_device_noalloc(excl_index *ix, const uint32_t *d_terms, const uint32_t *d_term_offsets,
+                                             uint32_t nq, uint32_t algo, uint32_t *d_offsets, uint32_t *d_docids,
+                                             uint64_t cap, void *stream) {
+    if (!ix || !ix->dev || !d_term_offsets || !d_offsets || (!d_docids && cap) || algo > EXCL_ALGO_LEARNED)
+        return EXCL_E_INVALID;
+    if (nq > kNAQueries) return EXCL_E_CAPACITY;
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return EXCL_E_CUDA;
+    if (dev != ix->dev->device) return EXCL_E_INVALID;  // the index lives on another device
+    uint32_t *base = nullptr;
+    int nsm = 0;
+    int s = setup_device(dev, &base, &nsm);
+    if (s) return s;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+
+    BatchView b{};
+    b.nq = nq;
+    b.qterms = base + kOffQterms;
+    b.qnterms = base + kOffQnterms;
+    b.tile_prefix = base + kOffTilePrefix;
+    b.tile_counter = base + kOffMisc + 1;
+    b.key_base = base + kOffKeyBase;
+    b.tile_count = base + kOffTileCount;
+    b.tile_slot = base + kOffTileSlot;
+    b.scratch = base + kOffSurvivors;
+    b.max_tiles = kNATiles;
+    b.max_keys = kNAKeys;
+    b.err = base + kOffMisc;
+    b.stats = reinterpret_cast<uint64_t *>(base + kOffStats);
+    uint32_t *ntiles = base + kOffNtiles, *nkeys = base + kOffNkeys, *tile_out = base + kOffTileOut;
+    uint64_t *scan_state = reinterpret_cast<uint64_t *>(base + kOffScanState);
+    uint32_t *ticket = base + kOffMisc + 2;
+    const DevIndexView ixv = ix->dev->view(ix->models ? model_view(ix->models) : ModelView{});
+
+    int e = 0;
+    e |= (int)cudaMemsetAsync(base + kOffMisc, 0, 64 * 4, st);   // error flag, work counter, tickets
+    e |= (int)cudaMemsetAsync(base + kOffStats, 0, 64 * 4, st);
+    e |= launch_pack(ix->dev->lists, ix->nlists, d_terms, d_term_offsets, nq, b, ntiles, nkeys, st);
+    e |= launch_scan(ntiles, base + kOffTilePrefix, nullptr, nq, kNAQueries, scan_state, ticket, b.err, st);
+    e |= launch_scan(nkeys, base + kOffKeyBase, nullptr, nq, kNAQueries, scan_state, ticket, b.err, st);
+    e |= launch_probe(ixv, b, (int)algo, 8, 4, nsm, st);
+    e |= launch_scan(b.tile_count, tile_out, base + kOffTilePrefix + nq, 0, kNATiles, scan_state, ticket, b.err, st);
+    e |= launch_scatter(b, tile_out, d_offsets, d_docids, cap, nsm, st);
+    if (e) return EXCL_E_CUDA;
+    // the device-side limits (keys, tiles, result capacity) surface here
+    uint32_t flags = 0;
+    if (cudaMemcpyAsync(&flags, base + kOffMisc, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess) return EXCL_E_CUDA;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return EXCL_E_CUDA;
+    if (flags & kErrCapacity) return EXCL_E_CAPACITY;
+    if (flags & (kErrTermId | kErrTerms)) return EXCL_E_INVALID;
+    if (flags) return EXCL_E_DEVICE_FLAG;
+    return EXCL_OK;
+}

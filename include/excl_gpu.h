@@ -165,6 +165,27 @@ int excl_intersect_device(excl_ctx *ctx, excl_index *ix, const uint32_t *d_terms
 /* Synchronises the context stream and reports device-side error flags. */
 int excl_ctx_check(excl_ctx *ctx);
 
+/* Allocation-free form of excl_intersect_device; it has no counterpart in the
+ * reference. For callers that cannot call cudaMalloc when they query (a host
+ * that fixes its device memory budget at start-up, or an embedding without an
+ * excl_ctx, whose creation allocates the batch buffers): the per-batch scratch
+ * lives in one fixed device array inside the library (5.0 MiB on every GPU that
+ * loads it, held until the process exits), so the call allocates nothing.
+ * The index must already be uploaded, on the current device. The caller passes
+ * the inputs and outputs as device pointers and the cudaStream_t to run on;
+ * the call returns after that stream has finished the batch.
+ * Limits: nq <= EXCL_NOALLOC_MAX_QUERIES (else EXCL_E_CAPACITY before any
+ * work) and at most EXCL_NOALLOC_MAX_KEYS docIDs over the queries' shortest
+ * lists (else EXCL_E_CAPACITY after the batch).
+ * The first call on a device looks up the array's device address; make that
+ * first call before any stream capture. All calls share the array: calls whose
+ * work overlaps on the GPU race and must be serialised by the caller. */
+#define EXCL_NOALLOC_MAX_QUERIES 4096u
+#define EXCL_NOALLOC_MAX_KEYS (1u << 20)
+int excl_intersect_device_noalloc(excl_index *ix, const uint32_t *d_terms, const uint32_t *d_term_offsets,
+                                  uint32_t nq, uint32_t algo, uint32_t *d_offsets, uint32_t *d_docids, uint64_t cap,
+                                  void *stream);
+
 /* Per-kernel timing of the last excl_intersect_device / excl_wait (ms, CUDA events). */
 typedef struct {
     float pack_ms, probe_ms, compact_ms, total_ms;
