@@ -211,6 +211,42 @@ def run_queries(docs, list_offsets, terms, term_offsets, threads: int = 1) -> tu
     return float(secs), counts[:nq]
 
 
+_runqc = _f(_lib, "or_run_queries_compressed", C.c_double, u32p, u32p, u32p, u32p, u32p, u64p, u32p, u32p, u32p,
+            u32p, u32p, u64p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, u64p)
+
+
+class CompressedImage:
+    """The arrays of an exported index, laid out for the compressed CPU path."""
+
+    def __init__(self, arrays):
+        L = arrays.lists
+        self.words = np.ascontiguousarray(arrays.words, dtype=np.uint32)
+        self.lcodec = np.ascontiguousarray(L["codec"], dtype=np.uint32)
+        self.ln = np.ascontiguousarray(L["n"], dtype=np.uint32)
+        self.lseg = np.ascontiguousarray(L["seg_base"], dtype=np.uint32)
+        self.lnseg = np.ascontiguousarray(L["nseg"], dtype=np.uint32)
+        self.lword = np.ascontiguousarray(L["word_base"], dtype=np.uint64)
+        self.lreg = np.ascontiguousarray(np.stack([np.asarray(L["reg"][:, i]) for i in range(4)], axis=1)
+                                         if len(L) else np.zeros((0, 4)), dtype=np.uint32).reshape(-1)
+        self.head = np.ascontiguousarray(arrays.seg_head, dtype=np.uint32)
+        self.rec = np.ascontiguousarray(arrays.seg_rec, dtype=np.uint32).reshape(-1)
+        self.sreg = np.ascontiguousarray(arrays.seg_reg, dtype=np.uint32).reshape(-1)
+        self.max_list = int(self.ln.max()) if len(self.ln) else 1
+        self.max_seg = int(arrays.seg_rec[:, 3].max()) if len(arrays.seg_rec) else 1
+
+
+def run_queries_compressed(img: CompressedImage, terms, term_offsets, threads: int = 1):
+    """Decode + exact AND of every query on the compressed image; (seconds, counts)."""
+    t = _u32(terms) if len(terms) else np.zeros(1, np.uint32)
+    to = np.ascontiguousarray(term_offsets, dtype=np.uint64)
+    nq = len(to) - 1
+    counts = np.zeros(max(nq, 1), dtype=np.uint64)
+    secs = _runqc(_p(img.words), _p(img.lcodec), _p(img.ln), _p(img.lseg), _p(img.lnseg), _p(img.lword, u64p),
+                  _p(img.lreg), _p(img.head), _p(img.rec), _p(img.sreg), _p(t), _p(to, u64p), nq, threads,
+                  img.max_list, img.max_seg, _p(counts, u64p))
+    return float(secs), counts[:nq]
+
+
 def answer(docs, list_offsets, terms, term_offsets) -> tuple[np.ndarray, np.ndarray]:
     """Expected (offsets[nq+1], docids) of a batch."""
     lo = np.asarray(list_offsets, dtype=np.uint64)

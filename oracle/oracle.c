@@ -486,8 +486,144 @@ void or_checksum(uint32_t nq, const uint64_t *offsets, const uint32_t *res, uint
 }
 
 /* ---------------------------------------------------------------------------
- * Threaded CPU baseline over already-decoded lists (CSR) — used by bench.py's
- * CPU leg and the reference arm: per query, exact galloping AND.
+ * CPU path over the compressed index image (the layout libexcl_gpu exports:
+ * per list {codec, n, seg_base, nseg, word_base, reg[4]}, per segment head,
+ * rec {start, off, aux, count}, reg {a, b, L, R}). Per query: decode the
+ * shortest list; for each longer list walk its segment heads with a cursor
+ * (keys ascend), decode a segment once when a key first lands in it
+ * (ParaPFor.cpp decodeBlock + the codec's reconstruction) and binary-search
+ * the key there. This is the reference's decode + AND on the host.
+ * ------------------------------------------------------------------------- */
+typedef struct {
+    const uint32_t *words;
+    const uint32_t *lcodec, *ln, *lseg, *lnseg;
+    const uint64_t *lword;
+    const uint32_t *lreg;     /* 4 per list */
+    const uint32_t *head;
+    const uint32_t *rec;      /* 4 per segment */
+    const uint32_t *sreg;     /* 4 per segment */
+} or_image;
+
+static void or_decode_seg(const or_image *im, uint32_t l, uint32_t s, uint32_t *out) {
+    const uint32_t sg = im->lseg[l] + s;
+    const uint32_t *r = im->rec + 4 * (size_t)sg;
+    const uint32_t st = r[0], cnt = r[3];
+    const uint32_t codec = im->lcodec[l];
+    or_parapfd_decode_block(im->words + im->lword[l] + r[1], cnt, out);
+    if (codec == 0 || codec == 5) {
+        out[0] = im->head[sg];
+        for (uint32_t i = 1; i < cnt; ++i) out[i] += out[i - 1];
+    } else if (codec == 1) {
+        float slope; int32_t icpt;
+        memcpy(&slope, &im->lreg[4 * l], 4);
+        memcpy(&icpt, &im->lreg[4 * l + 1], 4);
+        for (uint32_t i = 0; i < cnt; ++i) out[i] += (uint32_t)or_pred_lrc(st + i, slope) + (uint32_t)icpt;
+    } else {
+        float a, b;
+        if (codec == 2) { memcpy(&a, &im->lreg[4 * l], 4); memcpy(&b, &im->lreg[4 * l + 1], 4); }
+        else { memcpy(&a, &im->sreg[4 * (size_t)sg], 4); memcpy(&b, &im->sreg[4 * (size_t)sg + 1], 4); }
+        for (uint32_t i = 0; i < cnt; ++i) {
+            uint32_t idx = (codec == 2) ? st + i : i;
+            out[i] += (uint32_t)or_pred_fma(idx, a, b) + r[2];
+        }
+    }
+}
+
+typedef struct {
+    const or_image *im;
+    const uint32_t *terms;
+    const uint64_t *toff;
+    uint32_t q0, q1;
+    uint64_t *counts;
+    uint32_t *keys, *tmp, *seg;
+} or_cjob;
+
+static void *or_cworker(void *arg) {
+    or_cjob *j = (or_cjob *)arg;
+    const or_image *im = j->im;
+    for (uint32_t q = j->q0; q < j->q1; ++q) {
+        uint32_t k = (uint32_t)(j->toff[q + 1] - j->toff[q]);
+        const uint32_t *t = j->terms + j->toff[q];
+        if (k == 0) { j->counts[q] = 0; continue; }
+        uint32_t sh = 0;
+        for (uint32_t i = 1; i < k; ++i) if (im->ln[t[i]] < im->ln[t[sh]]) sh = i;
+        /* decode the shortest list */
+        uint32_t ls = t[sh], n = 0;
+        for (uint32_t s = 0; s < im->lnseg[ls]; ++s) {
+            or_decode_seg(im, ls, s, j->keys + n);
+            n += im->rec[4 * (size_t)(im->lseg[ls] + s) + 3];
+        }
+        /* probe the others in ascending length */
+        uint8_t done[64] = {0};
+        done[sh] = 1;
+        for (uint32_t r = 1; r < k && n; ++r) {
+            uint32_t b = 0;
+            while (done[b]) ++b;
+            for (uint32_t i = b + 1; i < k; ++i) if (!done[i] && im->ln[t[i]] < im->ln[t[b]]) b = i;
+            done[b] = 1;
+            const uint32_t l = t[b];
+            const uint32_t *hd = im->head + im->lseg[l];
+            const uint32_t ns = im->lnseg[l];
+            uint32_t cur = 0, cached = 0xffffffffu, cnt = 0, m = 0;
+            for (uint32_t i = 0; i < n; ++i) {
+                const uint32_t key = j->keys[i];
+                if (key < hd[0]) continue;
+                /* gallop to the last head <= key */
+                uint32_t step = 1, hi = cur + 1;
+                while (hi < ns && hd[hi] <= key) { cur = hi; hi += step; step <<= 1; }
+                if (hi > ns) hi = ns;
+                uint32_t lo = cur;
+                while (lo + 1 < hi) { uint32_t mid = (lo + hi) >> 1; if (hd[mid] <= key) lo = mid; else hi = mid; }
+                cur = lo;
+                if (cur != cached) {
+                    or_decode_seg(im, l, cur, j->seg);
+                    cnt = im->rec[4 * (size_t)(im->lseg[l] + cur) + 3];
+                    cached = cur;
+                }
+                uint32_t a = 0, z = cnt;
+                while (a < z) { uint32_t mid = (a + z) >> 1; if (j->seg[mid] < key) a = mid + 1; else z = mid; }
+                if (a < cnt && j->seg[a] == key) j->keys[m++] = key;
+            }
+            n = m;
+        }
+        j->counts[q] = n;
+    }
+    return NULL;
+}
+
+/* Runs queries [0, nq) over the compressed image on `threads` threads; wall seconds. */
+double or_run_queries_compressed(const uint32_t *words, const uint32_t *lcodec, const uint32_t *ln,
+                                 const uint32_t *lseg, const uint32_t *lnseg, const uint64_t *lword,
+                                 const uint32_t *lreg, const uint32_t *head, const uint32_t *rec,
+                                 const uint32_t *sreg, const uint32_t *terms, const uint64_t *toff, uint32_t nq,
+                                 uint32_t threads, uint32_t max_list, uint32_t max_seg, uint64_t *counts) {
+    or_image im = {words, lcodec, ln, lseg, lnseg, lword, lreg, head, rec, sreg};
+    if (threads < 1) threads = 1;
+    pthread_t *th = (pthread_t *)malloc(sizeof(pthread_t) * threads);
+    or_cjob *jobs = (or_cjob *)malloc(sizeof(or_cjob) * threads);
+    for (uint32_t t = 0; t < threads; ++t) {
+        jobs[t].im = &im; jobs[t].terms = terms; jobs[t].toff = toff;
+        jobs[t].q0 = (uint32_t)((uint64_t)nq * t / threads);
+        jobs[t].q1 = (uint32_t)((uint64_t)nq * (t + 1) / threads);
+        jobs[t].counts = counts;
+        jobs[t].keys = (uint32_t *)malloc(((size_t)max_list + 8) * 4);
+        jobs[t].seg = (uint32_t *)malloc(((size_t)max_seg + 8) * 4);
+        jobs[t].tmp = NULL;
+    }
+    struct timespec a, b;
+    clock_gettime(CLOCK_MONOTONIC, &a);
+    for (uint32_t t = 0; t < threads; ++t) pthread_create(&th[t], NULL, or_cworker, &jobs[t]);
+    for (uint32_t t = 0; t < threads; ++t) pthread_join(th[t], NULL);
+    clock_gettime(CLOCK_MONOTONIC, &b);
+    for (uint32_t t = 0; t < threads; ++t) { free(jobs[t].keys); free(jobs[t].seg); }
+    free(th);
+    free(jobs);
+    return (double)(b.tv_sec - a.tv_sec) + 1e-9 * (double)(b.tv_nsec - a.tv_nsec);
+}
+
+/* ---------------------------------------------------------------------------
+ * Threaded CPU baseline over already-decoded lists (CSR): per query, exact
+ * galloping AND.
  * ------------------------------------------------------------------------- */
 typedef struct {
     const uint32_t *docs;
