@@ -71,6 +71,19 @@ class BatchStats(C.Structure):
                 ("fallbacks", C.c_uint64)]
 
 
+class LearnParams(C.Structure):
+    _fields_ = [("min_postings", C.c_uint32), ("nleaves", C.c_uint32), ("steps", C.c_uint32), ("batch", C.c_uint32),
+                ("lr", C.c_float), ("max_window", C.c_uint32), ("seed", C.c_uint32)]
+
+
+class LearnReport(C.Structure):
+    _fields_ = [("models", C.c_uint32), ("train_ms", C.c_double), ("fit_ms", C.c_double), ("final_loss", C.c_float),
+                ("mean_window", C.c_double), ("wide_leaf_frac", C.c_double), ("params_bytes", C.c_uint64)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 def _sig(name, res, *args):
     f = getattr(_lib, name)
     f.restype = res
@@ -104,7 +117,15 @@ _check = _sig("excl_ctx_check", C.c_int, C.c_void_p)
 _stats = _sig("excl_last_stats", C.c_int, C.c_void_p, C.POINTER(BatchStats))
 _checksum = _sig("excl_checksum", C.c_int, C.c_uint32, u32p, u32p, C.POINTER(C.c_uint64 * 3))
 
-EXPORTED = ["excl_parapfd_encode", "excl_parapfd_decode", "excl_set_frac", "encodeArray", "decodeArray",
+_learn = _sig("excl_learn_models", C.c_int, C.c_void_p, C.c_void_p, C.POINTER(LearnParams), C.POINTER(LearnReport))
+_mexport = _sig("excl_model_export", C.c_int, C.c_void_p, C.c_uint32, C.POINTER(C.c_float), C.POINTER(C.c_float),
+                C.POINTER(C.c_int32), C.POINTER(C.c_uint32))
+_mgrad = _sig("excl_model_grad", C.c_int, C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_float),
+              C.POINTER(C.c_float), C.c_uint32, C.POINTER(C.c_float), C.POINTER(C.c_float))
+
+_mtables = _sig("excl_model_tables", C.c_int, C.c_void_p, C.c_uint32, C.POINTER(C.c_uint16), u32p, u32p)
+
+EXPORTED = ["excl_learn_models", "excl_model_export", "excl_model_grad", "excl_model_tables", "excl_parapfd_encode", "excl_parapfd_decode", "excl_set_frac", "encodeArray", "decodeArray",
             "excl_index_build", "excl_index_free", "excl_index_sizes_get", "excl_index_export", "excl_ctx_create",
             "excl_ctx_destroy", "excl_last_error", "excl_ctx_stream", "excl_index_upload",
             "excl_decode_lists_device", "excl_decode_lists", "excl_submit", "excl_wait", "excl_batch_free",
@@ -222,6 +243,29 @@ class Index:
         arr = np.ctypeslib.as_array(lists).copy() if s.nlists else np.zeros(0)
         return IndexArrays(arr, words, head, rec, reg, d[: s.ndir])
 
+    def model(self, list_id: int):
+        """(root params[1153], header {kmin, kscale, nleaves, max_window}, leaves[L, 4] as int32 words) or None."""
+        L = C.c_uint32(0)
+        hdr = np.zeros(4, dtype=np.float32)
+        if _mexport(self._h, list_id, None, hdr.ctypes.data_as(C.POINTER(C.c_float)), None, C.byref(L)) != OK:
+            return None
+        root = np.zeros(1153, dtype=np.float32)
+        leaves = np.zeros((L.value, 4), dtype=np.int32)
+        _check_status(_mexport(self._h, list_id, root.ctypes.data_as(C.POINTER(C.c_float)),
+                               hdr.ctypes.data_as(C.POINTER(C.c_float)), leaves.ctypes.data_as(C.POINTER(C.c_int32)),
+                               C.byref(L)))
+        return root, hdr, leaves
+
+    def model_tables(self, list_id: int):
+        """(grid[grid_n+1] uint16, bnd[nleaves] uint32, first, grid_shift) of a list's stored routing, or None."""
+        meta = np.zeros(4, dtype=np.uint32)
+        if _mtables(self._h, list_id, None, None, _p32(meta)) != OK:
+            return None
+        grid = np.zeros(int(meta[2]) + 1, dtype=np.uint16)
+        bnd = np.zeros(int(meta[3]), dtype=np.uint32)
+        _check_status(_mtables(self._h, list_id, grid.ctypes.data_as(C.POINTER(C.c_uint16)), _p32(bnd), _p32(meta)))
+        return grid, bnd, int(meta[0]), int(meta[1])
+
     def close(self) -> None:
         if self._h:
             _ifree(self._h)
@@ -295,6 +339,26 @@ class Context:
 
     def check(self) -> None:
         _check_status(_check(self._h), self, "excl_ctx_check")
+
+    def learn(self, ix: Index, min_postings: int = 1 << 20, nleaves: int = 4096, steps: int = 300,
+              batch: int = 16384, lr: float = 3e-3, max_window: int = 4096, seed: int = 1) -> dict:
+        """Trains the learned position models of the index's long lists on this device."""
+        p = LearnParams(min_postings, nleaves, steps, batch, lr, max_window, seed)
+        r = LearnReport()
+        _check_status(_learn(self._h, ix._h, C.byref(p), C.byref(r)), self, "excl_learn_models")
+        return r.as_dict()
+
+    def model_grad(self, params, x, y) -> tuple[np.ndarray, float]:
+        """Gradient of the training kernels for given samples (for checks)."""
+        fp = C.POINTER(C.c_float)
+        P = np.ascontiguousarray(params, dtype=np.float32)
+        xs = np.ascontiguousarray(x, dtype=np.float32)
+        ys = np.ascontiguousarray(y, dtype=np.float32)
+        g = np.zeros(1153, dtype=np.float32)
+        loss = C.c_float(0)
+        _check_status(_mgrad(self._h, P.ctypes.data_as(fp), xs.ctypes.data_as(fp), ys.ctypes.data_as(fp), len(xs),
+                             g.ctypes.data_as(fp), C.byref(loss)), self, "excl_model_grad")
+        return g, loss.value
 
     def stats(self) -> BatchStats:
         s = BatchStats()

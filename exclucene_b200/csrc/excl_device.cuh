@@ -15,13 +15,23 @@ constexpr int kHidden = 32;
 constexpr int kRootParams = kHidden + kHidden + kHidden * kHidden + kHidden + kHidden + 1;  // 1153
 constexpr int kRootStride = 1156;
 
-struct ModelHdr {
+// The root is trained with non-negative weights, so its FP32 evaluation (and
+// the leaf floor(out * L)) is non-decreasing in the key. Its routing is
+// therefore a step function of the key and is stored exactly as the first key
+// of every leaf (bnd) plus a coarse grid of the routing over the key range;
+// the probe routes with two or three loads instead of evaluating the network.
+struct alignas(16) ModelHdr {
     float kmin, kscale;    // x = (key - kmin) * kscale in [0, 1]
     uint32_t nleaves;      // leaves of this model
     uint32_t leaf_base;    // first leaf in the leaf array
     uint32_t n;            // postings of the list
     uint32_t max_window;   // leaves with a wider window fall back to the directory search
-    uint32_t pad[2];
+    uint32_t first;        // first docID of the list (grid origin)
+    uint32_t grid_shift;   // grid cell = (key - first) >> grid_shift
+    uint32_t grid_n;       // cells; the grid holds grid_n + 1 leaf ids
+    uint32_t grid_base;    // first entry in the grid array
+    uint32_t bnd_base;     // first entry in the boundary array (nleaves entries)
+    uint32_t pad;
 };
 
 struct alignas(16) Leaf {
@@ -34,6 +44,8 @@ struct ModelView {
     const float *root = nullptr;      // kRootStride floats per model
     const ModelHdr *hdr = nullptr;
     const Leaf *leaves = nullptr;
+    const uint16_t *grid = nullptr;   // routing at grid points
+    const uint32_t *bnd = nullptr;    // bnd[l] = first key routed to a leaf >= l (0xffffffff: none)
 };
 
 struct DevIndexView {
@@ -45,6 +57,8 @@ struct DevIndexView {
     const uint32_t *dir;
     const uint64_t *tilemap;
     const uint64_t *post_base;
+    const uint32_t *seg_list;   // list of each segment
+    const uint64_t *seg_gword;  // first word of each segment's block (nsegs + 1 entries)
     ModelView models;
 };
 
@@ -324,6 +338,27 @@ __device__ __forceinline__ uint32_t model_leaf_of(float root_out, uint32_t nleav
 
 __device__ __forceinline__ float model_norm(const ModelHdr &m, uint32_t key) {
     return __fmul_rn(__fsub_rn(__uint2float_rn(key), m.kmin), m.kscale);
+}
+
+// Leaf of `key` (first <= key <= last) from the stored routing: the grid cell
+// bounds the leaf to [grid[j], grid[j+1]]; the boundaries resolve it exactly.
+__device__ __forceinline__ uint32_t model_route(const uint16_t *grid, const uint32_t *bnd, const ModelHdr &m,
+                                                uint32_t key) {
+    const uint32_t j = (key - m.first) >> m.grid_shift;
+    uint32_t lo = grid[m.grid_base + j];
+    uint32_t hi = grid[m.grid_base + j + 1];
+    const uint32_t *b = bnd + m.bnd_base;
+    if (hi - lo <= 8) {
+        while (lo < hi && __ldg(b + lo + 1) <= key) ++lo;
+        return lo;
+    }
+    // many leaves inside one cell: last l in [lo, hi] with b[l] <= key
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        if (__ldg(b + mid) <= key) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
 }
 
 __device__ __forceinline__ int model_pred_rank(const Leaf &lf, float x) {

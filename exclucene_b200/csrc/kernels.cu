@@ -1,8 +1,6 @@
 // sm_100a kernels of the batched decode + AND-intersection path.
 //
-//   k_decode_lists   K1/K2: warp-per-segment decode of whole lists (ParaPFD
-//                    d-gaps with a warp scan; residual codecs with the
-//                    regression prediction), coalesced stores through smem.
+//   (whole-list decode, K1/K2, is in decode.cu)
 //   k_pack           per-query term sort by list length + tiles of the
 //                    shortest list (replaces CPUPreprocess, ParaPFD_Intersection.cu:126-227).
 //   k_scan_excl      device-wide exclusive scan, single pass with decoupled
@@ -21,195 +19,6 @@
 #include "kernels.h"
 
 namespace excl {
-
-// ---------------------------------------------------------------------------
-// K1/K2 whole-list decode.
-
-constexpr int kDecodeWarps = 8;
-constexpr uint32_t kStageWords = kTileKeys * 31 / 32 + 2;  // lows of a 256-value block at b <= 31, + window word
-constexpr int kPrefetch = (kStageWords + 31) / 32;         // words per lane held in registers
-
-// Whole-list decode. Each warp owns a contiguous range of segments and walks
-// it in groups of 32: lane i first loads the metadata of the group's i-th
-// segment (record, list, descriptor, regression) so those dependent loads run
-// 32-wide; then, segment by segment, the warp stages the block's packed low
-// bits in shared memory while the next segment's words are already being
-// fetched into registers, extracts each lane's run of values with a
-// shared-memory bit window, patches exceptions, reconstructs docIDs and writes
-// them with coalesced 128-byte stores.
-__global__ void __launch_bounds__(kDecodeWarps * 32, 4) k_decode_lists(DevIndexView ix, uint32_t l0, uint32_t l1,
-                                                                    uint64_t out_base0, uint32_t *__restrict__ out,
-                                                                    uint32_t seg0, uint32_t nsegs, uint32_t per_warp) {
-    __shared__ uint32_t s_words[kDecodeWarps][kStageWords + 2];
-    __shared__ uint32_t s_vals[kDecodeWarps][kTileKeys];
-    const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
-    const uint32_t gw = blockIdx.x * kDecodeWarps + w;
-    const uint64_t sb64 = (uint64_t)gw * per_warp;
-    if (sb64 >= nsegs) return;
-    const uint32_t sb = seg0 + (uint32_t)sb64;
-    const uint32_t se = seg0 + (uint32_t)(sb64 + per_warp < (uint64_t)nsegs ? sb64 + per_warp : (uint64_t)nsegs);
-    // list containing segment sb: last list in [l0, l1) with seg_base <= sb
-    uint32_t lo = l0, hi = l1;
-    while (lo < hi) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (ix.lists[mid].seg_base <= sb) lo = mid + 1;
-        else hi = mid;
-    }
-    uint32_t lcur = lo - 1;
-    uint32_t *wbuf = s_words[w], *vbuf = s_vals[w];
-    uint32_t Lidx = 0xffffffffu;
-    uint32_t Lcodec = 0, Lreg0 = 0, Lreg1 = 0;
-    for (uint32_t g0 = sb; g0 < se; g0 += 32) {
-        const uint32_t gn = min(32u, se - g0);
-        // ---- per-lane metadata of segment g0 + lane
-        uint32_t my_l = lcur, m_start = 0, m_aux = 0, m_count = 0, m_desc = 0, m_head = 0;
-        uint64_t m_gword = 0, m_ob = 0;
-        float m_a = 1.0f, m_b = 0.0f;
-        if (lane < gn) {
-            const uint32_t s = g0 + lane;
-            while (s >= ix.lists[my_l].seg_base + ix.lists[my_l].nseg) ++my_l;
-            const SegRec rec = ix.seg_rec[s];
-            m_start = rec.start;
-            m_aux = rec.aux;
-            m_count = rec.count;
-            m_gword = ix.lists[my_l].word_base + rec.off;
-            m_ob = ix.post_base[my_l] - out_base0 + rec.start;
-            m_desc = ldg(ix.words + m_gword);
-            const uint32_t c = ix.lists[my_l].codec;
-            if (codec_is_dgap(c)) m_head = ldg(ix.seg_head + s);
-            if (c == EXCL_CODEC_SEGLRC || c == EXCL_CODEC_HS_SEGLRC) {
-                const SegReg rg = ix.seg_reg[s];
-                m_a = rg.a;
-                m_b = rg.b;
-            }
-        }
-        lcur = __shfl_sync(0xffffffffu, my_l, gn - 1);
-        auto lows_words = [&](uint32_t desc, uint32_t count) -> uint32_t {
-            return count > kTileKeys ? 0u : words_for(count, (desc >> 26) & 31u) + 1u;
-        };
-        // prefetch the first segment's low-bit words
-        uint32_t pw[kPrefetch];
-        {
-            const uint64_t gwd = __shfl_sync(0xffffffffu, m_gword, 0);
-            const uint32_t nw = lows_words(__shfl_sync(0xffffffffu, m_desc, 0), __shfl_sync(0xffffffffu, m_count, 0));
-#pragma unroll
-            for (int k = 0; k < kPrefetch; ++k) {
-                const uint32_t i = lane + 32u * k;
-                pw[k] = i < nw ? ldg(ix.words + gwd + 1 + i) : 0u;
-            }
-        }
-        for (uint32_t j = 0; j < gn; ++j) {
-            const uint32_t desc = __shfl_sync(0xffffffffu, m_desc, j);
-            const uint32_t count = __shfl_sync(0xffffffffu, m_count, j);
-            const uint32_t start = __shfl_sync(0xffffffffu, m_start, j);
-            const uint32_t aux = __shfl_sync(0xffffffffu, m_aux, j);
-            const uint32_t head = __shfl_sync(0xffffffffu, m_head, j);
-            const uint32_t l = __shfl_sync(0xffffffffu, my_l, j);
-            const uint64_t gwd = __shfl_sync(0xffffffffu, m_gword, j);
-            const uint64_t ob = __shfl_sync(0xffffffffu, m_ob, j);
-            const float sa = __shfl_sync(0xffffffffu, m_a, j), sbb = __shfl_sync(0xffffffffu, m_b, j);
-            if (l != Lidx) {
-                Lidx = l;
-                Lcodec = ix.lists[l].codec;
-                Lreg0 = ix.lists[l].reg[0];
-                Lreg1 = ix.lists[l].reg[1];
-            }
-            const BlkHdr h = blk_hdr(desc);
-            // stage this segment's words, then start fetching the next one's
-            const uint32_t nw = lows_words(desc, count);
-#pragma unroll
-            for (int k = 0; k < kPrefetch; ++k) {
-                const uint32_t i = lane + 32u * k;
-                if (i < nw) wbuf[i] = pw[k];
-            }
-            if (j + 1 < gn) {
-                const uint64_t ngw = __shfl_sync(0xffffffffu, m_gword, j + 1);
-                const uint32_t nnw =
-                    lows_words(__shfl_sync(0xffffffffu, m_desc, j + 1), __shfl_sync(0xffffffffu, m_count, j + 1));
-#pragma unroll
-                for (int k = 0; k < kPrefetch; ++k) {
-                    const uint32_t i = lane + 32u * k;
-                    pw[k] = i < nnw ? ldg(ix.words + ngw + 1 + i) : 0u;
-                }
-            }
-            __syncwarp();
-            if (count > kTileKeys) {
-                // large hash bucket: 256-slices straight from global memory
-                const ListDesc L = ix.lists[l];
-                for (uint32_t e0 = 0; e0 < count; e0 += kTileKeys) {
-                    const uint32_t kc = min(kTileKeys, count - e0);
-                    warp_decode(ix, L, g0 + j, e0, kc, vbuf, lane);
-                    for (uint32_t i = lane; i < kc; i += 32) out[ob + e0 + i] = vbuf[i];
-                    __syncwarp();
-                }
-            } else {
-                const uint32_t vpl = (count + 31u) >> 5;
-                const uint32_t el = lane * vpl;
-                const uint32_t mask = (1u << h.lb) - 1u;
-                uint32_t v[8];
-#pragma unroll
-                for (int q = 0; q < 8; ++q) {
-                    const uint32_t bit = (el + q) * h.lb;
-                    const uint32_t wi = bit >> 5;
-                    v[q] = (q < (int)vpl && el + q < count)
-                               ? (__funnelshift_r(wbuf[wi], wbuf[wi + 1], bit & 31u) & mask)
-                               : 0u;
-                }
-                if (h.en) {
-#pragma unroll
-                    for (int q = 0; q < 8; ++q)
-                        if (q < (int)vpl && el + q < count) vbuf[el + q] = v[q];
-                    __syncwarp();
-                    const uint32_t *pb = ix.words + gwd + 1 + words_for(count, h.lb);
-                    const uint32_t *hp = pb + words_for(h.en, h.eb);
-                    for (uint32_t x = lane; x < h.en; x += 32) {
-                        const uint32_t p = get_bits(pb, x * h.eb, h.eb);
-                        if (p < count) vbuf[p] |= get_bits(hp, x * h.hb, h.hb) << h.lb;
-                    }
-                    __syncwarp();
-#pragma unroll
-                    for (int q = 0; q < 8; ++q)
-                        if (q < (int)vpl && el + q < count) v[q] = vbuf[el + q];
-                    __syncwarp();
-                }
-                if (codec_is_dgap(Lcodec)) {
-                    if (lane == 0) v[0] = head;
-                    uint32_t run = 0;
-#pragma unroll
-                    for (int q = 0; q < 8; ++q) {
-                        run += v[q];
-                        v[q] = run;
-                    }
-                    uint32_t incl = run;
-#pragma unroll
-                    for (int o = 1; o < 32; o <<= 1) {
-                        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
-                        if (lane >= (uint32_t)o) incl += t;
-                    }
-                    const uint32_t ex = incl - run;
-#pragma unroll
-                    for (int q = 0; q < 8; ++q) v[q] += ex;
-                } else if (Lcodec == EXCL_CODEC_LRC) {
-#pragma unroll
-                    for (int q = 0; q < 8; ++q) v[q] += pred_lrc(start + el + q, __uint_as_float(Lreg0), (int32_t)Lreg1);
-                } else if (Lcodec == EXCL_CODEC_LRCSEG) {
-#pragma unroll
-                    for (int q = 0; q < 8; ++q)
-                        v[q] += pred_fma(start + el + q, __uint_as_float(Lreg0), __uint_as_float(Lreg1)) + aux;
-                } else {
-#pragma unroll
-                    for (int q = 0; q < 8; ++q) v[q] += pred_fma(el + q, sa, sbb) + aux;
-                }
-#pragma unroll
-                for (int q = 0; q < 8; ++q)
-                    if (q < (int)vpl && el + q < count) vbuf[el + q] = v[q];
-                __syncwarp();
-                for (uint32_t i = lane; i < count; i += 32) out[ob + i] = vbuf[i];
-                __syncwarp();
-            }
-        }
-    }
-}
 
 // ---------------------------------------------------------------------------
 // Query pack: sort each query's terms by list length (stable insertion sort,
@@ -391,8 +200,9 @@ __device__ __forceinline__ bool probe_key(const DevIndexView &ix, const ListDesc
     if ((ALGO == EXCL_ALGO_LEARNED || ALGO == EXCL_ALGO_AUTO) && L.model != kNoModel) {
         const ModelHdr m = ix.models.hdr[L.model];
         const float x = model_norm(m, key);
-        const float r = model_root(ix.models.root + (size_t)L.model * kRootStride, x);
-        const Leaf lf = ix.models.leaves[m.leaf_base + model_leaf_of(r, m.nleaves)];
+        const Leaf lf = ix.models.leaves[m.leaf_base + model_route(ix.models.grid, ix.models.bnd, m, key)];
+        // no posting of the list routes to an empty leaf, and routing is deterministic
+        if (lf.ehi < lf.elo) return false;
         if ((uint32_t)(lf.ehi - lf.elo) <= m.max_window) {
             const int pr = model_pred_rank(lf, x);
             plo = imax64(0, (int64_t)pr + lf.elo);
@@ -586,18 +396,6 @@ __global__ void k_scatter(BatchView b, const uint32_t *__restrict__ tile_out, ui
 
 // ---------------------------------------------------------------------------
 // Launchers.
-
-int launch_decode(const DevIndexView &ix, uint32_t l0, uint32_t l1, uint64_t out_base0, uint32_t *out, uint32_t seg0,
-                  uint32_t nsegs, int nsm, cudaStream_t st) {
-    if (nsegs == 0) return 0;
-    const uint64_t max_warps = (uint64_t)nsm * 8 * kDecodeWarps;
-    const uint64_t nwarps = std::min<uint64_t>(nsegs, max_warps);
-    const uint32_t per = (uint32_t)((nsegs + nwarps - 1) / nwarps);
-    const uint64_t used = (nsegs + per - 1) / per;
-    const uint32_t blocks = (uint32_t)((used + kDecodeWarps - 1) / kDecodeWarps);
-    k_decode_lists<<<blocks, kDecodeWarps * 32, 0, st>>>(ix, l0, l1, out_base0, out, seg0, nsegs, per);
-    return (int)cudaGetLastError();
-}
 
 int launch_pack(const ListDesc *lists, uint32_t nlists, const uint32_t *terms, const uint32_t *toff, uint32_t nq,
                 const BatchView &b, uint32_t *ntiles, uint32_t *nkeys, cudaStream_t st) {

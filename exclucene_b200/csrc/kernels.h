@@ -25,7 +25,7 @@ struct BatchView {
 };
 
 int launch_decode(const DevIndexView &ix, uint32_t l0, uint32_t l1, uint64_t out_base0, uint32_t *out, uint32_t seg0,
-                  uint32_t nsegs, int nsm, cudaStream_t st);
+                  uint32_t nsegs, int nsm, uint32_t *err, cudaStream_t st);
 int launch_pack(const ListDesc *lists, uint32_t nlists, const uint32_t *terms, const uint32_t *toff, uint32_t nq,
                 const BatchView &b, uint32_t *ntiles, uint32_t *nkeys, cudaStream_t st);
 uint32_t scan_blocks_for(uint64_t n);

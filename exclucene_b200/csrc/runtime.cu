@@ -161,6 +161,10 @@ void DeviceIndex::release() {
     cudaFree(dir);
     cudaFree(tilemap);
     cudaFree(post_base);
+    cudaFree(seg_list);
+    cudaFree(seg_gword);
+    seg_list = nullptr;
+    seg_gword = nullptr;
     lists = nullptr;
     words = seg_head = dir = nullptr;
     seg_rec = nullptr;
@@ -178,6 +182,8 @@ DevIndexView DeviceIndex::view(const ModelView &mv) const {
     v.dir = dir;
     v.tilemap = tilemap;
     v.post_base = post_base;
+    v.seg_list = seg_list;
+    v.seg_gword = seg_gword;
     v.models = mv;
     return v;
 }
@@ -350,6 +356,18 @@ extern "C" int excl_index_upload(excl_ctx *ctx, excl_index *ix) {
     if (!d) return EXCL_E_NOMEM;
     std::vector<uint64_t> pb(ix->nlists + 1, 0);
     for (uint32_t l = 0; l < ix->nlists; ++l) pb[l + 1] = pb[l] + ix->lists[l].n;
+    // per-segment list id and global block start (blocks of consecutive
+    // segments are contiguous, so a block ends where the next one starts)
+    const size_t nsegs = ix->seg_head.size();
+    std::vector<uint32_t> slist(nsegs);
+    std::vector<uint64_t> sgw(nsegs + 1);
+    for (uint32_t l = 0; l < ix->nlists; ++l)
+        for (uint32_t s = 0; s < ix->lists[l].nseg; ++s) {
+            const size_t g = (size_t)ix->lists[l].seg_base + s;
+            slist[g] = l;
+            sgw[g] = ix->lists[l].word_base + ix->seg_rec[g].off;
+        }
+    sgw[nsegs] = ix->words.size() - kWordPad;
     int st = 0;
     st |= dalloc(ctx, &d->lists, ix->lists.size(), "index lists");
     st |= dalloc(ctx, &d->words, ix->words.size(), "index words");
@@ -359,6 +377,8 @@ extern "C" int excl_index_upload(excl_ctx *ctx, excl_index *ix) {
     st |= dalloc(ctx, &d->dir, ix->dir.size(), "index dir");
     st |= dalloc(ctx, &d->tilemap, ix->tilemap.size(), "index tilemap");
     st |= dalloc(ctx, &d->post_base, pb.size(), "index post base");
+    st |= dalloc(ctx, &d->seg_list, slist.size(), "index seg list");
+    st |= dalloc(ctx, &d->seg_gword, sgw.size(), "index seg words");
     if (st) {
         d->release();
         delete d;
@@ -375,6 +395,8 @@ extern "C" int excl_index_upload(excl_ctx *ctx, excl_index *ix) {
     up(d->dir, ix->dir.data(), ix->dir.size() * 4);
     up(d->tilemap, ix->tilemap.data(), ix->tilemap.size() * 8);
     up(d->post_base, pb.data(), pb.size() * 8);
+    up(d->seg_list, slist.data(), slist.size() * 4);
+    up(d->seg_gword, sgw.data(), sgw.size() * 8);
     if (st) {
         d->release();
         delete d;
@@ -382,7 +404,7 @@ extern "C" int excl_index_upload(excl_ctx *ctx, excl_index *ix) {
     }
     d->bytes = ix->lists.size() * sizeof(ListDesc) + ix->words.size() * 4 + ix->seg_head.size() * 4 +
                ix->seg_rec.size() * sizeof(SegRec) + ix->seg_reg.size() * sizeof(SegReg) + ix->dir.size() * 4 +
-               ix->tilemap.size() * 8 + pb.size() * 8;
+               ix->tilemap.size() * 8 + pb.size() * 8 + slist.size() * 4 + sgw.size() * 8;
     d->device = ctx->device;
     ix->dev = d;
     if (ix->models) st = models_upload(ctx, ix);
@@ -413,7 +435,7 @@ extern "C" int excl_decode_lists_device(excl_ctx *ctx, excl_index *ix, uint32_t 
     const uint32_t seg0 = ix->lists[l0].seg_base;
     const uint32_t seg1 = ix->lists[l1 - 1].seg_base + ix->lists[l1 - 1].nseg;
     const int e = launch_decode(ix->dev->view(ModelView{}), l0, l1, base0, d_out, seg0, seg1 - seg0, ctx->nsm,
-                                ctx->stream);
+                                ctx->d_misc + kMiscErr, ctx->stream);
     return cuda_status(ctx, (cudaError_t)e, "decode launch");
 }
 

@@ -18,6 +18,8 @@ struct DeviceIndex {
     uint32_t *dir = nullptr;
     uint64_t *tilemap = nullptr;
     uint64_t *post_base = nullptr;
+    uint32_t *seg_list = nullptr;
+    uint64_t *seg_gword = nullptr;
     size_t bytes = 0;
     int device = 0;
     void release();

@@ -196,6 +196,53 @@ typedef struct {
 } excl_batch_stats;
 int excl_last_stats(excl_ctx *ctx, excl_batch_stats *st);
 
+/* ---------------------------------------------------------------------------
+ * Learned position models. The reference's analogue is SegLRC's two-level
+ * linear model: a list-level regression bounding the segment window and a
+ * per-segment regression with a safe range (SegLRC_Generator.cu:264-331,
+ * SegLRC_Intersection_kernel.cu:281-371). Here a root FP32 MLP 1->32->32->1,
+ * trained on the device on the list's (docID, rank) pairs, routes each key to
+ * one of `nleaves` linear leaves; each leaf stores the exact rank-error window
+ * of its keys, measured with the query-time arithmetic, so probes stay exact.
+ * Leaves wider than max_window fall back to the directory search. Models are
+ * built for fixed-block lists of at least min_postings postings and uploaded
+ * with the index; EXCL_ALGO_LEARNED / EXCL_ALGO_AUTO use them. */
+typedef struct {
+    uint32_t min_postings; /* lists with fewer postings get no model (0 = 2^20) */
+    uint32_t nleaves;      /* 0 = 4096 */
+    uint32_t steps;        /* training steps (0 = 300) */
+    uint32_t batch;        /* sampled (docID, rank) pairs per step (0 = 16384) */
+    float lr;              /* Adam learning rate (0 = 3e-3), cosine decay */
+    uint32_t max_window;   /* widest leaf window used (0 = 4096) */
+    uint32_t seed;
+} excl_learn_params;
+
+typedef struct {
+    uint32_t models;
+    double train_ms, fit_ms;   /* device time of training and of the leaf fits */
+    float final_loss;          /* largest final MSE on normalized rank over the models */
+    double mean_window;        /* mean leaf window (ranks) over non-empty leaves */
+    double wide_leaf_frac;     /* share of non-empty leaves wider than max_window */
+    uint64_t params_bytes;
+} excl_learn_report;
+
+int excl_learn_models(excl_ctx *ctx, excl_index *ix, const excl_learn_params *params, excl_learn_report *report);
+/* Model of one list: root parameters (1153 floats), header {kmin, kscale,
+ * nleaves, max_window}, leaves as {a, b, elo, ehi} (4 x 32-bit each). */
+int excl_model_export(const excl_index *ix, uint32_t list, float *root, float *hdr4, int32_t *leaves,
+                      uint32_t *nleaves);
+/* The stored routing of one list's model: because the root is trained with
+ * non-negative weights its leaf is non-decreasing in the key, so it is kept as
+ * bnd[l] = first key routed to a leaf >= l (0xffffffff if none) plus grid[j] =
+ * leaf of key first + (j << grid_shift), j in [0, grid_n]. meta = {first,
+ * grid_shift, grid_n, nleaves}. The probe routes with these tables. */
+int excl_model_tables(const excl_index *ix, uint32_t list, uint16_t *grid, uint32_t *bnd, uint32_t meta[4]);
+/* One forward/backward pass of the training kernels over n given (x, y)
+ * samples: the gradient of the mean squared error w.r.t. the 1153 root
+ * parameters (for checking the kernels against a CPU restatement). */
+int excl_model_grad(excl_ctx *ctx, const float *params, const float *x, const float *y, uint32_t n, float *grad,
+                    float *loss);
+
 /* Checksum triple of the reference (ParaPFD_Intersection.cu:378-403): empty
  * queries, total results, XOR of first/middle/last result per query. */
 int excl_checksum(uint32_t nq, const uint32_t *offsets, const uint32_t *docids, uint64_t cs[3]);

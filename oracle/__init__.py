@@ -247,6 +247,53 @@ def run_queries_compressed(img: CompressedImage, terms, term_offsets, threads: i
     return float(secs), counts[:nq]
 
 
+_mlp_grad = _f(_lib, "or_mlp_grad", None, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float),
+               C.c_uint32, C.POINTER(C.c_double), C.POINTER(C.c_double))
+_model_check = _f(_lib, "or_model_check", C.c_uint64, C.POINTER(C.c_float), C.c_float, C.c_float, C.c_uint32,
+                  i32p, u32p, C.c_uint64, u32p)
+
+MLP_PARAMS = 1153
+
+
+def mlp_grad(params, x, y) -> tuple[np.ndarray, float]:
+    """Double-precision gradient of the mean squared error of the root MLP."""
+    P = np.ascontiguousarray(params, dtype=np.float32)
+    xs = np.ascontiguousarray(x, dtype=np.float32)
+    ys = np.ascontiguousarray(y, dtype=np.float32)
+    g = np.zeros(MLP_PARAMS, dtype=np.float64)
+    loss = C.c_double(0)
+    fp = C.POINTER(C.c_float)
+    _mlp_grad(P.ctypes.data_as(fp), xs.ctypes.data_as(fp), ys.ctypes.data_as(fp), len(xs),
+              g.ctypes.data_as(C.POINTER(C.c_double)), C.byref(loss))
+    return g, loss.value
+
+
+_model_leaves = _f(_lib, "or_model_leaves", None, C.POINTER(C.c_float), C.c_float, C.c_float, C.c_uint32, u32p,
+                   C.c_uint64, u32p)
+
+
+def model_leaves(root, hdr4, keys) -> np.ndarray:
+    """Leaf of each key as the root network routes it (FP32 restatement)."""
+    P = np.ascontiguousarray(root, dtype=np.float32)
+    k = _u32(keys)
+    out = np.zeros(max(len(k), 1), dtype=np.uint32)
+    _model_leaves(P.ctypes.data_as(C.POINTER(C.c_float)), float(hdr4[0]), float(hdr4[1]), int(hdr4[2]), _p(k), len(k),
+                  _p(out))
+    return out[:len(k)]
+
+
+def model_check(root, hdr4, leaves, keys) -> tuple[int, np.ndarray]:
+    """Keys whose rank falls outside their leaf's window (0 = exact), and keys per leaf."""
+    P = np.ascontiguousarray(root, dtype=np.float32)
+    lv = np.ascontiguousarray(leaves, dtype=np.int32).reshape(-1)
+    k = _u32(keys)
+    L = int(hdr4[2])
+    counts = np.zeros(L, dtype=np.uint32)
+    bad = _model_check(P.ctypes.data_as(C.POINTER(C.c_float)), float(hdr4[0]), float(hdr4[1]), L,
+                       lv.ctypes.data_as(i32p), _p(k), len(k), _p(counts))
+    return int(bad), counts
+
+
 def answer(docs, list_offsets, terms, term_offsets) -> tuple[np.ndarray, np.ndarray]:
     """Expected (offsets[nq+1], docids) of a batch."""
     lo = np.asarray(list_offsets, dtype=np.uint64)

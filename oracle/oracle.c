@@ -486,6 +486,109 @@ void or_checksum(uint32_t nq, const uint64_t *offsets, const uint32_t *res, uint
 }
 
 /* ---------------------------------------------------------------------------
+ * Learned position model (no reference counterpart; checks the library's
+ * training kernels and its exactness claim). Parameter layout:
+ * w1[32] b1[32] w2[32][32] b2[32] w3[32] b3.
+ * ------------------------------------------------------------------------- */
+#define OR_H 32
+#define OR_NP (OR_H + OR_H + OR_H * OR_H + OR_H + OR_H + 1)
+
+/* Gradient of mean((f(x) - y)^2) in double precision. */
+void or_mlp_grad(const float *P, const float *x, const float *y, uint32_t n, double *grad, double *loss) {
+    const float *w1 = P, *b1 = P + OR_H, *w2 = P + 2 * OR_H, *b2 = w2 + OR_H * OR_H, *w3 = b2 + OR_H, *b3 = w3 + OR_H;
+    for (int j = 0; j < OR_NP; ++j) grad[j] = 0;
+    double L = 0;
+    for (uint32_t s = 0; s < n; ++s) {
+        double z1[OR_H], h1[OR_H], z2[OR_H], h2[OR_H];
+        for (int i = 0; i < OR_H; ++i) { z1[i] = (double)w1[i] * x[s] + b1[i]; h1[i] = z1[i] > 0 ? z1[i] : 0; }
+        double out = b3[0];
+        for (int o = 0; o < OR_H; ++o) {
+            double acc = b2[o];
+            for (int i = 0; i < OR_H; ++i) acc += (double)w2[o * OR_H + i] * h1[i];
+            z2[o] = acc;
+            h2[o] = acc > 0 ? acc : 0;
+            out += (double)w3[o] * h2[o];
+        }
+        const double d = out - y[s];
+        L += d * d;
+        const double dout = 2.0 * d / n;
+        double dz2[OR_H];
+        for (int o = 0; o < OR_H; ++o) {
+            grad[2 * OR_H + OR_H * OR_H + OR_H + o] += dout * h2[o];  /* w3 */
+            dz2[o] = z2[o] > 0 ? dout * w3[o] : 0;
+            grad[2 * OR_H + OR_H * OR_H + o] += dz2[o];               /* b2 */
+            for (int i = 0; i < OR_H; ++i) grad[2 * OR_H + o * OR_H + i] += dz2[o] * h1[i];
+        }
+        grad[OR_NP - 1] += dout;                                        /* b3 */
+        for (int i = 0; i < OR_H; ++i) {
+            double dh = 0;
+            for (int o = 0; o < OR_H; ++o) dh += (double)w2[o * OR_H + i] * dz2[o];
+            const double dz1 = z1[i] > 0 ? dh : 0;
+            grad[i] += dz1 * x[s];                                      /* w1 */
+            grad[OR_H + i] += dz1;                                      /* b1 */
+        }
+    }
+    *loss = L / n;
+}
+
+/* The query-time inference in single precision, operation for operation as
+ * the device evaluates it (fused multiply-adds in the same order). */
+static float or_mlp_root(const float *P, float x) {
+    const float *w1 = P, *b1 = P + OR_H, *w2 = P + 2 * OR_H, *b2 = w2 + OR_H * OR_H, *w3 = b2 + OR_H, *b3 = w3 + OR_H;
+    float h1[OR_H];
+    for (int i = 0; i < OR_H; ++i) h1[i] = fmaxf(fmaf(w1[i], x, b1[i]), 0.0f);
+    float out = b3[0];
+    for (int o = 0; o < OR_H; ++o) {
+        float acc = b2[o];
+        for (int i = 0; i < OR_H; ++i) acc = fmaf(w2[o * OR_H + i], h1[i], acc);
+        out = fmaf(w3[o], fmaxf(acc, 0.0f), out);
+    }
+    return out;
+}
+
+/* Leaf of each key as the network routes it (single-precision restatement). */
+void or_model_leaves(const float *P, float kmin, float kscale, uint32_t nleaves, const uint32_t *keys, uint64_t n,
+                     uint32_t *out) {
+    for (uint64_t p = 0; p < n; ++p) {
+        volatile float xs = (float)keys[p] - kmin;
+        const float x = xs * kscale;
+        volatile float f = or_mlp_root(P, x) * (float)nleaves;
+        int li = (int)floorf(f);
+        if (li < 0) li = 0;
+        if (li >= (int)nleaves) li = (int)nleaves - 1;
+        out[p] = (uint32_t)li;
+    }
+}
+
+/* For every key of a sorted list: its leaf and whether its rank lies inside
+ * the leaf's window. leaves: 4 x 32-bit per leaf {a, b, elo, ehi}. Returns the
+ * number of keys outside their window (0 when the model is exact) and fills
+ * per-leaf key counts if counts != NULL. */
+uint64_t or_model_check(const float *P, float kmin, float kscale, uint32_t nleaves, const int32_t *leaves,
+                        const uint32_t *keys, uint64_t n, uint32_t *counts) {
+    uint64_t bad = 0;
+    for (uint64_t p = 0; p < n; ++p) {
+        volatile float xs = (float)keys[p] - kmin;
+        const float x = xs * kscale;
+        const float r = or_mlp_root(P, x);
+        volatile float f = r * (float)nleaves;
+        int li = (int)floorf(f);
+        if (li < 0) li = 0;
+        if (li >= (int)nleaves) li = (int)nleaves - 1;
+        float a, b;
+        memcpy(&a, &leaves[4 * li], 4);
+        memcpy(&b, &leaves[4 * li + 1], 4);
+        float pr = fmaf(a, x, b);
+        pr = fminf(fmaxf(pr, -1.0e9f), 1.0e9f);
+        const int64_t pred = (int64_t)floorf(pr);
+        const int64_t lo = pred + leaves[4 * li + 2], hi = pred + leaves[4 * li + 3];
+        if ((int64_t)p < lo || (int64_t)p > hi) ++bad;
+        if (counts) ++counts[li];
+    }
+    return bad;
+}
+
+/* ---------------------------------------------------------------------------
  * CPU path over the compressed index image (the layout libexcl_gpu exports:
  * per list {codec, n, seg_base, nseg, word_base, reg[4]}, per segment head,
  * rec {start, off, aux, count}, reg {a, b, L, R}). Per query: decode the
