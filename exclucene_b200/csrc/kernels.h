@@ -13,7 +13,8 @@ struct BatchView {
     const uint32_t *qterms;      // nq * kMaxTerms list ids, ascending length
     const uint32_t *qnterms;     // terms per query
     const uint32_t *tile_prefix; // nq + 1, exclusive prefix of tiles per query
-    uint32_t *tile_counter;      // work-queue head (zeroed by k_pack)
+    uint32_t *tile_q;            // max_tiles, query owning each tile
+    uint32_t *tile_counter;      // work-queue head (zeroed by k_pack_scan)
     const uint32_t *key_base;    // nq + 1, exclusive prefix of shortest-list lengths
     uint32_t *tile_count;        // survivors per tile
     uint32_t *tile_slot;         // scratch position of each tile's survivors
@@ -24,16 +25,29 @@ struct BatchView {
     uint64_t *stats;             // [probes, fallbacks] or null
 };
 
+// pipeline.cu
+constexpr uint32_t kPackThreads = 256;
+constexpr uint32_t kPackMaxCtas = 256;
+constexpr uint32_t kPackMaxQueries = kPackThreads * kPackMaxCtas;
+constexpr uint32_t kSSThreads = 256;
+constexpr uint32_t kSSChunk = 512;
+
+// Cross-CTA state of k_pack_scan (zero between batches; the kernel leaves it so).
+struct PackSync {
+    uint32_t done;
+    uint32_t flag[kPackMaxCtas];
+    uint32_t agg_t[kPackMaxCtas];
+    uint32_t agg_k[kPackMaxCtas];
+};
+
+int launch_pack_scan(const ListDesc *lists, uint32_t nlists, const uint32_t *terms, const uint32_t *toff, uint32_t nq,
+                     const BatchView &b, PackSync *sync, cudaStream_t st);
+int launch_scan_scatter(const BatchView &b, uint32_t *tile_out, uint32_t *chunk_agg, uint32_t *offsets,
+                        uint32_t *docids, uint64_t cap, int nsm, cudaStream_t st);
+
 int launch_decode(const DevIndexView &ix, uint32_t l0, uint32_t l1, uint64_t out_base0, uint32_t *out, uint32_t seg0,
                   uint32_t nsegs, int nsm, uint32_t *err, cudaStream_t st);
-int launch_pack(const ListDesc *lists, uint32_t nlists, const uint32_t *terms, const uint32_t *toff, uint32_t nq,
-                const BatchView &b, uint32_t *ntiles, uint32_t *nkeys, cudaStream_t st);
-uint32_t scan_blocks_for(uint64_t n);
-int launch_scan(const uint32_t *in, uint32_t *out, const uint32_t *n_dev, uint32_t n_host, uint64_t max_n,
-                uint64_t *state, uint32_t *ticket, uint32_t *err, cudaStream_t st);
 int launch_probe(const DevIndexView &ix, const BatchView &b, int algo, int warps, int ctas_per_sm, int nsm,
                  cudaStream_t st);
-int launch_scatter(const BatchView &b, const uint32_t *tile_out, uint32_t *offsets, uint32_t *docids, uint64_t cap,
-                   int nsm, cudaStream_t st);
 
 }  // namespace excl

@@ -7,12 +7,12 @@
 // every allocation, or an embedding that cannot create a context (an
 // excl_ctx reserves its batch buffers with cudaMalloc). This entry point runs
 // the same kernels as excl_intersect_device, but all of its per-batch scratch
-// (sorted query terms, tile and key prefixes, per-tile counts, survivor slots,
-// scan state, error flag) lives in one file-scope device array of fixed size.
+// (sorted query terms, tile and key prefixes, tile owners, per-tile counts,
+// survivor slots, scan state, error flag) lives in one file-scope device array of fixed size.
 //
 // Limits: at most EXCL_NOALLOC_MAX_QUERIES queries per call and at most
 // EXCL_NOALLOC_MAX_KEYS docIDs summed over the queries' shortest lists. The
-// array takes 5,245,440 bytes (5.0 MiB) on every GPU that loads the library,
+// array takes 5,392,896 bytes (5.1 MiB) on every GPU that loads the library,
 // until the process exits.
 //
 // Sharing: every call uses the same array and it keeps the last call's
@@ -32,28 +32,28 @@ namespace {
 
 constexpr uint32_t kNAQueries = EXCL_NOALLOC_MAX_QUERIES;
 constexpr uint32_t kNAKeys = EXCL_NOALLOC_MAX_KEYS;
-constexpr uint32_t kNATiles = kNAKeys / kMinBlock + kNAQueries + 1;
-constexpr uint32_t kScanItemsPerBlock = 2048;  // k_scan_excl tile
-constexpr uint32_t kNAScanBlocks = (kNATiles + 1 + kScanItemsPerBlock - 1) / kScanItemsPerBlock;
+constexpr uint32_t kNATiles = kNAKeys / kMinBlock + kNAQueries + 1;  // bound as in ctx_alloc_batch
 
 constexpr uint64_t up64(uint64_t w) { return (w + 63) & ~63ull; }  // regions start on 256-byte boundaries
 
 // word offsets of the regions inside the array
 constexpr uint64_t kOffQterms = 0;
 constexpr uint64_t kOffQnterms = kOffQterms + up64((uint64_t)kNAQueries * kMaxTerms);
-constexpr uint64_t kOffNtiles = kOffQnterms + up64(kNAQueries);
-constexpr uint64_t kOffNkeys = kOffNtiles + up64(kNAQueries + 1);
-constexpr uint64_t kOffTilePrefix = kOffNkeys + up64(kNAQueries + 1);
+constexpr uint64_t kOffSync = kOffQnterms + up64(kNAQueries);        // PackSync
+constexpr uint64_t kOffChunkAgg = kOffSync + up64(kNAQueries + 1);   // per-chunk survivor sums
+constexpr uint64_t kOffTilePrefix = kOffChunkAgg + up64(kNAQueries + 1);
 constexpr uint64_t kOffKeyBase = kOffTilePrefix + up64(kNAQueries + 2);
-constexpr uint64_t kOffTileCount = kOffKeyBase + up64(kNAQueries + 2);
+constexpr uint64_t kOffTileQ = kOffKeyBase + up64(kNAQueries + 2);
+constexpr uint64_t kOffTileCount = kOffTileQ + up64(kNATiles + 1);
 constexpr uint64_t kOffTileSlot = kOffTileCount + up64(kNATiles + 1);
 constexpr uint64_t kOffTileOut = kOffTileSlot + up64(kNATiles + 1);
 constexpr uint64_t kOffSurvivors = kOffTileOut + up64(kNATiles + 2);
 constexpr uint64_t kOffMisc = kOffSurvivors + up64(kNAKeys);
 constexpr uint64_t kOffStats = kOffMisc + 64;           // 3 x u64 counters
-constexpr uint64_t kOffScanState = kOffStats + 64;      // kNAScanBlocks x u64
-constexpr uint64_t kWords = kOffScanState + up64(2ull * kNAScanBlocks);
-static_assert(kWords * 4 == 5245440, "scratch size stated in the comments and excl_gpu.h");
+constexpr uint64_t kWords = kOffStats + 64;
+static_assert(sizeof(PackSync) <= 4 * (kOffChunkAgg - kOffSync), "pack state region");
+static_assert(kNATiles / kSSChunk + 2 <= kOffTilePrefix - kOffChunkAgg, "chunk sum region");
+static_assert(kWords * 4 == 5392896, "scratch size stated in the comments and excl_gpu.h");
 
 static __device__ __align__(256) uint32_t g_noalloc_scratch[kWords];
 
@@ -68,11 +68,12 @@ int g_nsm[kMaxDevices];
 int setup_device(int dev, uint32_t **base, int *nsm) {
     std::lock_guard<std::mutex> g(g_mu);
     if (!g_base[dev]) {
-        // the look-back scan must fit its per-block state in the region above
-        if (scan_blocks_for((uint64_t)kNATiles + 1) > kNAScanBlocks) return EXCL_E_CAPACITY;
         void *p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess || !p) return EXCL_E_CUDA;
+        // the batch pipeline expects its cross-CTA state zeroed (it leaves it so)
+        e = cudaMemset(static_cast<uint32_t *>(p) + kOffSync, 0, sizeof(PackSync));
+        if (e != cudaSuccess) return EXCL_E_CUDA;
         int n = 0;
         e = cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
         if (e != cudaSuccess) return EXCL_E_CUDA;
@@ -109,6 +110,7 @@ extern "C" int excl_intersect_device_noalloc(excl_index *ix, const uint32_t *d_t
     b.qterms = base + kOffQterms;
     b.qnterms = base + kOffQnterms;
     b.tile_prefix = base + kOffTilePrefix;
+    b.tile_q = base + kOffTileQ;
     b.tile_counter = base + kOffMisc + 1;
     b.key_base = base + kOffKeyBase;
     b.tile_count = base + kOffTileCount;
@@ -118,20 +120,15 @@ extern "C" int excl_intersect_device_noalloc(excl_index *ix, const uint32_t *d_t
     b.max_keys = kNAKeys;
     b.err = base + kOffMisc;
     b.stats = reinterpret_cast<uint64_t *>(base + kOffStats);
-    uint32_t *ntiles = base + kOffNtiles, *nkeys = base + kOffNkeys, *tile_out = base + kOffTileOut;
-    uint64_t *scan_state = reinterpret_cast<uint64_t *>(base + kOffScanState);
-    uint32_t *ticket = base + kOffMisc + 2;
+    uint32_t *tile_out = base + kOffTileOut;
     const DevIndexView ixv = ix->dev->view(ix->models ? model_view(ix->models) : ModelView{});
 
     int e = 0;
-    e |= (int)cudaMemsetAsync(base + kOffMisc, 0, 64 * 4, st);   // error flag, work counter, tickets
-    e |= (int)cudaMemsetAsync(base + kOffStats, 0, 64 * 4, st);
-    e |= launch_pack(ix->dev->lists, ix->nlists, d_terms, d_term_offsets, nq, b, ntiles, nkeys, st);
-    e |= launch_scan(ntiles, base + kOffTilePrefix, nullptr, nq, kNAQueries, scan_state, ticket, b.err, st);
-    e |= launch_scan(nkeys, base + kOffKeyBase, nullptr, nq, kNAQueries, scan_state, ticket, b.err, st);
+    e |= (int)cudaMemsetAsync(base + kOffMisc, 0, 64 * 4, st);   // error flag, work counter
+    e |= launch_pack_scan(ix->dev->lists, ix->nlists, d_terms, d_term_offsets, nq, b,
+                          reinterpret_cast<PackSync *>(base + kOffSync), st);
     e |= launch_probe(ixv, b, (int)algo, 8, 4, nsm, st);
-    e |= launch_scan(b.tile_count, tile_out, base + kOffTilePrefix + nq, 0, kNATiles, scan_state, ticket, b.err, st);
-    e |= launch_scatter(b, tile_out, d_offsets, d_docids, cap, nsm, st);
+    e |= launch_scan_scatter(b, tile_out, base + kOffChunkAgg, d_offsets, d_docids, cap, nsm, st);
     if (e) return EXCL_E_CUDA;
     // the device-side limits (keys, tiles, result capacity) surface here
     uint32_t flags = 0;

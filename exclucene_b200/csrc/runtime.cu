@@ -191,25 +191,25 @@ DevIndexView DeviceIndex::view(const ModelView &mv) const {
 int ctx_alloc_batch(excl_ctx *ctx) {
     const excl_ctx_config &c = ctx->cfg;
     // Tiles hold >= kMinBlock keys except where consecutive HS segments are
-    // grouped (>= 128 keys on average) or a list ends, so this bounds them.
+    // grouped (two neighbouring tiles always hold > 256 keys) or a list ends,
+    // so this bounds them; larger batches raise EXCL_E_CAPACITY.
     ctx->max_tiles = (uint32_t)std::min<uint64_t>(0xfffffff0ull, c.max_keys / kMinBlock + c.max_queries + 1);
     int st = 0;
     st |= dalloc(ctx, &ctx->d_terms, (size_t)c.max_queries * kMaxTerms, "alloc terms");
     st |= dalloc(ctx, &ctx->d_toff, (size_t)c.max_queries + 1, "alloc term offsets");
     st |= dalloc(ctx, &ctx->d_qterms, (size_t)c.max_queries * kMaxTerms, "alloc qterms");
     st |= dalloc(ctx, &ctx->d_qnterms, (size_t)c.max_queries, "alloc qnterms");
-    st |= dalloc(ctx, &ctx->d_ntiles, (size_t)c.max_queries + 1, "alloc ntiles");
-    st |= dalloc(ctx, &ctx->d_nkeys, (size_t)c.max_queries + 1, "alloc nkeys");
     st |= dalloc(ctx, &ctx->d_tile_prefix, (size_t)c.max_queries + 2, "alloc tile prefix");
     st |= dalloc(ctx, &ctx->d_key_base, (size_t)c.max_queries + 2, "alloc key base");
+    st |= dalloc(ctx, &ctx->d_tile_q, (size_t)ctx->max_tiles + 1, "alloc tile owner");
     st |= dalloc(ctx, &ctx->d_tile_count, (size_t)ctx->max_tiles + 1, "alloc tile count");
     st |= dalloc(ctx, &ctx->d_tile_slot, (size_t)ctx->max_tiles + 1, "alloc tile slot");
     st |= dalloc(ctx, &ctx->d_tile_out, (size_t)ctx->max_tiles + 2, "alloc tile out");
     st |= dalloc(ctx, &ctx->d_scratch, (size_t)c.max_keys, "alloc scratch");
     st |= dalloc(ctx, &ctx->d_misc, 16, "alloc misc");
     st |= dalloc(ctx, &ctx->d_stats, 4, "alloc stats");
-    const uint32_t nsb = std::max(scan_blocks_for(c.max_queries + 1), scan_blocks_for(ctx->max_tiles + 1));
-    st |= dalloc(ctx, &ctx->d_scan_state, nsb, "alloc scan state");
+    st |= dalloc(ctx, &ctx->d_sync, 1, "alloc pack sync");
+    st |= dalloc(ctx, &ctx->d_chunk_agg, (size_t)ctx->max_tiles / kSSChunk + 2, "alloc chunk sums");
     st |= dalloc(ctx, &ctx->d_offsets, (size_t)c.max_queries + 1, "alloc offsets");
     ctx->docids_cap = c.max_keys;
     st |= dalloc(ctx, &ctx->d_docids, ctx->docids_cap, "alloc docids");
@@ -219,6 +219,7 @@ int ctx_alloc_batch(excl_ctx *ctx) {
     if (st) return EXCL_E_NOMEM;
     cudaMemsetAsync(ctx->d_misc, 0, 16 * 4, ctx->stream);
     cudaMemsetAsync(ctx->d_stats, 0, 4 * 8, ctx->stream);
+    cudaMemsetAsync(ctx->d_sync, 0, sizeof(PackSync), ctx->stream);
     return cuda_status(ctx, cudaStreamSynchronize(ctx->stream), "ctx init");
 }
 
@@ -243,6 +244,7 @@ int run_pipeline(excl_ctx *ctx, excl_index *ix, const uint32_t *d_terms, const u
     b.qterms = ctx->d_qterms;
     b.qnterms = ctx->d_qnterms;
     b.tile_prefix = ctx->d_tile_prefix;
+    b.tile_q = ctx->d_tile_q;
     b.tile_counter = ctx->d_misc + kMiscTileCounter;
     b.key_base = ctx->d_key_base;
     b.tile_count = ctx->d_tile_count;
@@ -253,20 +255,13 @@ int run_pipeline(excl_ctx *ctx, excl_index *ix, const uint32_t *d_terms, const u
     b.err = ctx->d_misc + kMiscErr;
     b.stats = ctx->collect_stats ? ctx->d_stats : nullptr;
     const DevIndexView ixv = ix->dev->view(ix->models ? model_view(ix->models) : ModelView{});
-    if (ctx->collect_stats) cudaMemsetAsync(ctx->d_stats, 0, 3 * 8, st);
     cudaEventRecord(ctx->ev[0], st);
     int e = 0;
-    e |= launch_pack(ix->dev->lists, ix->nlists, d_terms, d_toff, nq, b, ctx->d_ntiles, ctx->d_nkeys, st);
-    e |= launch_scan(ctx->d_ntiles, ctx->d_tile_prefix, nullptr, nq, ctx->cfg.max_queries, ctx->d_scan_state,
-                     ctx->d_misc + kMiscTicket0, b.err, st);
-    e |= launch_scan(ctx->d_nkeys, ctx->d_key_base, nullptr, nq, ctx->cfg.max_queries, ctx->d_scan_state,
-                     ctx->d_misc + kMiscTicket0, b.err, st);
+    e |= launch_pack_scan(ix->dev->lists, ix->nlists, d_terms, d_toff, nq, b, ctx->d_sync, st);
     cudaEventRecord(ctx->ev[1], st);
     e |= launch_probe(ixv, b, (int)algo, ctx->warps, ctx->ctas_per_sm, ctx->nsm, st);
     cudaEventRecord(ctx->ev[2], st);
-    e |= launch_scan(ctx->d_tile_count, ctx->d_tile_out, ctx->d_tile_prefix + nq, 0, ctx->max_tiles,
-                     ctx->d_scan_state, ctx->d_misc + kMiscTicket1, b.err, st);
-    e |= launch_scatter(b, ctx->d_tile_out, d_offsets, d_docids, cap, ctx->nsm, st);
+    e |= launch_scan_scatter(b, ctx->d_tile_out, ctx->d_chunk_agg, d_offsets, d_docids, cap, ctx->nsm, st);
     cudaEventRecord(ctx->ev[3], st);
     if (e) return cuda_status(ctx, (cudaError_t)e, "launch");
     ctx->last_nq = nq;
@@ -299,12 +294,12 @@ extern "C" int excl_ctx_create(int device, const excl_ctx_config *cfg, excl_ctx 
     ctx->device = device;
     excl_ctx_config c{};
     if (cfg) c = *cfg;
-    if (c.max_queries == 0) c.max_queries = 65536;
+    if (c.max_queries == 0 || c.max_queries > kPackMaxQueries) c.max_queries = kPackMaxQueries;
     if (c.max_terms == 0 || c.max_terms > kMaxTerms) c.max_terms = kMaxTerms;
     if (c.max_keys == 0) c.max_keys = 1ull << 26;
     ctx->cfg = c;
     ctx->warps = c.warps_per_cta ? (int)c.warps_per_cta : 8;
-    ctx->ctas_per_sm = c.ctas_per_sm ? (int)c.ctas_per_sm : 4;
+    ctx->ctas_per_sm = c.ctas_per_sm ? (int)c.ctas_per_sm : 8;
     int st = cuda_status(ctx, cudaSetDevice(device), "cudaSetDevice");
     if (!st) st = cuda_status(ctx, cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, device), "attr");
     if (!st) st = cuda_status(ctx, cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking), "stream");
@@ -323,13 +318,14 @@ extern "C" int excl_ctx_destroy(excl_ctx *ctx) {
     if (!ctx) return EXCL_E_INVALID;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-    uint32_t *bufs[] = {ctx->d_terms,      ctx->d_toff,     ctx->d_qterms, ctx->d_qnterms, ctx->d_ntiles,
-                        ctx->d_tile_prefix, ctx->d_tile_count, ctx->d_tile_out, ctx->d_scratch, ctx->d_misc,
-                        ctx->d_nkeys,      ctx->d_key_base, ctx->d_tile_slot,
+    uint32_t *bufs[] = {ctx->d_terms,      ctx->d_toff,      ctx->d_qterms,     ctx->d_qnterms,
+                        ctx->d_tile_prefix, ctx->d_tile_q,    ctx->d_tile_count, ctx->d_tile_out,
+                        ctx->d_scratch,    ctx->d_misc,      ctx->d_key_base,   ctx->d_tile_slot,
                         ctx->d_offsets,    ctx->d_docids};
     for (uint32_t *p : bufs) cudaFree(p);
     cudaFree(ctx->d_stats);
-    cudaFree(ctx->d_scan_state);
+    cudaFree(ctx->d_sync);
+    cudaFree(ctx->d_chunk_agg);
     cudaFreeHost(ctx->h_terms);
     cudaFreeHost(ctx->h_toff);
     cudaFreeHost(ctx->h_offsets);

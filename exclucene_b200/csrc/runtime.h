@@ -6,6 +6,7 @@
 #include <string>
 
 #include "excl_device.cuh"
+#include "kernels.h"
 
 namespace excl {
 
@@ -45,10 +46,11 @@ struct excl_ctx {
     uint32_t max_tiles = 0;
     uint32_t last_nq = 0;
     uint32_t *d_terms = nullptr, *d_toff = nullptr;
-    uint32_t *d_qterms = nullptr, *d_qnterms = nullptr, *d_ntiles = nullptr, *d_tile_prefix = nullptr;
+    uint32_t *d_qterms = nullptr, *d_qnterms = nullptr, *d_tile_prefix = nullptr, *d_tile_q = nullptr;
     uint32_t *d_tile_count = nullptr, *d_tile_out = nullptr, *d_scratch = nullptr, *d_misc = nullptr;
-    uint32_t *d_nkeys = nullptr, *d_key_base = nullptr, *d_tile_slot = nullptr;
-    uint64_t *d_stats = nullptr, *d_scan_state = nullptr;
+    uint32_t *d_key_base = nullptr, *d_tile_slot = nullptr, *d_chunk_agg = nullptr;
+    excl::PackSync *d_sync = nullptr;
+    uint64_t *d_stats = nullptr;
     uint32_t *d_offsets = nullptr, *d_docids = nullptr;
     uint64_t docids_cap = 0;
     uint32_t *h_terms = nullptr, *h_toff = nullptr, *h_offsets = nullptr;
