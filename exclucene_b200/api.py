@@ -418,7 +418,7 @@ def library_path() -> str:
 # Allocation-free form of Context.intersect_device, for callers that cannot
 # allocate device memory when they query (their budget is fixed at start-up,
 # or they run without a Context, whose creation allocates the batch buffers).
-# Its scratch is a fixed 5.1 MiB device array inside the library, shared by
+# Its scratch is a fixed 5.0 MiB device array inside the library, shared by
 # all calls: calls that overlap on the GPU race. The first call on a device
 # looks the array up; make it before any stream capture.
 
@@ -434,3 +434,98 @@ def intersect_device_noalloc(ix: Index, d_terms: int, d_toff: int, nq: int, algo
     a = ALGO_NAMES[algo] if isinstance(algo, str) else int(algo)
     _check_status(_isect_noalloc(ix._h, C.c_void_p(d_terms), C.c_void_p(d_toff), nq, a, C.c_void_p(d_offsets),
                                  C.c_void_p(d_docids), cap, C.c_void_p(stream)), what="excl_intersect_device_noalloc")
+
+
+# ---------------------------------------------------------------------------
+# Serving loop: continuous batching of single queries on a resident index.
+
+class ServerConfig(C.Structure):
+    _fields_ = [("slots", C.c_uint32), ("max_batch_queries", C.c_uint32), ("max_batch_keys", C.c_uint64),
+                ("hbm_budget_bytes", C.c_uint64), ("algo", C.c_uint32), ("warps_per_cta", C.c_uint32),
+                ("ctas_per_sm", C.c_uint32)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("batches", C.c_uint64),
+                ("rejected", C.c_uint64), ("mean_batch", C.c_double), ("pool_bytes", C.c_uint64),
+                ("pool_peak_bytes", C.c_uint64), ("max_inflight", C.c_uint32), ("p50_us", C.c_double),
+                ("p99_us", C.c_double), ("max_us", C.c_double)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_srv_create = _sig("excl_server_create", C.c_int, C.c_int, C.c_void_p, C.POINTER(ServerConfig),
+                   C.POINTER(C.c_void_p))
+_srv_destroy = _sig("excl_server_destroy", C.c_int, C.c_void_p)
+_srv_submit = _sig("excl_server_submit", C.c_int, C.c_void_p, u32p, C.c_uint32, C.POINTER(C.c_uint64))
+_srv_wait = _sig("excl_server_wait", C.c_int, C.c_void_p, C.c_uint64, u32p, C.c_size_t, C.POINTER(C.c_uint32),
+                 C.c_int)
+_srv_stats = _sig("excl_server_stats_get", C.c_int, C.c_void_p, C.POINTER(ServerStats))
+_srv_reset = _sig("excl_server_stats_reset", C.c_int, C.c_void_p)
+_srv_replay = _sig("excl_server_replay", C.c_int, C.c_void_p, u32p, u32p, C.c_uint32, C.POINTER(C.c_double),
+                   C.POINTER(C.c_double), C.POINTER(C.c_uint64 * 3), C.POINTER(C.c_double))
+EXPORTED += ["excl_server_create", "excl_server_destroy", "excl_server_submit", "excl_server_wait",
+             "excl_server_stats_get", "excl_server_stats_reset", "excl_server_replay",
+             "excl_intersect_device_noalloc"]
+
+
+class Server:
+    """Continuous-batching server over an index uploaded to `device`."""
+
+    def __init__(self, ix: Index, device: int = 0, slots: int = 4, max_batch_queries: int = 4096,
+                 max_batch_keys: int = 1 << 22, hbm_budget_bytes: int = 0, algo="auto", warps_per_cta: int = 0,
+                 ctas_per_sm: int = 0):
+        self._h = None
+        self._ix = ix  # the server reads the index; keep it alive
+        a = ALGO_NAMES[algo] if isinstance(algo, str) else int(algo)
+        cfg = ServerConfig(slots, max_batch_queries, max_batch_keys, hbm_budget_bytes, a, warps_per_cta, ctas_per_sm)
+        h = C.c_void_p()
+        _check_status(_srv_create(device, ix._h, C.byref(cfg), C.byref(h)), what="excl_server_create")
+        self._h = h
+
+    def submit(self, terms) -> int:
+        t = _u32(terms) if len(terms) else np.zeros(1, dtype=np.uint32)
+        tk = C.c_uint64()
+        _check_status(_srv_submit(self._h, _p32(t), len(terms), C.byref(tk)), what="excl_server_submit")
+        return int(tk.value)
+
+    def wait(self, ticket: int, cap: int = 1 << 20, timeout_ms: int = -1) -> np.ndarray:
+        out = np.zeros(max(cap, 1), dtype=np.uint32)
+        n = C.c_uint32()
+        _check_status(_srv_wait(self._h, ticket, _p32(out), cap, C.byref(n), timeout_ms), what="excl_server_wait")
+        return out[: n.value].copy()
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        _check_status(_srv_stats(self._h, C.byref(st)))
+        return st.as_dict()
+
+    def reset_stats(self) -> None:
+        _check_status(_srv_reset(self._h))
+
+    def replay(self, terms, term_offsets, arrival_s) -> tuple[np.ndarray, tuple[int, int, int], float]:
+        """Open-loop load: query q is submitted arrival_s[q] s after the start.
+        Returns per-query latencies (s), the checksum triple and the wall time."""
+        t = _u32(terms) if len(terms) else np.zeros(1, dtype=np.uint32)
+        o = _u32(term_offsets)
+        nq = len(o) - 1
+        arr = np.ascontiguousarray(arrival_s, dtype=np.float64)
+        lat = np.zeros(max(nq, 1), dtype=np.float64)
+        cs = (C.c_uint64 * 3)()
+        wall = C.c_double()
+        dp = C.POINTER(C.c_double)
+        _check_status(_srv_replay(self._h, _p32(t), _p32(o), nq, arr.ctypes.data_as(dp), lat.ctypes.data_as(dp),
+                                  C.byref(cs), C.byref(wall)), what="excl_server_replay")
+        return lat[:nq], (int(cs[0]), int(cs[1]), int(cs[2])), float(wall.value)
+
+    def close(self) -> None:
+        if self._h:
+            _srv_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -25,7 +25,8 @@ NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", *ARCH, "-Xcompiler", "-fPIC,-ffp
               "--expt-relaxed-constexpr", f"-I{INCLUDE}"]
 CXX_FLAGS = ["-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-pthread", f"-I{INCLUDE}"]
 
-GPU_SOURCES = ["codec.cpp", "kernels.cu", "pipeline.cu", "decode.cu", "runtime.cu", "learned_train.cu", "noalloc.cu"]
+GPU_SOURCES = ["codec.cpp", "kernels.cu", "pipeline.cu", "decode.cu", "runtime.cu", "learned_train.cu", "noalloc.cu",
+               "serve.cu"]
 GPU_HEADERS = ["excl_internal.h", "excl_device.cuh", "kernels.h", "runtime.h"]
 SYNTH_SOURCES = ["synth.cpp"]
 

@@ -32,18 +32,35 @@ constexpr uint32_t kPackMaxQueries = kPackThreads * kPackMaxCtas;
 constexpr uint32_t kSSThreads = 256;
 constexpr uint32_t kSSChunk = 512;
 
-// Cross-CTA state of k_pack_scan (zero between batches; the kernel leaves it so).
+// Cross-CTA state of one stream's batches (zeroed once at allocation; the
+// kernels tag what they publish with the batch, so it is never cleared).
 struct PackSync {
-    uint32_t done;
+    uint32_t epoch;           // tag of the last batch packed on this state
+    uint32_t ticket, done;    // k_pack_scan: CTA order, CTAs finished
+    uint32_t sticket, sdone;  // k_scatter: chunk order, CTAs finished
     uint32_t flag[kPackMaxCtas];
     uint32_t agg_t[kPackMaxCtas];
     uint32_t agg_k[kPackMaxCtas];
 };
 
-int launch_pack_scan(const ListDesc *lists, uint32_t nlists, const uint32_t *terms, const uint32_t *toff, uint32_t nq,
-                     const BatchView &b, PackSync *sync, cudaStream_t st);
-int launch_scan_scatter(const BatchView &b, uint32_t *tile_out, uint32_t *chunk_agg, uint32_t *offsets,
-                        uint32_t *docids, uint64_t cap, int nsm, cudaStream_t st);
+// Everything one batch launch needs.
+struct BatchLaunch {
+    DevIndexView ixv;
+    const ListDesc *lists;
+    uint32_t nlists;
+    const uint32_t *terms, *toff;  // the batch's queries (device or host-mapped)
+    BatchView b;
+    PackSync *sync;
+    uint64_t *chunk_state;  // max_tiles / kSSChunk + 1 words
+    uint32_t *offsets;      // nq + 1
+    uint32_t *docids;       // cap
+    uint64_t cap;
+    int algo, warps, ctas_per_sm, nsm;
+    cudaEvent_t *ev;  // 4 events around the three kernels, or null
+};
+
+// pack -> probe -> scatter on `st`.
+int launch_batch(const BatchLaunch &L, cudaStream_t st);
 
 int launch_decode(const DevIndexView &ix, uint32_t l0, uint32_t l1, uint64_t out_base0, uint32_t *out, uint32_t seg0,
                   uint32_t nsegs, int nsm, uint32_t *err, cudaStream_t st);

@@ -12,7 +12,7 @@
 //
 // Limits: at most EXCL_NOALLOC_MAX_QUERIES queries per call and at most
 // EXCL_NOALLOC_MAX_KEYS docIDs summed over the queries' shortest lists. The
-// array takes 5,392,896 bytes (5.1 MiB) on every GPU that loads the library,
+// array takes 5,245,184 bytes (5.0 MiB) on every GPU that loads the library,
 // until the process exits.
 //
 // Sharing: every call uses the same array and it keeps the last call's
@@ -40,20 +40,19 @@ constexpr uint64_t up64(uint64_t w) { return (w + 63) & ~63ull; }  // regions st
 constexpr uint64_t kOffQterms = 0;
 constexpr uint64_t kOffQnterms = kOffQterms + up64((uint64_t)kNAQueries * kMaxTerms);
 constexpr uint64_t kOffSync = kOffQnterms + up64(kNAQueries);        // PackSync
-constexpr uint64_t kOffChunkAgg = kOffSync + up64(kNAQueries + 1);   // per-chunk survivor sums
-constexpr uint64_t kOffTilePrefix = kOffChunkAgg + up64(kNAQueries + 1);
+constexpr uint64_t kOffChunkState = kOffSync + up64(kNAQueries + 1);  // u64 look-back state per chunk
+constexpr uint64_t kOffTilePrefix = kOffChunkState + up64(kNAQueries + 1);
 constexpr uint64_t kOffKeyBase = kOffTilePrefix + up64(kNAQueries + 2);
 constexpr uint64_t kOffTileQ = kOffKeyBase + up64(kNAQueries + 2);
 constexpr uint64_t kOffTileCount = kOffTileQ + up64(kNATiles + 1);
 constexpr uint64_t kOffTileSlot = kOffTileCount + up64(kNATiles + 1);
-constexpr uint64_t kOffTileOut = kOffTileSlot + up64(kNATiles + 1);
-constexpr uint64_t kOffSurvivors = kOffTileOut + up64(kNATiles + 2);
+constexpr uint64_t kOffSurvivors = kOffTileSlot + up64(kNATiles + 1);
 constexpr uint64_t kOffMisc = kOffSurvivors + up64(kNAKeys);
 constexpr uint64_t kOffStats = kOffMisc + 64;           // 3 x u64 counters
 constexpr uint64_t kWords = kOffStats + 64;
-static_assert(sizeof(PackSync) <= 4 * (kOffChunkAgg - kOffSync), "pack state region");
-static_assert(kNATiles / kSSChunk + 2 <= kOffTilePrefix - kOffChunkAgg, "chunk sum region");
-static_assert(kWords * 4 == 5392896, "scratch size stated in the comments and excl_gpu.h");
+static_assert(sizeof(PackSync) <= 4 * (kOffChunkState - kOffSync), "pack state region");
+static_assert(2 * (kNATiles / kSSChunk + 2) <= kOffTilePrefix - kOffChunkState, "chunk state region");
+static_assert(kWords * 4 == 5245184, "scratch size stated in the comments and excl_gpu.h");
 
 static __device__ __align__(256) uint32_t g_noalloc_scratch[kWords];
 
@@ -71,8 +70,8 @@ int setup_device(int dev, uint32_t **base, int *nsm) {
         void *p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess || !p) return EXCL_E_CUDA;
-        // the batch pipeline expects its cross-CTA state zeroed (it leaves it so)
-        e = cudaMemset(static_cast<uint32_t *>(p) + kOffSync, 0, sizeof(PackSync));
+        // the batch pipeline's cross-CTA state starts zeroed (its tags start at 1)
+        e = cudaMemset(static_cast<uint32_t *>(p) + kOffSync, 0, 4 * (kOffTilePrefix - kOffSync));
         if (e != cudaSuccess) return EXCL_E_CUDA;
         int n = 0;
         e = cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
@@ -120,15 +119,26 @@ extern "C" int excl_intersect_device_noalloc(excl_index *ix, const uint32_t *d_t
     b.max_keys = kNAKeys;
     b.err = base + kOffMisc;
     b.stats = reinterpret_cast<uint64_t *>(base + kOffStats);
-    uint32_t *tile_out = base + kOffTileOut;
-    const DevIndexView ixv = ix->dev->view(ix->models ? model_view(ix->models) : ModelView{});
+    BatchLaunch L{};
+    L.ixv = ix->dev->view(ix->models ? model_view(ix->models) : ModelView{});
+    L.lists = ix->dev->lists;
+    L.nlists = ix->nlists;
+    L.terms = d_terms;
+    L.toff = d_term_offsets;
+    L.b = b;
+    L.sync = reinterpret_cast<PackSync *>(base + kOffSync);
+    L.chunk_state = reinterpret_cast<uint64_t *>(base + kOffChunkState);
+    L.offsets = d_offsets;
+    L.docids = d_docids;
+    L.cap = cap;
+    L.algo = (int)algo;
+    L.warps = 8;
+    L.ctas_per_sm = 8;
+    L.nsm = nsm;
+    L.ev = nullptr;
 
-    int e = 0;
-    e |= (int)cudaMemsetAsync(base + kOffMisc, 0, 64 * 4, st);   // error flag, work counter
-    e |= launch_pack_scan(ix->dev->lists, ix->nlists, d_terms, d_term_offsets, nq, b,
-                          reinterpret_cast<PackSync *>(base + kOffSync), st);
-    e |= launch_probe(ixv, b, (int)algo, 8, 4, nsm, st);
-    e |= launch_scan_scatter(b, tile_out, base + kOffChunkAgg, d_offsets, d_docids, cap, nsm, st);
+    int e = (int)cudaMemsetAsync(base + kOffMisc, 0, 64 * 4, st);  // error flag
+    e |= launch_batch(L, st);
     if (e) return EXCL_E_CUDA;
     // the device-side limits (keys, tiles, result capacity) surface here
     uint32_t flags = 0;

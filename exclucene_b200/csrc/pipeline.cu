@@ -1,24 +1,28 @@
-// The batch pipeline's bookkeeping kernels, fused so a batch is three launches
-// (k_pack_scan -> k_probe -> k_scan_scatter) with no memsets in between.
+// The batch pipeline: three launches per batch, no memsets, no host sync.
 //
-//   k_pack_scan     per query: sort the terms by list length (stable insertion
-//                   sort, ParaPFD_Intersection.cu:155-173), count the shortest
-//                   list's tiles and docIDs; then the exclusive prefixes of both
-//                   over the batch. The <= 256 CTAs publish their totals with
-//                   release/acquire flags and each sums its predecessors'; the
-//                   last CTA to finish clears the flags for the next batch.
-//                   Also resets the probe's work counter and statistics.
-//   k_scan_scatter  cooperative: per-chunk sums of the per-tile survivor
-//                   counts, grid sync, chunk prefixes and per-tile output
-//                   positions, survivors copied to the result array (replaces
-//                   cudppScan + saCompact, ParaPFD_Intersection.cu:262,279),
-//                   grid sync, per-query offsets (replaces ucntResult, :301).
-#include <cooperative_groups.h>
+//   k_pack_scan  per query: sort the terms by list length (stable insertion
+//                sort, ParaPFD_Intersection.cu:155-173), count the shortest
+//                list's tiles and docIDs; then the exclusive prefixes of both
+//                over the batch and the owner query of every tile. CTAs take
+//                their place in the scan from a ticket, so a CTA only waits
+//                on CTAs that are already running (decoupled look-back).
+//   k_probe      kernels.cu.
+//   k_scatter    single-pass decoupled look-back over chunks of 512 tiles:
+//                chunk survivor totals, their prefixes, each tile's output
+//                position and the per-query offsets (replaces cudppScan and
+//                ucntResult, ParaPFD_Intersection.cu:262,301); then every
+//                warp of the grid copies survivors to the result array
+//                (replaces saCompact, :279).
+//
+// Cross-CTA state (PackSync, chunk states) carries the batch's tag, so it
+// needs no clearing between batches; every wait is bounded and raises
+// kErrScanSpin when it gives up. Nothing here needs all CTAs to be resident,
+// so batches may run concurrently on several streams.
 #include <cuda_runtime.h>
 
-#include "kernels.h"
+#include <algorithm>
 
-namespace cg = cooperative_groups;
+#include "kernels.h"
 
 namespace excl {
 
@@ -30,8 +34,26 @@ __device__ __forceinline__ uint32_t ld_acquire(const uint32_t *p) {
     asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
+__device__ __forceinline__ void st_release64(uint64_t *p, uint64_t v) {
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ uint64_t ld_acquire64(const uint64_t *p) {
+    uint64_t v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
 
-constexpr uint32_t kSpin = 1u << 22;
+constexpr uint32_t kPackRegTerms = 8;  // queries with up to this many terms are sorted in registers
+constexpr uint32_t kSpin = 1u << 22;  // x >= 32 ns: a wait gives up after > 0.1 s
+
+// Batch tags cycle through 1 .. 2^30 - 1 (0 is the state of fresh memory).
+__device__ __forceinline__ uint32_t next_tag(uint32_t e) { return e >= (1u << 30) - 1u ? 1u : e + 1u; }
+
+// Chunk state of k_scatter: tag (30 bits) | status (2 bits) | value (32 bits).
+constexpr uint32_t kAggregate = 1u, kPrefix = 2u;
+__device__ __forceinline__ uint64_t chunk_word(uint32_t tag, uint32_t status, uint32_t v) {
+    return ((uint64_t)tag << 34) | ((uint64_t)status << 32) | v;
+}
 
 // Block-wide exclusive scan of two values at once; returns the block totals.
 __device__ __forceinline__ void block_scan2(uint32_t a, uint32_t b, uint32_t &ea, uint32_t &eb, uint32_t &ta,
@@ -78,13 +100,21 @@ __device__ __forceinline__ void block_scan2(uint32_t a, uint32_t b, uint32_t &ea
     tb = sb[32];
 }
 
+// ---------------------------------------------------------------------------
+
 __global__ void __launch_bounds__(kPackThreads) k_pack_scan(const ListDesc *__restrict__ lists, uint32_t nlists,
                                                             const uint32_t *__restrict__ terms,
                                                             const uint32_t *__restrict__ toff, uint32_t nq,
                                                             BatchView b, PackSync *__restrict__ sync) {
-    __shared__ uint32_t sa[33], sb[33], s_pre[2], s_et[kPackThreads];
+    __shared__ uint32_t sa[33], sb[33], s_pre[2], s_et[kPackThreads], s_id, s_tag;
     static_assert(kPackMaxCtas <= 32 * 8, "warp 0 reads up to 8 predecessors per lane");
-    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (threadIdx.x == 0) {
+        s_id = atomicAdd(&sync->ticket, 1u);
+        s_tag = next_tag(*(volatile uint32_t *)&sync->epoch);
+    }
+    __syncthreads();
+    const uint32_t bid = s_id, tag = s_tag;
+    const uint32_t q = bid * blockDim.x + threadIdx.x;
     uint32_t nt = 0, nk = 0;
     if (q < nq) {
         const uint32_t t0 = toff[q], t1 = toff[q + 1];
@@ -93,49 +123,93 @@ __global__ void __launch_bounds__(kPackThreads) k_pack_scan(const ListDesc *__re
             atomicOr(b.err, kErrTerms);
             k = 0;
         }
-        uint32_t id[kMaxTerms], len[kMaxTerms];
-        for (uint32_t i = 0; i < k; ++i) {
-            const uint32_t tid = terms[t0 + i];
-            if (tid >= nlists) {
+        uint32_t *dst = const_cast<uint32_t *>(b.qterms) + (size_t)q * kMaxTerms;
+        if (k <= kPackRegTerms) {
+            // common case: all in registers, every load of the query issued at once
+            uint32_t id[kPackRegTerms], len[kPackRegTerms], ntl[kPackRegTerms];
+            bool bad = false;
+#pragma unroll
+            for (uint32_t j = 0; j < kPackRegTerms; ++j) id[j] = j < k ? __ldg(terms + t0 + j) : 0u;
+#pragma unroll
+            for (uint32_t j = 0; j < kPackRegTerms; ++j) {
+                const bool v = j < k && id[j] < nlists;
+                bad |= j < k && id[j] >= nlists;
+                len[j] = v ? __ldg(&lists[id[j]].n) : 0xffffffffu;  // absent terms sort last
+                ntl[j] = v ? __ldg(&lists[id[j]].ntiles) : 0u;
+            }
+            if (bad) {
                 atomicOr(b.err, kErrTermId);
                 k = 0;
-                break;
             }
-            id[i] = tid;
-            len[i] = lists[tid].n;
-        }
-        for (uint32_t i = 1; i < k; ++i) {
-            const uint32_t ci = id[i], cl = len[i];
-            uint32_t j = i;
-            while (j && cl < len[j - 1]) {
-                id[j] = id[j - 1];
-                len[j] = len[j - 1];
-                --j;
+            // stable insertion sort by length with fixed indices (strict compare keeps input order on ties)
+#pragma unroll
+            for (uint32_t i = 1; i < kPackRegTerms; ++i)
+#pragma unroll
+                for (uint32_t j = i; j > 0; --j)
+                    if (len[j] < len[j - 1]) {
+                        uint32_t x = id[j]; id[j] = id[j - 1]; id[j - 1] = x;
+                        x = len[j]; len[j] = len[j - 1]; len[j - 1] = x;
+                        x = ntl[j]; ntl[j] = ntl[j - 1]; ntl[j - 1] = x;
+                    }
+#pragma unroll
+            for (uint32_t j = 0; j < kPackRegTerms; ++j)
+                if (j < k) dst[j] = id[j];
+            nt = k ? ntl[0] : 0u;
+            nk = k ? len[0] : 0u;
+        } else {
+            uint32_t id[kMaxTerms], len[kMaxTerms];
+            bool bad = false;
+            // loads in groups of four so their latencies overlap
+            for (uint32_t i0 = 0; i0 < k; i0 += 4) {
+#pragma unroll
+                for (uint32_t j = 0; j < 4; ++j)
+                    if (i0 + j < k) id[i0 + j] = __ldg(terms + t0 + i0 + j);
             }
-            id[j] = ci;
-            len[j] = cl;
+            for (uint32_t i0 = 0; i0 < k; i0 += 4) {
+#pragma unroll
+                for (uint32_t j = 0; j < 4; ++j)
+                    if (i0 + j < k) {
+                        const uint32_t tid = id[i0 + j];
+                        bad |= tid >= nlists;
+                        len[i0 + j] = tid < nlists ? __ldg(&lists[tid].n) : 0u;
+                    }
+            }
+            if (bad) {
+                atomicOr(b.err, kErrTermId);
+                k = 0;
+            }
+            for (uint32_t i = 1; i < k; ++i) {
+                const uint32_t ci = id[i], cl = len[i];
+                uint32_t j = i;
+                while (j && cl < len[j - 1]) {
+                    id[j] = id[j - 1];
+                    len[j] = len[j - 1];
+                    --j;
+                }
+                id[j] = ci;
+                len[j] = cl;
+            }
+            for (uint32_t i = 0; i < k; ++i) dst[i] = id[i];
+            nt = k ? __ldg(&lists[id[0]].ntiles) : 0u;
+            nk = k ? len[0] : 0u;
         }
-        uint32_t *dst = const_cast<uint32_t *>(b.qterms) + (size_t)q * kMaxTerms;
-        for (uint32_t i = 0; i < k; ++i) dst[i] = id[i];
         const_cast<uint32_t *>(b.qnterms)[q] = k;
-        nt = k ? lists[id[0]].ntiles : 0u;
-        nk = k ? len[0] : 0u;
     }
     uint32_t et, ek, bt, bk;
     block_scan2(nt, nk, et, ek, bt, bk, sa, sb);
-    const uint32_t bid = blockIdx.x;
     if (threadIdx.x == 0) {
         sync->agg_t[bid] = bt;
         sync->agg_k[bid] = bk;
-        st_release(&sync->flag[bid], 1u);
+        st_release(&sync->flag[bid], tag);
     }
     if (threadIdx.x < 32) {
-        // warp 0: the predecessors' totals, read in parallel (all CTAs are resident)
+        // warp 0: the predecessors' totals, read in parallel; every
+        // predecessor took its ticket earlier, so it is running or done
         const uint32_t lane = threadIdx.x;
         uint32_t pt = 0, pk = 0;
         for (uint32_t p = lane; p < bid; p += 32) {
             uint32_t spins = 0;
-            while (ld_acquire(&sync->flag[p]) == 0u) {
+            while (ld_acquire(&sync->flag[p]) != tag) {
                 if (++spins > kSpin) {
                     atomicOr(b.err, kErrScanSpin);
                     break;
@@ -155,8 +229,11 @@ __global__ void __launch_bounds__(kPackThreads) k_pack_scan(const ListDesc *__re
             s_pre[1] = pk;
         }
     }
+    s_et[threadIdx.x] = et;
+    __syncthreads();
+    const uint32_t pt = s_pre[0];
     if (threadIdx.x == 0) {
-        const uint32_t pt = s_pre[0], pk = s_pre[1];
+        const uint32_t pk = s_pre[1];
         if (bid == gridDim.x - 1) {
             const_cast<uint32_t *>(b.tile_prefix)[nq] = pt + bt;
             const_cast<uint32_t *>(b.key_base)[nq] = pk + bk;
@@ -166,17 +243,15 @@ __global__ void __launch_bounds__(kPackThreads) k_pack_scan(const ListDesc *__re
             *b.tile_counter = 0u;
             if (b.stats) b.stats[0] = b.stats[1] = b.stats[2] = 0ull;
         }
-        // the last CTA to get here clears the flags for the next batch
+        // the last CTA out hands the state to the next batch
         __threadfence();
         if (atomicAdd(&sync->done, 1u) == gridDim.x - 1) {
-            for (uint32_t p = 0; p < gridDim.x; ++p) sync->flag[p] = 0u;
+            sync->ticket = 0u;
             sync->done = 0u;
+            sync->epoch = tag;
             __threadfence();
         }
     }
-    s_et[threadIdx.x] = et;
-    __syncthreads();
-    const uint32_t pt = s_pre[0];
     if (q < nq) {
         const_cast<uint32_t *>(b.tile_prefix)[q] = pt + et;
         const_cast<uint32_t *>(b.key_base)[q] = s_pre[1] + ek;
@@ -190,120 +265,199 @@ __global__ void __launch_bounds__(kPackThreads) k_pack_scan(const ListDesc *__re
             if (s_et[mid] <= tl) lo = mid;
             else hi = mid - 1;
         }
-        b.tile_q[pt + tl] = blockIdx.x * blockDim.x + lo;
+        b.tile_q[pt + tl] = bid * blockDim.x + lo;
     }
 }
 
-__global__ void __launch_bounds__(kSSThreads) k_scan_scatter(BatchView b, uint32_t *__restrict__ tile_out,
-                                                             uint32_t *__restrict__ chunk_agg,
-                                                             uint32_t *__restrict__ offsets,
-                                                             uint32_t *__restrict__ docids, uint64_t cap) {
-    cg::grid_group grid = cg::this_grid();
-    __shared__ uint32_t s_red[kSSThreads / 32 + 1];
+// ---------------------------------------------------------------------------
+
+// One warp finds two lower bounds in a[0, n) (first i with a[i] >= x, n if
+// none): lanes 0-15 search x1, lanes 16-31 x2, each a 16-way split per round.
+__device__ __forceinline__ void warp_lower_bound2(const uint32_t *a, uint32_t n, uint32_t x1, uint32_t x2,
+                                                  uint32_t &r1, uint32_t &r2) {
+    const uint32_t lane = threadIdx.x & 31u, sub = lane & 15u;
+    const uint32_t half = lane >> 4 ? 0xffff0000u : 0x0000ffffu;
+    const uint32_t x = lane >> 4 ? x2 : x1;
+    uint32_t lo = 0, hi = n;
+    while (__any_sync(0xffffffffu, lo < hi)) {
+        const uint32_t len = hi - lo;
+        const uint32_t step = (len + 15u) >> 4;
+        const uint32_t m = step ? (len + step - 1u) / step : 0u;  // probes inside [lo, hi)
+        const uint32_t pos = lo + sub * step;
+        const bool pred = sub < m && a[pos] < x;
+        const uint32_t k = __popc(__ballot_sync(0xffffffffu, pred) & half);
+        if (lo < hi) {
+            const uint32_t nlo = k ? lo + (k - 1u) * step + 1u : lo;
+            const uint32_t nhi = k < m ? lo + k * step : hi;
+            lo = nlo;
+            hi = nhi;
+        }
+    }
+    r1 = __shfl_sync(0xffffffffu, lo, 0);
+    r2 = __shfl_sync(0xffffffffu, lo, 16);
+}
+
+// Phase A (CTAs holding a chunk ticket): survivor total of the chunk,
+// decoupled look-back for its base, the absolute output position of each of
+// its tiles (into tile_q, free once the probe kernel is done) and the offsets
+// of the queries starting in it; then the chunk's inclusive prefix is
+// published. Phase B (every warp of the grid, once all chunk tickets are
+// taken, so every chunk is owned by a running CTA): survivors copied tile by
+// tile, each tile after its chunk's prefix is out.
+__global__ void __launch_bounds__(kSSThreads) k_scatter(BatchView b, PackSync *__restrict__ sync,
+                                                        uint64_t *__restrict__ chunk_state,
+                                                        uint32_t *__restrict__ offsets,
+                                                        uint32_t *__restrict__ docids, uint64_t cap) {
+    __shared__ uint32_t s_out[kSSChunk + 1];  // output position of each tile of the chunk, within the chunk
     __shared__ uint32_t sa[33], sb[33];
-    constexpr int kPer = kSSChunk / kSSThreads;  // tiles per thread in a chunk
+    __shared__ uint32_t s_c, s_base, s_qlo, s_qhi;
+    constexpr uint32_t kPer = kSSChunk / kSSThreads;
+    static_assert(kPer == 2, "two tiles per thread");
+    const uint32_t tag = *(volatile uint32_t *)&sync->epoch;  // set by this batch's k_pack_scan
     const uint32_t nq = b.nq;
     const uint32_t T = min(b.tile_prefix[nq], b.max_tiles);
     const uint32_t nch = (T + kSSChunk - 1) / kSSChunk;
     const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
-    // phase 1: survivors per chunk of tiles
-    for (uint32_t c = blockIdx.x; c < nch; c += gridDim.x) {
-        uint32_t s = 0;
-#pragma unroll
-        for (int j = 0; j < kPer; ++j) {
-            const uint32_t t = c * kSSChunk + j * kSSThreads + threadIdx.x;
-            if (t < T) s += b.tile_count[t];
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (lane == 0) s_red[w] = s;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            uint32_t tot = 0;
-            for (int i = 0; i < kSSThreads / 32; ++i) tot += s_red[i];
-            chunk_agg[c] = tot;
-        }
-        __syncthreads();
+    uint32_t *tile_out = b.tile_q;
+    if (nch == 0) {  // no tiles in the batch: every offset is 0, no ticket taken
+        for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q <= nq; q += gridDim.x * blockDim.x) offsets[q] = 0u;
+        return;
     }
-    grid.sync();
-    // phase 2: output position of every tile (chunk prefix + scan inside the chunk)
-    for (uint32_t c = blockIdx.x; c < nch; c += gridDim.x) {
-        uint32_t pre = 0;
-        for (uint32_t i = threadIdx.x; i < c; i += kSSThreads) pre += chunk_agg[i];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) pre += __shfl_xor_sync(0xffffffffu, pre, o);
-        if (lane == 0) s_red[w] = pre;
+    for (;;) {
+        if (threadIdx.x == 0) s_c = atomicAdd(&sync->sticket, 1u);
         __syncthreads();
-        if (threadIdx.x == 0) {
-            uint32_t tot = 0;
-            for (int i = 0; i < kSSThreads / 32; ++i) tot += s_red[i];
-            s_red[kSSThreads / 32] = tot;
-        }
-        __syncthreads();
-        const uint32_t base = s_red[kSSThreads / 32];
-        uint32_t cnt[kPer], sum = 0;
-#pragma unroll
-        for (int j = 0; j < kPer; ++j) {
-            const uint32_t t = c * kSSChunk + threadIdx.x * kPer + j;
-            cnt[j] = t < T ? b.tile_count[t] : 0u;
-            sum += cnt[j];
-        }
+        const uint32_t c = s_c;
+        if (c >= nch) break;
+        const uint32_t t0 = c * kSSChunk;
+        const uint32_t ta = t0 + threadIdx.x * kPer;
+        const uint32_t c0 = ta < T ? b.tile_count[ta] : 0u;
+        const uint32_t c1 = ta + 1 < T ? b.tile_count[ta + 1] : 0u;
         uint32_t ex, e2, tot, t2;
-        block_scan2(sum, 0u, ex, e2, tot, t2, sa, sb);
-        uint32_t run = base + ex;
+        block_scan2(c0 + c1, 0u, ex, e2, tot, t2, sa, sb);
+        if (threadIdx.x == 0) st_release64(&chunk_state[c], chunk_word(tag, kAggregate, tot));
+        if (w == 0) {
+            // look-back: sum the aggregates of the preceding chunks up to the
+            // nearest one that has published its inclusive prefix
+            uint32_t excl = 0;
+            int64_t p = (int64_t)c - 1;
+            for (;;) {
+                const int64_t idx = p - (int64_t)lane;
+                uint32_t st = kPrefix, v = 0;
+                if (idx >= 0) {
+                    uint64_t s = ld_acquire64(&chunk_state[idx]);
+                    uint32_t spins = 0;
+                    while ((uint32_t)(s >> 34) != tag) {
+                        if (++spins > kSpin) {
+                            atomicOr(b.err, kErrScanSpin);
+                            s = chunk_word(tag, kPrefix, 0u);
+                            break;
+                        }
+                        __nanosleep(32);
+                        s = ld_acquire64(&chunk_state[idx]);
+                    }
+                    st = (uint32_t)(s >> 32) & 3u;
+                    v = (uint32_t)s;
+                }
+                const uint32_t m = __ballot_sync(0xffffffffu, st == kPrefix);
+                const uint32_t stop = m ? (uint32_t)(__ffs(m) - 1) : 31u;
+                uint32_t contrib = lane <= stop ? v : 0u;
 #pragma unroll
-        for (int j = 0; j < kPer; ++j) {
-            const uint32_t t = c * kSSChunk + threadIdx.x * kPer + j;
-            if (t < T) tile_out[t] = run;
-            run += cnt[j];
+                for (int o = 16; o > 0; o >>= 1) contrib += __shfl_xor_sync(0xffffffffu, contrib, o);
+                excl += contrib;
+                if (m) break;
+                p -= 32;
+            }
+            if (lane == 0) s_base = excl;
+        } else if (w == 1) {
+            // meanwhile: the queries whose first tile lies in this chunk (the
+            // last chunk also takes the end offset and queries starting at T)
+            uint32_t qlo, qhi;
+            warp_lower_bound2(b.tile_prefix, nq + 1, t0, t0 + kSSChunk, qlo, qhi);
+            if (lane == 0) {
+                s_qlo = qlo;
+                s_qhi = c == nch - 1 ? nq + 1 : qhi;
+            }
         }
-        if (c == nch - 1 && threadIdx.x == kSSThreads - 1) tile_out[T] = run;
+        s_out[threadIdx.x * kPer] = ex;
+        s_out[threadIdx.x * kPer + 1] = ex + c0;
+        if (threadIdx.x == 0) s_out[kSSChunk] = tot;
         __syncthreads();
+        const uint32_t base = s_base;
+        if (ta < T) tile_out[ta] = base + ex;
+        if (ta + 1 < T) tile_out[ta + 1] = base + ex + c0;
+        const uint32_t qlo = s_qlo, qhi = s_qhi;
+        for (uint32_t qq = qlo + threadIdx.x; qq < qhi; qq += blockDim.x) {
+            const uint32_t lt = min(b.tile_prefix[qq], T) - t0;
+            offsets[qq] = base + s_out[min(lt, kSSChunk)];
+        }
+        if (c == nch - 1 && threadIdx.x == 0 && (uint64_t)base + tot > cap) atomicOr(b.err, kErrCapacity);
+        __syncthreads();  // tile positions written before the prefix goes out
+        if (threadIdx.x == 0) {
+            __threadfence();
+            st_release64(&chunk_state[c], chunk_word(tag, kPrefix, base + tot));
+        }
     }
-    if (nch == 0 && blockIdx.x == 0 && threadIdx.x == 0) tile_out[0] = 0u;
-    grid.sync();
-    // phase 3: every warp of the grid moves survivors; then the query offsets
-    if (blockIdx.x == 0 && threadIdx.x == 0 && tile_out[T] > cap) atomicOr(b.err, kErrCapacity);
-    const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    // phase B: warp per tile over the whole grid; eight independent loads per lane in flight
+    const uint32_t gw = blockIdx.x * (kSSThreads / 32) + w, nw = gridDim.x * (kSSThreads / 32);
+    const uint32_t *__restrict__ scr = b.scratch;
+    uint32_t ready = 0xffffffffu;  // chunk whose prefix this warp has seen
     for (uint32_t t = gw; t < T; t += nw) {
         const uint32_t n = b.tile_count[t];
         if (n == 0) continue;
-        const uint64_t o = tile_out[t];
-        const uint32_t *src = b.scratch + b.tile_slot[t];
-        for (uint32_t k = lane; k < n; k += 32)
-            if (o + k < cap) docids[o + k] = src[k];
+        const uint32_t c = t / kSSChunk;
+        if (c != ready) {
+            uint64_t s = ld_acquire64(&chunk_state[c]);
+            uint32_t spins = 0;
+            while ((uint32_t)(s >> 34) != tag || ((uint32_t)(s >> 32) & 3u) != kPrefix) {
+                if (++spins > kSpin) {
+                    atomicOr(b.err, kErrScanSpin);
+                    break;
+                }
+                __nanosleep(64);
+                s = ld_acquire64(&chunk_state[c]);
+            }
+            ready = c;
+        }
+        const uint64_t o = ld_acquire(&tile_out[t]);
+        const uint32_t *src = scr + b.tile_slot[t];
+        uint32_t v[kTileKeys / 32];
+#pragma unroll
+        for (uint32_t i = 0; i < kTileKeys / 32; ++i) {
+            const uint32_t k = lane + 32u * i;
+            if (k < n) v[i] = src[k];
+        }
+#pragma unroll
+        for (uint32_t i = 0; i < kTileKeys / 32; ++i) {
+            const uint32_t k = lane + 32u * i;
+            if (k < n && o + k < cap) docids[o + k] = v[i];
+        }
     }
-    const uint32_t gt = blockIdx.x * blockDim.x + threadIdx.x;
-    for (uint32_t q = gt; q <= nq; q += gridDim.x * blockDim.x) offsets[q] = tile_out[min(b.tile_prefix[q], T)];
+    // the last CTA out resets the chunk ticket
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&sync->sdone, 1u) == gridDim.x - 1) {
+            sync->sticket = 0u;
+            sync->sdone = 0u;
+            __threadfence();
+        }
+    }
 }
 
-int launch_pack_scan(const ListDesc *lists, uint32_t nlists, const uint32_t *terms, const uint32_t *toff, uint32_t nq,
-                     const BatchView &b, PackSync *sync, cudaStream_t st) {
-    if (nq > kPackMaxQueries) return (int)cudaErrorInvalidValue;
-    const uint32_t blocks = std::max(1u, (nq + kPackThreads - 1) / kPackThreads);
-    k_pack_scan<<<blocks, kPackThreads, 0, st>>>(lists, nlists, terms, toff, nq, b, sync);
-    return (int)cudaGetLastError();
-}
+// ---------------------------------------------------------------------------
 
-int scan_scatter_grid(int nsm) {
-    static int cached[64] = {};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev >= 0 && dev < 64 && cached[dev]) return cached[dev];
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_scan_scatter, kSSThreads, 0);
-    const int g = std::max(1, std::min(per_sm, 1) * nsm);
-    if (dev >= 0 && dev < 64) cached[dev] = g;
-    return g;
-}
-
-int launch_scan_scatter(const BatchView &b, uint32_t *tile_out, uint32_t *chunk_agg, uint32_t *offsets,
-                        uint32_t *docids, uint64_t cap, int nsm, cudaStream_t st) {
-    const int grid = scan_scatter_grid(nsm);
-    BatchView bb = b;
-    void *args[] = {&bb, &tile_out, &chunk_agg, &offsets, &docids, &cap};
-    return (int)cudaLaunchCooperativeKernel((const void *)k_scan_scatter, dim3(grid), dim3(kSSThreads), args, 0, st);
+int launch_batch(const BatchLaunch &L, cudaStream_t st) {
+    if (L.b.nq > kPackMaxQueries) return (int)cudaErrorInvalidValue;
+    if (L.ev) cudaEventRecord(L.ev[0], st);
+    const uint32_t pack_blocks = std::max(1u, (L.b.nq + kPackThreads - 1) / kPackThreads);
+    k_pack_scan<<<pack_blocks, kPackThreads, 0, st>>>(L.lists, L.nlists, L.terms, L.toff, L.b.nq, L.b, L.sync);
+    int e = (int)cudaGetLastError();
+    if (L.ev) cudaEventRecord(L.ev[1], st);
+    e |= launch_probe(L.ixv, L.b, L.algo, L.warps, L.ctas_per_sm, L.nsm, st);
+    if (L.ev) cudaEventRecord(L.ev[2], st);
+    k_scatter<<<std::max(1, 2 * L.nsm), kSSThreads, 0, st>>>(L.b, L.sync, L.chunk_state, L.offsets, L.docids, L.cap);
+    e |= (int)cudaGetLastError();
+    if (L.ev) cudaEventRecord(L.ev[3], st);
+    return e;
 }
 
 }  // namespace excl

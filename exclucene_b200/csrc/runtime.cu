@@ -204,12 +204,11 @@ int ctx_alloc_batch(excl_ctx *ctx) {
     st |= dalloc(ctx, &ctx->d_tile_q, (size_t)ctx->max_tiles + 1, "alloc tile owner");
     st |= dalloc(ctx, &ctx->d_tile_count, (size_t)ctx->max_tiles + 1, "alloc tile count");
     st |= dalloc(ctx, &ctx->d_tile_slot, (size_t)ctx->max_tiles + 1, "alloc tile slot");
-    st |= dalloc(ctx, &ctx->d_tile_out, (size_t)ctx->max_tiles + 2, "alloc tile out");
     st |= dalloc(ctx, &ctx->d_scratch, (size_t)c.max_keys, "alloc scratch");
     st |= dalloc(ctx, &ctx->d_misc, 16, "alloc misc");
     st |= dalloc(ctx, &ctx->d_stats, 4, "alloc stats");
     st |= dalloc(ctx, &ctx->d_sync, 1, "alloc pack sync");
-    st |= dalloc(ctx, &ctx->d_chunk_agg, (size_t)ctx->max_tiles / kSSChunk + 2, "alloc chunk sums");
+    st |= dalloc(ctx, &ctx->d_chunk_state, (size_t)ctx->max_tiles / kSSChunk + 2, "alloc chunk states");
     st |= dalloc(ctx, &ctx->d_offsets, (size_t)c.max_queries + 1, "alloc offsets");
     ctx->docids_cap = c.max_keys;
     st |= dalloc(ctx, &ctx->d_docids, ctx->docids_cap, "alloc docids");
@@ -220,6 +219,7 @@ int ctx_alloc_batch(excl_ctx *ctx) {
     cudaMemsetAsync(ctx->d_misc, 0, 16 * 4, ctx->stream);
     cudaMemsetAsync(ctx->d_stats, 0, 4 * 8, ctx->stream);
     cudaMemsetAsync(ctx->d_sync, 0, sizeof(PackSync), ctx->stream);
+    cudaMemsetAsync(ctx->d_chunk_state, 0, ((size_t)ctx->max_tiles / kSSChunk + 2) * 8, ctx->stream);
     return cuda_status(ctx, cudaStreamSynchronize(ctx->stream), "ctx init");
 }
 
@@ -254,15 +254,24 @@ int run_pipeline(excl_ctx *ctx, excl_index *ix, const uint32_t *d_terms, const u
     b.max_keys = ctx->cfg.max_keys;
     b.err = ctx->d_misc + kMiscErr;
     b.stats = ctx->collect_stats ? ctx->d_stats : nullptr;
-    const DevIndexView ixv = ix->dev->view(ix->models ? model_view(ix->models) : ModelView{});
-    cudaEventRecord(ctx->ev[0], st);
-    int e = 0;
-    e |= launch_pack_scan(ix->dev->lists, ix->nlists, d_terms, d_toff, nq, b, ctx->d_sync, st);
-    cudaEventRecord(ctx->ev[1], st);
-    e |= launch_probe(ixv, b, (int)algo, ctx->warps, ctx->ctas_per_sm, ctx->nsm, st);
-    cudaEventRecord(ctx->ev[2], st);
-    e |= launch_scan_scatter(b, ctx->d_tile_out, ctx->d_chunk_agg, d_offsets, d_docids, cap, ctx->nsm, st);
-    cudaEventRecord(ctx->ev[3], st);
+    BatchLaunch L{};
+    L.ixv = ix->dev->view(ix->models ? model_view(ix->models) : ModelView{});
+    L.lists = ix->dev->lists;
+    L.nlists = ix->nlists;
+    L.terms = d_terms;
+    L.toff = d_toff;
+    L.b = b;
+    L.sync = ctx->d_sync;
+    L.chunk_state = ctx->d_chunk_state;
+    L.offsets = d_offsets;
+    L.docids = d_docids;
+    L.cap = cap;
+    L.algo = (int)algo;
+    L.warps = ctx->warps;
+    L.ctas_per_sm = ctx->ctas_per_sm;
+    L.nsm = ctx->nsm;
+    L.ev = ctx->ev;
+    const int e = launch_batch(L, st);
     if (e) return cuda_status(ctx, (cudaError_t)e, "launch");
     ctx->last_nq = nq;
     return EXCL_OK;
@@ -318,14 +327,13 @@ extern "C" int excl_ctx_destroy(excl_ctx *ctx) {
     if (!ctx) return EXCL_E_INVALID;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-    uint32_t *bufs[] = {ctx->d_terms,      ctx->d_toff,      ctx->d_qterms,     ctx->d_qnterms,
-                        ctx->d_tile_prefix, ctx->d_tile_q,    ctx->d_tile_count, ctx->d_tile_out,
-                        ctx->d_scratch,    ctx->d_misc,      ctx->d_key_base,   ctx->d_tile_slot,
-                        ctx->d_offsets,    ctx->d_docids};
+    uint32_t *bufs[] = {ctx->d_terms,   ctx->d_toff, ctx->d_qterms,   ctx->d_qnterms,   ctx->d_tile_prefix,
+                        ctx->d_tile_q,  ctx->d_tile_count, ctx->d_scratch, ctx->d_misc, ctx->d_key_base,
+                        ctx->d_tile_slot, ctx->d_offsets, ctx->d_docids};
     for (uint32_t *p : bufs) cudaFree(p);
     cudaFree(ctx->d_stats);
     cudaFree(ctx->d_sync);
-    cudaFree(ctx->d_chunk_agg);
+    cudaFree(ctx->d_chunk_state);
     cudaFreeHost(ctx->h_terms);
     cudaFreeHost(ctx->h_toff);
     cudaFreeHost(ctx->h_offsets);

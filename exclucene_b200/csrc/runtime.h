@@ -47,10 +47,10 @@ struct excl_ctx {
     uint32_t last_nq = 0;
     uint32_t *d_terms = nullptr, *d_toff = nullptr;
     uint32_t *d_qterms = nullptr, *d_qnterms = nullptr, *d_tile_prefix = nullptr, *d_tile_q = nullptr;
-    uint32_t *d_tile_count = nullptr, *d_tile_out = nullptr, *d_scratch = nullptr, *d_misc = nullptr;
-    uint32_t *d_key_base = nullptr, *d_tile_slot = nullptr, *d_chunk_agg = nullptr;
+    uint32_t *d_tile_count = nullptr, *d_scratch = nullptr, *d_misc = nullptr;
+    uint32_t *d_key_base = nullptr, *d_tile_slot = nullptr;
     excl::PackSync *d_sync = nullptr;
-    uint64_t *d_stats = nullptr;
+    uint64_t *d_stats = nullptr, *d_chunk_state = nullptr;
     uint32_t *d_offsets = nullptr, *d_docids = nullptr;
     uint64_t docids_cap = 0;
     uint32_t *h_terms = nullptr, *h_toff = nullptr, *h_offsets = nullptr;

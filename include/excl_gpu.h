@@ -169,7 +169,7 @@ int excl_ctx_check(excl_ctx *ctx);
  * reference. For callers that cannot call cudaMalloc when they query (a host
  * that fixes its device memory budget at start-up, or an embedding without an
  * excl_ctx, whose creation allocates the batch buffers): the per-batch scratch
- * lives in one fixed device array inside the library (5.1 MiB on every GPU that
+ * lives in one fixed device array inside the library (5.0 MiB on every GPU that
  * loads it, held until the process exits), so the call allocates nothing.
  * The index must already be uploaded, on the current device. The caller passes
  * the inputs and outputs as device pointers and the cudaStream_t to run on;
@@ -195,6 +195,56 @@ typedef struct {
     uint64_t fallbacks; /* learned probes that fell back to the directory search */
 } excl_batch_stats;
 int excl_last_stats(excl_ctx *ctx, excl_batch_stats *st);
+
+/* ---------------------------------------------------------------------------
+ * Serving loop: continuous batching of single queries. No counterpart in the
+ * reference, whose benchmark binaries run fixed batches from a query file
+ * (ParaPFD_Intersection.cu:406-540). The index stays resident; queries are
+ * submitted one at a time from any thread. A dispatcher packs whatever has
+ * arrived into a batch whenever one of `slots` streams is idle, admitting
+ * queries (FIFO) only while the batch's device working set fits in the free
+ * part of a fixed HBM pool of hbm_budget_bytes; batches on different slots
+ * run concurrently. A query's result is the same whatever it was batched with.
+ * The index must be uploaded (excl_index_upload) to `device` first and outlive
+ * the server. */
+typedef struct excl_server excl_server;
+
+typedef struct {
+    uint32_t slots;             /* concurrent batches (streams), 0 = 4 */
+    uint32_t max_batch_queries; /* 0 = 4096 */
+    uint64_t max_batch_keys;    /* shortest-list docIDs per batch, 0 = 2^22; a query above it is rejected */
+    uint64_t hbm_budget_bytes;  /* working-set pool shared by the slots, 0 = room for every slot's largest batch */
+    uint32_t algo;              /* EXCL_ALGO_* */
+    uint32_t warps_per_cta;     /* probe launch shape, 0 = default */
+    uint32_t ctas_per_sm;
+} excl_server_config;
+
+typedef struct {
+    uint64_t submitted, completed, batches, rejected;
+    double mean_batch;           /* completed queries per batch */
+    uint64_t pool_bytes, pool_peak_bytes;
+    uint32_t max_inflight;       /* most batches on the device at once */
+    double p50_us, p99_us, max_us; /* submit -> result, completed queries */
+} excl_server_stats;
+
+int excl_server_create(int device, excl_index *ix, const excl_server_config *cfg, excl_server **out);
+/* Finishes the batches in flight, fails queued queries, frees everything. */
+int excl_server_destroy(excl_server *s);
+/* Queues one query (its term ids are copied). Never waits for the GPU. */
+int excl_server_submit(excl_server *s, const uint32_t *terms, uint32_t nterms, uint64_t *ticket);
+/* Waits for a submitted query; copies its docIDs (ascending) to docids and the
+ * count to *n, then releases the ticket. EXCL_E_CAPACITY if cap is too small
+ * (the ticket is kept), EXCL_E_TIMEOUT after timeout_ms (< 0: no limit). */
+int excl_server_wait(excl_server *s, uint64_t ticket, uint32_t *docids, size_t cap, uint32_t *n, int timeout_ms);
+int excl_server_stats_get(excl_server *s, excl_server_stats *st);
+int excl_server_stats_reset(excl_server *s);
+/* Open-loop load for measurements: query q (terms[term_offsets[q] ..
+ * term_offsets[q+1])) is submitted arrival_s[q] seconds after the call starts
+ * (non-decreasing); returns once all are answered, with each query's
+ * submit -> result latency in latency_s[q] (may be NULL), the excl_checksum
+ * triple of all results in cs (may be NULL) and the elapsed time in *wall_s. */
+int excl_server_replay(excl_server *s, const uint32_t *terms, const uint32_t *term_offsets, uint32_t nq,
+                       const double *arrival_s, double *latency_s, uint64_t cs[3], double *wall_s);
 
 /* ---------------------------------------------------------------------------
  * Learned position models. The reference's analogue is SegLRC's two-level
