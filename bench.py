@@ -48,6 +48,7 @@ def parse():
     p.add_argument("--learn-min", type=int, default=None,
                    help="lists with at least this many postings get a learned model (default per workload)")
     p.add_argument("--no-learn", action="store_true")
+    p.add_argument("--no-serve", action="store_true", help="skip the serving-loop latency measurement")
     return p.parse_args()
 
 
@@ -276,6 +277,46 @@ def decode_measure(ctx, ix, w, sizes, arrays, stream, flush, args):
             "peak_kind": kind, "prefix_matches_source": ok}
 
 
+def serving_measure(ix, w, algos, device, want_cs, seed=0xEC1E0005):
+    """Continuous-batching server on the resident index: open-loop Poisson
+    arrivals of the workload's queries at several rates (and all at once for
+    the saturated throughput); p50/p99 submit->result latency per rate, for
+    each search method. The replay's result checksum must equal the batch's."""
+    import exclucene_b200 as ex
+
+    lens = np.diff(w.list_offsets).astype(np.int64)
+    max_keys = max(int(min(lens[w.terms[w.term_offsets[q]:w.term_offsets[q + 1]]], default=0)) for q in range(w.nq))
+    out = {}
+    rng = np.random.default_rng(seed)
+    rates = [5_000, 50_000, 200_000]
+    arrivals = {r: np.cumsum(rng.exponential(1.0 / r, w.nq)) for r in rates}
+    for a in algos:
+        srv = ex.Server(ix, device=device, slots=4, max_batch_queries=4096, max_batch_keys=max(1 << 22, max_keys),
+                        algo=a)
+        try:
+            srv.replay(w.terms, w.term_offsets, np.zeros(w.nq))  # warm-up
+            res = {}
+            for r in rates:
+                srv.reset_stats()
+                lat, cs, wall = srv.replay(w.terms, w.term_offsets, arrivals[r])
+                st = srv.stats()
+                res[f"{r}"] = {"offered_qps": r, "qps": w.nq / wall, "p50_us": float(np.percentile(lat, 50) * 1e6),
+                               "p99_us": float(np.percentile(lat, 99) * 1e6), "mean_batch": st["mean_batch"],
+                               "max_inflight": st["max_inflight"], "checksum_ok": cs == want_cs}
+            srv.reset_stats()
+            lat, cs, wall = srv.replay(w.terms, w.term_offsets, np.zeros(w.nq))
+            st = srv.stats()
+            res["saturated"] = {"qps": w.nq / wall, "p50_us": float(np.percentile(lat, 50) * 1e6),
+                                "p99_us": float(np.percentile(lat, 99) * 1e6), "mean_batch": st["mean_batch"],
+                                "max_inflight": st["max_inflight"], "checksum_ok": cs == want_cs,
+                                "pool_peak_bytes": st["pool_peak_bytes"]}
+            out[a] = res
+        finally:
+            srv.close()
+    return {"slots": 4, "max_batch_queries": 4096, "queries": w.nq,
+            "arrivals": "open-loop Poisson, seeded; latency = submit to result in host memory", "by_algo": out}
+
+
 # ---------------------------------------------------------------------------
 
 def main():
@@ -326,14 +367,17 @@ def main():
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.int32, device=dev)  # > L2 (126 MB)
     torch.cuda.synchronize()
 
-    def step(algo):
-        ctx.intersect_device(ix, d_terms.data_ptr(), d_toff.data_ptr(), w.nq, algo, d_offs.data_ptr(),
-                             d_docs.data_ptr(), cap)
+    # a second context on the same resident index replays each batch as a CUDA graph
+    gctx = ex.Context(local, max_queries=max(w.nq, 1024), max_keys=max(1 << 20, 2 * shortest), use_graphs=True)
 
-    def measure(algo, k, warm):
+    def step(c, algo):
+        c.intersect_device(ix, d_terms.data_ptr(), d_toff.data_ptr(), w.nq, algo, d_offs.data_ptr(),
+                           d_docs.data_ptr(), cap)
+
+    def measure(c, algo, k, warm):
         for _ in range(warm):
-            step(algo)
-        ctx.check()
+            step(c, algo)
+        c.check()
         tot, probe = [], []
         if world > 1:
             dist.barrier()
@@ -341,26 +385,30 @@ def main():
         for _ in range(k):
             flush_l2(flush)
             torch.cuda.synchronize()
-            step(algo)
-            st = ctx.stats()
+            step(c, algo)
+            st = c.stats()
             tot.append(st.total_ms)
             probe.append(st.probe_ms)
         torch.cuda.synchronize()
-        ctx.check()
+        c.check()
         if world > 1:
             dist.barrier()
         return float(np.mean(tot)), float(np.mean(probe)), st
 
     postings = query_postings(w)
     algos = [args.algo] if args.algo else ["bsearch", "hashseg"] + ([] if args.no_learn else ["learned"])
-    per_algo = {}
+    per_algo, per_algo_graph = {}, {}
     with ClockSampler(local) as clk:
         for a in algos:
-            ms, pms, st = measure(a, args.steps, args.warmup)
-            per_algo[a] = (ms, pms, st)
+            per_algo[a] = measure(ctx, a, args.steps, args.warmup)
+            per_algo_graph[a] = measure(gctx, a, args.steps, args.warmup)
     clocks = clk.summary()
-    best = min(per_algo, key=lambda a: per_algo[a][0]) if not args.algo else args.algo
+    best = min(per_algo, key=lambda a: min(per_algo[a][0], per_algo_graph[a][0])) if not args.algo else args.algo
     ms, pms, st = per_algo[best]
+    launch_mode = "stream"
+    if per_algo_graph[best][0] < ms:
+        ms, launch_mode = per_algo_graph[best][0], "cuda graph"
+    main_ctx = gctx if launch_mode == "cuda graph" else ctx
     if world > 1:
         t = torch.tensor([ms, pms], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -376,13 +424,13 @@ def main():
     h_off = np.zeros(w.nq + 1, dtype=np.uint32)
     h_docs = np.zeros(cap, dtype=np.uint32)
     for _ in range(args.warmup):
-        b = ctx.submit(ix, w.terms, w.term_offsets, best)
+        b = main_ctx.submit(ix, w.terms, w.term_offsets, best)
         b.wait_into(h_off, h_docs)
         b.free()
     e2e_t = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        b = ctx.submit(ix, w.terms, w.term_offsets, best)
+        b = main_ctx.submit(ix, w.terms, w.term_offsets, best)
         tot = b.wait_into(h_off, h_docs)
         e2e_t.append(time.perf_counter() - t0)
         b.free()
@@ -400,6 +448,9 @@ def main():
 
     # whole-index decode (K1/K2): compressed words + per-segment metadata read, 4 B per posting written
     dec = decode_measure(ctx, ix, w, sizes, arrays, stream, flush, args)
+    serving = None
+    if not args.no_serve:
+        serving = serving_measure(ix, w, ["hashseg"] + ([] if args.no_learn else ["learned"]), local, cs)
     line = {
         "metric": "postings/s", "value": value, "unit": "postings/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
@@ -408,12 +459,20 @@ def main():
                    "postings_per_step": postings, "index_device_bytes": int(sizes.device_bytes),
                    "index_postings": int(sizes.postings), "l2": "flushed (512 MB read) before each timed step"},
         "queries_per_s": world * w.nq / (ms / 1e3),
+        "launch": launch_mode,
         "per_algo_ms": {a: round(per_algo[a][0], 4) for a in per_algo},
+        "per_algo_graph_ms": {a: round(per_algo_graph[a][0], 4) for a in per_algo_graph},
         "per_algo_probe_ms": {a: round(per_algo[a][1], 4) for a in per_algo},
-        "learned_over_plain": (min(per_algo[a][0] for a in per_algo if a in ("bsearch", "hashseg")) /
-                               per_algo["learned"][0]) if "learned" in per_algo else None,
+        "learned_over_plain": (min(min(per_algo[a][0], per_algo_graph[a][0]) for a in per_algo
+                                   if a in ("bsearch", "hashseg")) /
+                               min(per_algo["learned"][0], per_algo_graph["learned"][0]))
+        if "learned" in per_algo else None,
+        "learned_over_bsearch": (min(per_algo["bsearch"][0], per_algo_graph["bsearch"][0]) /
+                                 min(per_algo["learned"][0], per_algo_graph["learned"][0]))
+        if "learned" in per_algo and "bsearch" in per_algo else None,
         "learned_models": learn,
-        "per_algo_postings_per_s": {a: world * postings / (per_algo[a][0] / 1e3) for a in per_algo},
+        "per_algo_postings_per_s": {a: world * postings / (min(per_algo[a][0], per_algo_graph[a][0]) / 1e3)
+                                    for a in per_algo},
         "stats": {"tiles": int(st.tiles), "keys": int(st.keys), "probes": int(st.probes),
                   "fallbacks": int(st.fallbacks), "probe_ms": pms, "pack_ms": st.pack_ms,
                   "compact_ms": st.compact_ms},
@@ -423,9 +482,10 @@ def main():
                      "peak_kind": peak_kind},
         "e2e": {"value": world * postings / e2e_s, "unit": "postings/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_s * 1e3},
-        "gpu_launches": 6 * len(algos) * args.steps,
+        "gpu_launches": 3 * (2 * len(algos) + 1) * args.steps,  # pack, probe, scatter per batch, both launch modes + e2e
         "clocks": clocks,
         "decode": dec,
+        "serving": serving,
     }
     if rank == 0 and world == 1 and not args.no_cpu:
         import oracle
@@ -437,6 +497,7 @@ def main():
                                           "decode + exact AND on the same compressed index (oracle port)"}
     if rank == 0:
         print(json.dumps(line), flush=True)
+    gctx.close()
     ctx.close()
     if world > 1:
         dist.destroy_process_group()

@@ -62,7 +62,7 @@ class IndexSizes(C.Structure):
 
 class CtxConfig(C.Structure):
     _fields_ = [("max_queries", C.c_uint32), ("max_terms", C.c_uint32), ("max_keys", C.c_uint64),
-                ("warps_per_cta", C.c_uint32), ("ctas_per_sm", C.c_uint32)]
+                ("warps_per_cta", C.c_uint32), ("ctas_per_sm", C.c_uint32), ("use_graphs", C.c_uint32)]
 
 
 class BatchStats(C.Structure):
@@ -283,9 +283,9 @@ class Index:
 
 class Context:
     def __init__(self, device: int = 0, max_queries: int = 65536, max_keys: int = 1 << 26, warps_per_cta: int = 0,
-                 ctas_per_sm: int = 0):
+                 ctas_per_sm: int = 0, use_graphs: bool = False):
         self._h = None
-        cfg = CtxConfig(max_queries, 32, max_keys, warps_per_cta, ctas_per_sm)
+        cfg = CtxConfig(max_queries, 32, max_keys, warps_per_cta, ctas_per_sm, 1 if use_graphs else 0)
         h = C.c_void_p()
         st = _ctx_create(device, C.byref(cfg), C.byref(h))
         _check_status(st, what="excl_ctx_create")

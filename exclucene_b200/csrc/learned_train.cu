@@ -335,7 +335,7 @@ void init_root(float *P, uint32_t seed) {
 }  // namespace
 
 ModelView model_view(const ModelSet *m) {
-    ModelView v;
+    ModelView v{};
     if (m) {
         v.root = m->d_root;
         v.hdr = m->d_hdr;

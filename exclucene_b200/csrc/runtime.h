@@ -38,6 +38,11 @@ struct excl_ctx {
     int warps = 8;
     int ctas_per_sm = 4;
     bool collect_stats = true;
+    // CUDA graph of the last batch launched through excl_intersect_device
+    bool use_graphs = false, last_was_graph = false;
+    cudaGraphExec_t gexec = nullptr;
+    uint64_t gkey[10] = {};
+    bool gkey_seen = false;  // the key ran once uncaptured (first sighting)
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     excl_ctx_config cfg{};

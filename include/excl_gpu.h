@@ -121,6 +121,9 @@ typedef struct {
     uint64_t max_keys;       /* per batch, sum of shortest-list lengths (reference baseSize) */
     uint32_t warps_per_cta;  /* probe kernel launch shape (0 = autotuned/default) */
     uint32_t ctas_per_sm;
+    uint32_t use_graphs;     /* 1: excl_intersect_device replays a CUDA graph of the batch's three
+                                kernels when called again with the same arguments (per-kernel
+                                times in excl_last_stats are then 0; total_ms stays) */
 } excl_ctx_config;
 
 int excl_ctx_create(int device, const excl_ctx_config *cfg, excl_ctx **out);

@@ -113,3 +113,38 @@ def test_batching_does_not_change_results(gpu_ctx, corpus, expected):
         assert np.array_equal(docs, exp)
         assert np.array_equal(offs.astype(np.uint64), eoffs[q0:q1 + 1] - eoffs[q0])
     ix.close()
+
+
+def test_graph_replay_matches_oracle(corpus, expected):
+    """A context that replays its batches as CUDA graphs gives the same output
+    on every replay, and recaptures when the batch or the method changes."""
+    import torch
+
+    gctx = ex.Context(0, max_queries=65536, max_keys=1 << 24, use_graphs=True)
+    ix = _index(corpus, "seglrc")
+    gctx.upload(ix)
+    dev = torch.device("cuda", 0)
+    eoffs, edocs = expected
+    try:
+        for nq, algo in [(corpus.nq, "hashseg"), (1000, "hashseg"), (corpus.nq, "bsearch"), (1000, "hashseg")]:
+            n_terms = int(corpus.term_offsets[nq])
+            d_terms = torch.from_numpy(corpus.terms[:n_terms].astype(np.int32)).to(dev)
+            d_toff = torch.from_numpy(corpus.term_offsets[:nq + 1].astype(np.int32)).to(dev)
+            cap = int(eoffs[nq]) + 16
+            d_offs = torch.empty(nq + 1, dtype=torch.int32, device=dev)
+            d_docs = torch.empty(cap, dtype=torch.int32, device=dev)
+            for _ in range(3):  # first run uncaptured, then captured, then replayed
+                d_offs.fill_(-1)
+                d_docs.fill_(-1)
+                torch.cuda.synchronize()  # the context's stream does not wait for torch's
+                gctx.intersect_device(ix, d_terms.data_ptr(), d_toff.data_ptr(), nq, algo, d_offs.data_ptr(),
+                                      d_docs.data_ptr(), cap)
+                gctx.check()
+                offs = d_offs.cpu().numpy().astype(np.uint64)
+                assert np.array_equal(offs, eoffs[:nq + 1] - eoffs[0])
+                assert np.array_equal(d_docs[:int(offs[-1])].cpu().numpy().astype(np.uint32),
+                                      edocs[:int(eoffs[nq])])
+                assert gctx.stats().total_ms > 0
+    finally:
+        ix.close()
+        gctx.close()
