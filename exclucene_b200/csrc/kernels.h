@@ -62,8 +62,9 @@ struct BatchLaunch {
 // pack -> probe -> scatter on `st`.
 int launch_batch(const BatchLaunch &L, cudaStream_t st);
 
+// tk: two zeroed words (work counter, finished CTAs), left zeroed.
 int launch_decode(const DevIndexView &ix, uint32_t l0, uint32_t l1, uint64_t out_base0, uint32_t *out, uint32_t seg0,
-                  uint32_t nsegs, int nsm, uint32_t *err, cudaStream_t st);
+                  uint32_t nsegs, int nsm, uint32_t *tk, uint32_t *err, cudaStream_t st);
 int launch_probe(const DevIndexView &ix, const BatchView &b, int algo, int warps, int ctas_per_sm, int nsm,
                  cudaStream_t st);
 

@@ -489,7 +489,7 @@ extern "C" int excl_decode_lists_device(excl_ctx *ctx, excl_index *ix, uint32_t 
     const uint32_t seg0 = ix->lists[l0].seg_base;
     const uint32_t seg1 = ix->lists[l1 - 1].seg_base + ix->lists[l1 - 1].nseg;
     const int e = launch_decode(ix->dev->view(ModelView{}), l0, l1, base0, d_out, seg0, seg1 - seg0, ctx->nsm,
-                                ctx->d_misc + kMiscErr, ctx->stream);
+                                ctx->d_misc + kMiscDecodeTicket, ctx->d_misc + kMiscErr, ctx->stream);
     return cuda_status(ctx, (cudaError_t)e, "decode launch");
 }
 

@@ -28,7 +28,7 @@ struct DeviceIndex {
 };
 
 // slots of ctx->d_misc
-enum { kMiscErr = 0, kMiscTileCounter = 1, kMiscTicket0 = 2, kMiscTicket1 = 3 };
+enum { kMiscErr = 0, kMiscTileCounter = 1, kMiscDecodeTicket = 2 /* and 3: decode work counter, CTAs done */ };
 
 }  // namespace excl
 

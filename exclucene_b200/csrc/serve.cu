@@ -399,7 +399,9 @@ void slot_loop(excl_server *s, Slot *sl) {
     }
 }
 
-int submit_locked(excl_server *s, const uint32_t *terms, uint32_t nterms, Replay *rp, uint32_t q, uint64_t *ticket) {
+// Builds a request (no lock held): validates the terms and finds the
+// shortest list, the first of equal lengths as the batch kernel's stable sort.
+int make_request(excl_server *s, const uint32_t *terms, uint32_t nterms, ReqPtr *out) {
     if (nterms > kMaxTerms || (!terms && nterms)) return EXCL_E_INVALID;
     auto r = std::make_shared<Request>();
     r->terms.assign(terms, terms + nterms);
@@ -407,24 +409,29 @@ int submit_locked(excl_server *s, const uint32_t *terms, uint32_t nterms, Replay
     for (uint32_t i = 0; i < nterms; ++i) {
         const uint32_t t = terms[i];
         if (t >= s->ix->nlists) return EXCL_E_INVALID;
-        const ListDesc &d = s->ix->lists[t];
-        if (best == 0xffffffffu || d.n < s->ix->lists[best].n) best = t;  // first of the shortest, as the stable sort
+        if (best == 0xffffffffu || s->ix->lists[t].n < s->ix->lists[best].n) best = t;
     }
     if (nterms) {
         r->keys = s->ix->lists[best].n;
         r->tiles = s->ix->lists[best].ntiles;
     }
-    r->replay = rp;
-    r->replay_q = q;
-    r->t_submit = Clock::now();
+    *out = std::move(r);
+    return EXCL_OK;
+}
+
+// Queues requests in order under one lock; tickets only for the caller-waited ones.
+int enqueue(excl_server *s, ReqPtr *reqs, size_t n, uint64_t *ticket) {
     std::lock_guard<std::mutex> g(s->mu);
     if (s->stop) return EXCL_E_INVALID;
     if (s->sticky) return s->sticky;
-    r->id = s->next_id++;
-    if (!rp) s->tickets[r->id] = r;
-    if (ticket) *ticket = r->id;
-    s->queue.push_back(std::move(r));
-    ++s->submitted;
+    for (size_t i = 0; i < n; ++i) {
+        ReqPtr &r = reqs[i];
+        r->id = s->next_id++;
+        if (!r->replay) s->tickets[r->id] = r;
+        if (ticket) *ticket = r->id;
+        s->queue.push_back(std::move(r));
+    }
+    s->submitted += n;
     return EXCL_OK;
 }
 
@@ -539,7 +546,11 @@ extern "C" int excl_server_destroy(excl_server *s) {
 
 extern "C" int excl_server_submit(excl_server *s, const uint32_t *terms, uint32_t nterms, uint64_t *ticket) {
     if (!s || !ticket) return EXCL_E_INVALID;
-    const int st = submit_locked(s, terms, nterms, nullptr, 0, ticket);
+    ReqPtr r;
+    int st = make_request(s, terms, nterms, &r);
+    if (st) return st;
+    r->t_submit = Clock::now();
+    st = enqueue(s, &r, 1, ticket);
     if (!st) s->cv_dispatch.notify_one();
     return st;
 }
@@ -618,22 +629,41 @@ extern "C" int excl_server_replay(excl_server *s, const uint32_t *terms, const u
     rp.latency_s = latency_s;
     rp.remaining.store(nq);
     const Clock::time_point t0 = Clock::now();
-    for (uint32_t q = 0; q < nq; ++q) {
-        const Clock::time_point due = t0 + std::chrono::duration_cast<Clock::duration>(
-                                                std::chrono::duration<double>(arrival_s[q]));
-        for (;;) {
-            const Clock::time_point now = Clock::now();
-            if (now >= due) break;
-            if (due - now > std::chrono::microseconds(200)) std::this_thread::sleep_for(due - now - std::chrono::microseconds(100));
+    auto due = [&](uint32_t q) {
+        return t0 + std::chrono::duration_cast<Clock::duration>(std::chrono::duration<double>(arrival_s[q]));
+    };
+    std::vector<ReqPtr> reqs;
+    uint32_t q = 0;
+    while (q < nq) {
+        Clock::time_point now = Clock::now();
+        if (now < due(q)) {
+            const auto wait = due(q) - now;
+            if (wait > std::chrono::microseconds(200)) std::this_thread::sleep_for(wait - std::chrono::microseconds(100));
             else std::this_thread::yield();
+            continue;
         }
-        const int st = submit_locked(s, terms + term_offsets[q], term_offsets[q + 1] - term_offsets[q], &rp, q, nullptr);
+        // every query already due goes in under one lock; its latency counts
+        // from its scheduled arrival, so a late submit is not hidden
+        reqs.clear();
+        uint32_t qe = q;
+        while (qe < nq && due(qe) <= now) {
+            ReqPtr r;
+            const int st = make_request(s, terms + term_offsets[qe], term_offsets[qe + 1] - term_offsets[qe], &r);
+            if (st) return st;  // validated above
+            r->replay = &rp;
+            r->replay_q = qe;
+            r->t_submit = due(qe);
+            reqs.push_back(std::move(r));
+            ++qe;
+        }
+        const int st = enqueue(s, reqs.data(), reqs.size(), nullptr);
         if (st) {
             rp.status.store(st);
             rp.remaining.fetch_sub(nq - q);
             break;
         }
         s->cv_dispatch.notify_one();
+        q = qe;
     }
     while (rp.remaining.load() != 0) std::this_thread::sleep_for(std::chrono::microseconds(50));
     if (wall_s) *wall_s = std::chrono::duration<double>(Clock::now() - t0).count();
