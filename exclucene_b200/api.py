@@ -62,13 +62,26 @@ class IndexSizes(C.Structure):
 
 class CtxConfig(C.Structure):
     _fields_ = [("max_queries", C.c_uint32), ("max_terms", C.c_uint32), ("max_keys", C.c_uint64),
-                ("warps_per_cta", C.c_uint32), ("ctas_per_sm", C.c_uint32), ("use_graphs", C.c_uint32)]
+                ("warps_per_cta", C.c_uint32), ("ctas_per_sm", C.c_uint32), ("use_graphs", C.c_uint32),
+                ("merge_segs", C.c_uint32)]
+
+MERGE_OFF = 0xFFFFFFFF
+
+
+class TuneReport(C.Structure):
+    _fields_ = [("algo", C.c_uint32), ("warps_per_cta", C.c_uint32), ("ctas_per_sm", C.c_uint32),
+                ("merge_segs", C.c_uint32), ("best_ms", C.c_float), ("default_ms", C.c_float), ("tried", C.c_uint32)]
+
+    def as_dict(self) -> dict:
+        d = {k: getattr(self, k) for k, _ in self._fields_}
+        d["algo"] = {v: k for k, v in ALGO_NAMES.items()}.get(d["algo"], d["algo"])
+        return d
 
 
 class BatchStats(C.Structure):
     _fields_ = [("pack_ms", C.c_float), ("probe_ms", C.c_float), ("compact_ms", C.c_float),
                 ("total_ms", C.c_float), ("tiles", C.c_uint64), ("keys", C.c_uint64), ("probes", C.c_uint64),
-                ("fallbacks", C.c_uint64)]
+                ("fallbacks", C.c_uint64), ("merges", C.c_uint64)]
 
 
 class LearnParams(C.Structure):
@@ -117,6 +130,7 @@ _check = _sig("excl_ctx_check", C.c_int, C.c_void_p)
 _stats = _sig("excl_last_stats", C.c_int, C.c_void_p, C.POINTER(BatchStats))
 _checksum = _sig("excl_checksum", C.c_int, C.c_uint32, u32p, u32p, C.POINTER(C.c_uint64 * 3))
 
+_autotune = _sig("excl_autotune", C.c_int, C.c_void_p, C.c_void_p, u32p, u32p, C.c_uint32, C.POINTER(TuneReport))
 _learn = _sig("excl_learn_models", C.c_int, C.c_void_p, C.c_void_p, C.POINTER(LearnParams), C.POINTER(LearnReport))
 _mexport = _sig("excl_model_export", C.c_int, C.c_void_p, C.c_uint32, C.POINTER(C.c_float), C.POINTER(C.c_float),
                 C.POINTER(C.c_int32), C.POINTER(C.c_uint32))
@@ -283,9 +297,9 @@ class Index:
 
 class Context:
     def __init__(self, device: int = 0, max_queries: int = 65536, max_keys: int = 1 << 26, warps_per_cta: int = 0,
-                 ctas_per_sm: int = 0, use_graphs: bool = False):
+                 ctas_per_sm: int = 0, use_graphs: bool = False, merge_segs: int = 0):
         self._h = None
-        cfg = CtxConfig(max_queries, 32, max_keys, warps_per_cta, ctas_per_sm, 1 if use_graphs else 0)
+        cfg = CtxConfig(max_queries, 32, max_keys, warps_per_cta, ctas_per_sm, 1 if use_graphs else 0, merge_segs)
         h = C.c_void_p()
         st = _ctx_create(device, C.byref(cfg), C.byref(h))
         _check_status(st, what="excl_ctx_create")
@@ -359,6 +373,15 @@ class Context:
         _check_status(_mgrad(self._h, P.ctypes.data_as(fp), xs.ctypes.data_as(fp), ys.ctypes.data_as(fp), len(xs),
                              g.ctypes.data_as(fp), C.byref(loss)), self, "excl_model_grad")
         return g, loss.value
+
+    def autotune(self, ix: Index, terms, term_offsets) -> dict:
+        """Times the sample batch under every candidate setting and keeps the
+        fastest for later batches run with algo="auto"."""
+        t = _u32(terms) if len(terms) else np.zeros(1, dtype=np.uint32)
+        o = _u32(term_offsets)
+        r = TuneReport()
+        _check_status(_autotune(self._h, ix._h, _p32(t), _p32(o), len(o) - 1, C.byref(r)), self, "excl_autotune")
+        return r.as_dict()
 
     def stats(self) -> BatchStats:
         s = BatchStats()
@@ -465,7 +488,7 @@ _srv_stats = _sig("excl_server_stats_get", C.c_int, C.c_void_p, C.POINTER(Server
 _srv_reset = _sig("excl_server_stats_reset", C.c_int, C.c_void_p)
 _srv_replay = _sig("excl_server_replay", C.c_int, C.c_void_p, u32p, u32p, C.c_uint32, C.POINTER(C.c_double),
                    C.POINTER(C.c_double), C.POINTER(C.c_uint64 * 3), C.POINTER(C.c_double))
-EXPORTED += ["excl_server_create", "excl_server_destroy", "excl_server_submit", "excl_server_wait",
+EXPORTED += ["excl_autotune", "excl_server_create", "excl_server_destroy", "excl_server_submit", "excl_server_wait",
              "excl_server_stats_get", "excl_server_stats_reset", "excl_server_replay",
              "excl_intersect_device_noalloc"]
 

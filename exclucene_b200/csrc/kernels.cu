@@ -100,18 +100,43 @@ __device__ __forceinline__ bool probe_key(const DevIndexView &ix, const ListDesc
     return resid_find(blk, h, rp, rec.count, (int)t0, (int)t1, key);
 }
 
+// Segment of L (list-relative) whose head is the last one <= key, found with
+// the directory (or a binary search over all heads for BSEARCH); -1 if key
+// precedes the list.
+template <int ALGO>
+__device__ __forceinline__ int locate_segment(const DevIndexView &ix, const ListDesc &L, uint32_t key) {
+    if (key < L.first_doc) return -1;
+    if (key > L.last_doc) return (int)L.nseg - 1;
+    uint32_t lo = 0, hi = L.nseg;
+    if (ALGO != EXCL_ALGO_BSEARCH) {
+        const uint32_t bk = (uint32_t)((uint64_t)key >> L.dir_shift);
+        const uint32_t d0 = ldg(ix.dir + L.dir_base + bk), d1 = ldg(ix.dir + L.dir_base + bk + 1);
+        lo = codec_is_hs(L.codec) ? d0 : (d0 ? d0 - 1u : 0u);
+        hi = d1;
+    }
+    return last_head_le(ix.seg_head + L.seg_base, lo, hi, key);
+}
+
 // ---------------------------------------------------------------------------
 // Persistent probe kernel.
+//
+// For each longer list a tile chooses between two methods (the merge-path /
+// probe choice): when the tile's surviving keys span few of the list's
+// segments (at most b.merge_segs, whose docIDs fit kMergeCap), the warp
+// decodes that span into shared memory once and every key is looked up there;
+// otherwise each key is probed on its own (probe_key).
 
 template <int ALGO, int WARPS>
 __global__ void __launch_bounds__(WARPS * 32) k_probe(DevIndexView ix, BatchView b) {
     __shared__ uint32_t s_keys[WARPS][kTileKeys];
+    __shared__ uint32_t s_merge[WARPS][kMergeCap];
     __shared__ ListDesc s_list[WARPS];
     const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
     uint32_t *keys = s_keys[w];
+    uint32_t *mbuf = s_merge[w];
     ListDesc &L = s_list[w];
     const uint32_t T = min(b.tile_prefix[b.nq], b.max_tiles);
-    uint32_t probes = 0, fallbacks = 0, nkeys = 0;
+    uint32_t probes = 0, fallbacks = 0, nkeys = 0, merges = 0;
     for (;;) {
         uint32_t t = 0;
         if (lane == 0) t = atomicAdd(b.tile_counter, 1u);
@@ -149,12 +174,55 @@ __global__ void __launch_bounds__(WARPS * 32) k_probe(DevIndexView ix, BatchView
             __syncwarp();
             if (lane < 5) reinterpret_cast<uint4 *>(&L)[lane] = reinterpret_cast<const uint4 *>(ix.lists + qt[j])[lane];
             __syncwarp();
+            // merge when the keys' range covers few segments: estimated from
+            // the list's density first (no loads), then measured
+            uint32_t span = 0, mseg0 = 0;
+            if (b.merge_segs && alive >= kMergeMinKeys) {
+                const uint32_t klo = keys[0], khi = keys[alive - 1];
+                const double dens = (double)L.n / ((double)(L.last_doc - L.first_doc) + 1.0);
+                if ((double)(khi - klo) * dens < 0.75 * kMergeCap) {
+                    int sl = 0;
+                    if (lane < 2) sl = locate_segment<ALGO>(ix, L, lane ? khi : klo);
+                    const int s0 = max(__shfl_sync(0xffffffffu, sl, 0), 0), s1 = __shfl_sync(0xffffffffu, sl, 1);
+                    if (s1 >= s0 && (uint32_t)(s1 - s0) < b.merge_segs) {
+                        const uint32_t a0 = ix.seg_rec[L.seg_base + s0].start;
+                        const SegRec r1 = ix.seg_rec[L.seg_base + s1];
+                        if (r1.start + r1.count - a0 <= kMergeCap) {
+                            span = r1.start + r1.count - a0;
+                            mseg0 = (uint32_t)s0;
+                            ++merges;
+                            for (uint32_t sg = L.seg_base + s0; sg <= L.seg_base + (uint32_t)s1; ++sg) {
+                                const SegRec r = ix.seg_rec[sg];
+                                for (uint32_t e0 = 0; e0 < r.count; e0 += kTileKeys)
+                                    warp_decode(ix, L, sg, e0, min(kTileKeys, r.count - e0), mbuf + (r.start - a0) + e0,
+                                                lane);
+                            }
+                        }
+                    } else if (s1 < 0) {
+                        alive = 0;  // every key precedes the list: nothing survives
+                        continue;
+                    }
+                }
+            }
+            (void)mseg0;
             uint32_t nout = 0;
             for (uint32_t base = 0; base < alive; base += 32) {
                 const uint32_t i = base + lane;
                 const bool valid = i < alive;
                 const uint32_t key = valid ? keys[i] : 0u;
-                const bool f = valid && probe_key<ALGO>(ix, L, key, fallbacks);
+                bool f;
+                if (span) {
+                    // first position with mbuf[pos] >= key, in shared memory
+                    uint32_t lo = 0, hi = span;
+                    while (lo < hi) {
+                        const uint32_t mid = (lo + hi) >> 1;
+                        if (mbuf[mid] < key) lo = mid + 1;
+                        else hi = mid;
+                    }
+                    f = valid && lo < span && mbuf[lo] == key;
+                } else {
+                    f = valid && probe_key<ALGO>(ix, L, key, fallbacks);
+                }
                 probes += valid;
                 const uint32_t m = __ballot_sync(0xffffffffu, f);
                 const uint32_t pos = nout + __popc(m & ((1u << lane) - 1u));
@@ -186,10 +254,12 @@ __global__ void __launch_bounds__(WARPS * 32) k_probe(DevIndexView ix, BatchView
             probes += __shfl_xor_sync(0xffffffffu, probes, o);
             fallbacks += __shfl_xor_sync(0xffffffffu, fallbacks, o);
         }
+        // nkeys and merges are warp-uniform: lane 0's count is the warp's
         if (lane == 0) {
             atomicAdd((unsigned long long *)&b.stats[0], (unsigned long long)probes);
             atomicAdd((unsigned long long *)&b.stats[1], (unsigned long long)fallbacks);
             atomicAdd((unsigned long long *)&b.stats[2], (unsigned long long)nkeys);
+            atomicAdd((unsigned long long *)&b.stats[3], (unsigned long long)merges);
         }
     }
 }
@@ -230,7 +300,6 @@ int launch_probe(const DevIndexView &ix, const BatchView &b, int algo, int warps
     const uint32_t blocks = (uint32_t)std::max(1, nsm * ctas_per_sm);
     switch (warps) {
         case 4: launch_probe_w<4>(ix, b, algo, blocks, nsm, st); break;
-        case 16: launch_probe_w<16>(ix, b, algo, blocks, nsm, st); break;
         default: launch_probe_w<8>(ix, b, algo, blocks, nsm, st); break;
     }
     return (int)cudaGetLastError();

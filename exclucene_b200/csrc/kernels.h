@@ -20,10 +20,15 @@ struct BatchView {
     uint32_t *tile_slot;         // scratch position of each tile's survivors
     uint32_t *scratch;           // max_keys survivor slots, indexed by key position
     uint32_t max_tiles;
+    uint32_t merge_segs;         // probe: merge when a tile's keys span at most this many segments (0: never)
     uint64_t max_keys;
     uint32_t *err;               // error flag bits
     uint64_t *stats;             // [probes, fallbacks] or null
 };
+
+// probe kernel: shared-memory merge of a tile's keys against a decoded span
+constexpr uint32_t kMergeCap = 512;      // docIDs of the span (two 256-blocks)
+constexpr uint32_t kMergeMinKeys = 32;   // fewer keys than this: always probe
 
 // pipeline.cu
 constexpr uint32_t kPackThreads = 256;

@@ -116,6 +116,7 @@ extern "C" int excl_intersect_device_noalloc(excl_index *ix, const uint32_t *d_t
     b.tile_slot = base + kOffTileSlot;
     b.scratch = base + kOffSurvivors;
     b.max_tiles = kNATiles;
+    b.merge_segs = 2;
     b.max_keys = kNAKeys;
     b.err = base + kOffMisc;
     b.stats = reinterpret_cast<uint64_t *>(base + kOffStats);

@@ -241,7 +241,7 @@ __global__ void __launch_bounds__(kPackThreads) k_pack_scan(const ListDesc *__re
         }
         if (bid == 0) {
             *b.tile_counter = 0u;
-            if (b.stats) b.stats[0] = b.stats[1] = b.stats[2] = 0ull;
+            if (b.stats) b.stats[0] = b.stats[1] = b.stats[2] = b.stats[3] = 0ull;
         }
         // the last CTA out hands the state to the next batch
         __threadfence();

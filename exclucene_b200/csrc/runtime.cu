@@ -2,6 +2,7 @@
 // batched query pipeline and its host-buffer submit/wait form.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cstdarg>
 #include <cstdio>
@@ -238,6 +239,7 @@ int run_pipeline(excl_ctx *ctx, excl_index *ix, const uint32_t *d_terms, const u
         ctx_error(ctx, "unknown algo %u", algo);
         return EXCL_E_INVALID;
     }
+    if (algo == EXCL_ALGO_AUTO && ctx->tuned_algo >= 0) algo = (uint32_t)ctx->tuned_algo;
     cudaStream_t st = ctx->stream;
     BatchView b{};
     b.nq = nq;
@@ -251,6 +253,7 @@ int run_pipeline(excl_ctx *ctx, excl_index *ix, const uint32_t *d_terms, const u
     b.tile_slot = ctx->d_tile_slot;
     b.scratch = ctx->d_scratch;
     b.max_tiles = ctx->max_tiles;
+    b.merge_segs = ctx->merge_segs;
     b.max_keys = ctx->cfg.max_keys;
     b.err = ctx->d_misc + kMiscErr;
     b.stats = ctx->collect_stats ? ctx->d_stats : nullptr;
@@ -280,7 +283,9 @@ int run_pipeline(excl_ctx *ctx, excl_index *ix, const uint32_t *d_terms, const u
         for (size_t i = 0; i < sizeof L.ixv; ++i) vh = (vh ^ vb[i]) * 1099511628211ull;
         const uint64_t key[10] = {(uint64_t)(uintptr_t)ix, vh, (uint64_t)(uintptr_t)d_terms,
                                   (uint64_t)(uintptr_t)d_toff, nq, algo, (uint64_t)(uintptr_t)d_offsets,
-                                  (uint64_t)(uintptr_t)d_docids, cap, (uint64_t)ctx->collect_stats};
+                                  (uint64_t)(uintptr_t)d_docids, cap,
+                                  (uint64_t)ctx->collect_stats | (uint64_t)ctx->merge_segs << 8 |
+                                      (uint64_t)ctx->warps << 16 | (uint64_t)ctx->ctas_per_sm << 32};
         const bool same = ctx->gkey_seen && std::memcmp(key, ctx->gkey, sizeof key) == 0;
         if (same || ctx->gexec) {
             if (!same || !ctx->gexec) {
@@ -358,6 +363,7 @@ extern "C" int excl_ctx_create(int device, const excl_ctx_config *cfg, excl_ctx 
     ctx->warps = c.warps_per_cta ? (int)c.warps_per_cta : 8;
     ctx->ctas_per_sm = c.ctas_per_sm ? (int)c.ctas_per_sm : 8;
     ctx->use_graphs = c.use_graphs != 0;
+    ctx->merge_segs = c.merge_segs == 0 ? 2u : c.merge_segs == EXCL_MERGE_OFF ? 0u : std::min(c.merge_segs, 4u);
     int st = cuda_status(ctx, cudaSetDevice(device), "cudaSetDevice");
     if (!st) st = cuda_status(ctx, cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, device), "attr");
     if (!st) st = cuda_status(ctx, cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking), "stream");
@@ -535,10 +541,10 @@ struct excl_batch {
     bool waited;
 };
 
-extern "C" int excl_submit(excl_ctx *ctx, excl_index *ix, const uint32_t *terms, const uint32_t *term_offsets,
-                           uint32_t nq, uint32_t algo, excl_batch **ticket) {
-    if (!ctx || !ix || !term_offsets || !ticket) return EXCL_E_INVALID;
-    *ticket = nullptr;
+// Copies a host batch into the context's query buffers (after the previous
+// batch has released them). Returns the number of terms through *nterms.
+static int stage_host_batch(excl_ctx *ctx, excl_index *ix, const uint32_t *terms, const uint32_t *term_offsets,
+                            uint32_t nq, uint32_t *nterms_out) {
     if (nq > ctx->cfg.max_queries) {
         ctx_error(ctx, "batch of %u queries exceeds max_queries %u", nq, ctx->cfg.max_queries);
         return EXCL_E_CAPACITY;
@@ -558,16 +564,104 @@ extern "C" int excl_submit(excl_ctx *ctx, excl_index *ix, const uint32_t *terms,
             return EXCL_E_INVALID;
         }
     cudaSetDevice(ctx->device);
-    // wait for the previous batch to release the shared buffers
     cudaStreamSynchronize(ctx->stream);
     std::memcpy(ctx->h_terms, terms + term_offsets[0], (size_t)nterms * 4);
     for (uint32_t q = 0; q <= nq; ++q) ctx->h_toff[q] = term_offsets[q] - term_offsets[0];
-    cudaStream_t st = ctx->stream;
-    int s = cuda_status(ctx, cudaMemcpyAsync(ctx->d_terms, ctx->h_terms, (size_t)nterms * 4, cudaMemcpyHostToDevice, st),
+    int s = cuda_status(ctx, cudaMemcpyAsync(ctx->d_terms, ctx->h_terms, (size_t)nterms * 4, cudaMemcpyHostToDevice,
+                                             ctx->stream),
                         "h2d terms");
     if (!s)
-        s = cuda_status(ctx, cudaMemcpyAsync(ctx->d_toff, ctx->h_toff, ((size_t)nq + 1) * 4, cudaMemcpyHostToDevice, st),
+        s = cuda_status(ctx, cudaMemcpyAsync(ctx->d_toff, ctx->h_toff, ((size_t)nq + 1) * 4, cudaMemcpyHostToDevice,
+                                             ctx->stream),
                         "h2d offsets");
+    if (nterms_out) *nterms_out = nterms;
+    return s;
+}
+
+extern "C" int excl_autotune(excl_ctx *ctx, excl_index *ix, const uint32_t *terms, const uint32_t *term_offsets,
+                             uint32_t nq, excl_tune_report *rep) {
+    if (!ctx || !ix || !term_offsets || !rep) return EXCL_E_INVALID;
+    if (!ix->dev) return EXCL_E_INVALID;
+    int s = stage_host_batch(ctx, ix, terms, term_offsets, nq, nullptr);
+    if (s) return s;
+    // candidates are timed without graphs, on the context's own buffers
+    const bool graphs = ctx->use_graphs;
+    const int w0 = ctx->warps, c0 = ctx->ctas_per_sm, t0 = ctx->tuned_algo;
+    const uint32_t m0 = ctx->merge_segs;
+    ctx->use_graphs = false;
+    ctx->tuned_algo = -1;
+    auto time_one = [&](uint32_t algo, int warps, int ctas, uint32_t merge, float *ms) -> int {
+        ctx->warps = warps;
+        ctx->ctas_per_sm = ctas;
+        ctx->merge_segs = merge;
+        float t[3];
+        for (int r = 0; r < 4; ++r) {
+            int e = run_pipeline(ctx, ix, ctx->d_terms, ctx->d_toff, nq, algo, ctx->d_offsets, ctx->d_docids,
+                                 ctx->docids_cap);
+            if (!e) e = cuda_status(ctx, cudaStreamSynchronize(ctx->stream), "tune sync");
+            if (!e) e = read_device_flags(ctx);
+            if (e) return e;
+            if (r) cudaEventElapsedTime(&t[r - 1], ctx->ev[0], ctx->ev[3]);
+        }
+        std::sort(t, t + 3);
+        *ms = t[1];
+        return EXCL_OK;
+    };
+    std::memset(rep, 0, sizeof *rep);
+    s = time_one(EXCL_ALGO_AUTO, 8, 8, 2, &rep->default_ms);
+    float best = rep->default_ms;
+    uint32_t ba = EXCL_ALGO_AUTO, bm = 2;
+    int bw = 8, bc = 8;
+    const uint32_t algos[3] = {EXCL_ALGO_BSEARCH, EXCL_ALGO_HASHSEG, EXCL_ALGO_LEARNED};
+    const int warps[2] = {4, 8}, ctas[3] = {2, 4, 8};
+    const uint32_t merges[4] = {0u, 1u, 2u, 4u};
+    uint32_t tried = 1;
+    for (uint32_t a : algos) {
+        if (s) break;
+        if (a == EXCL_ALGO_LEARNED && !ix->models) continue;
+        for (int wv : warps)
+            for (int cv : ctas)
+                for (uint32_t mv : merges) {
+                    if (s) break;
+                    float ms = 0;
+                    s = time_one(a, wv, cv, mv, &ms);
+                    ++tried;
+                    if (!s && ms < best) {
+                        best = ms;
+                        ba = a;
+                        bw = wv;
+                        bc = cv;
+                        bm = mv;
+                    }
+                }
+    }
+    ctx->use_graphs = graphs;
+    if (s) {
+        ctx->warps = w0;
+        ctx->ctas_per_sm = c0;
+        ctx->merge_segs = m0;
+        ctx->tuned_algo = t0;
+        return s;
+    }
+    ctx->warps = bw;
+    ctx->ctas_per_sm = bc;
+    ctx->merge_segs = bm;
+    ctx->tuned_algo = (int)ba;
+    rep->algo = ba;
+    rep->warps_per_cta = (uint32_t)bw;
+    rep->ctas_per_sm = (uint32_t)bc;
+    rep->merge_segs = bm ? bm : EXCL_MERGE_OFF;
+    rep->best_ms = best;
+    rep->tried = tried;
+    return EXCL_OK;
+}
+
+extern "C" int excl_submit(excl_ctx *ctx, excl_index *ix, const uint32_t *terms, const uint32_t *term_offsets,
+                           uint32_t nq, uint32_t algo, excl_batch **ticket) {
+    if (!ctx || !ix || !term_offsets || !ticket) return EXCL_E_INVALID;
+    *ticket = nullptr;
+    cudaStream_t st = ctx->stream;
+    int s = stage_host_batch(ctx, ix, terms, term_offsets, nq, nullptr);
     if (!s) s = run_pipeline(ctx, ix, ctx->d_terms, ctx->d_toff, nq, algo, ctx->d_offsets, ctx->d_docids, ctx->docids_cap);
     if (!s)
         s = cuda_status(ctx, cudaMemcpyAsync(ctx->h_offsets, ctx->d_offsets, ((size_t)nq + 1) * 4,
@@ -641,11 +735,12 @@ extern "C" int excl_last_stats(excl_ctx *ctx, excl_batch_stats *stt) {
     uint32_t T = 0;
     cudaMemcpy(&T, ctx->d_tile_prefix + ctx->last_nq, 4, cudaMemcpyDeviceToHost);
     stt->tiles = T;
-    uint64_t hs[3] = {0, 0, 0};
-    if (ctx->collect_stats) cudaMemcpy(hs, ctx->d_stats, 24, cudaMemcpyDeviceToHost);
+    uint64_t hs[4] = {0, 0, 0, 0};
+    if (ctx->collect_stats) cudaMemcpy(hs, ctx->d_stats, 32, cudaMemcpyDeviceToHost);
     stt->probes = hs[0];
     stt->fallbacks = hs[1];
     stt->keys = hs[2];
+    stt->merges = hs[3];
     return EXCL_OK;
 }
 

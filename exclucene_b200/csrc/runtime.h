@@ -37,6 +37,8 @@ struct excl_ctx {
     int nsm = 148;
     int warps = 8;
     int ctas_per_sm = 4;
+    uint32_t merge_segs = 2;
+    int tuned_algo = -1;  // search method the autotuner chose for EXCL_ALGO_AUTO (-1: none)
     bool collect_stats = true;
     // CUDA graph of the last batch launched through excl_intersect_device
     bool use_graphs = false, last_was_graph = false;

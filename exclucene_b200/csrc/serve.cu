@@ -250,6 +250,7 @@ int launch_on_slot(excl_server *s, Slot *sl, uint64_t nterms, uint64_t tiles, ui
     b.tile_slot = at(L.tile_slot);
     b.scratch = at(L.scratch);
     b.max_tiles = (uint32_t)tiles;
+    b.merge_segs = 2;
     b.max_keys = keys;
     b.err = sl->d_misc;
     b.stats = nullptr;

@@ -124,7 +124,11 @@ typedef struct {
     uint32_t use_graphs;     /* 1: excl_intersect_device replays a CUDA graph of the batch's three
                                 kernels when called again with the same arguments (per-kernel
                                 times in excl_last_stats are then 0; total_ms stays) */
+    uint32_t merge_segs;     /* probe kernel: a tile whose keys span at most this many segments of a
+                                longer list decodes that span into shared memory and merges instead
+                                of probing key by key (0 = default 2, EXCL_MERGE_OFF = never; max 4) */
 } excl_ctx_config;
+#define EXCL_MERGE_OFF 0xffffffffu
 
 int excl_ctx_create(int device, const excl_ctx_config *cfg, excl_ctx **out);
 int excl_ctx_destroy(excl_ctx *ctx);
@@ -196,8 +200,26 @@ typedef struct {
     uint64_t keys;      /* shortest-list docIDs decoded */
     uint64_t probes;    /* (key, longer list) probes */
     uint64_t fallbacks; /* learned probes that fell back to the directory search */
+    uint64_t merges;    /* (tile, longer list) pairs merged in shared memory instead of probed */
 } excl_batch_stats;
 int excl_last_stats(excl_ctx *ctx, excl_batch_stats *st);
+
+/* Autotuner (no counterpart in the reference, which fixes one launch shape per
+ * binary). Runs a sample batch (host arrays, as excl_submit) under every
+ * candidate setting: search method (bsearch, hash directory, learned where
+ * models exist), probe launch shape (warps per CTA x CTAs per SM) and merge
+ * threshold (EXCL_MERGE_OFF, 1, 2, 4 segments). Each candidate is timed with
+ * CUDA events (median of 3 after a warm-up); the fastest is kept in the
+ * context and used by later batches submitted with EXCL_ALGO_AUTO. The sample
+ * must fit the context's limits. */
+typedef struct {
+    uint32_t algo, warps_per_cta, ctas_per_sm, merge_segs; /* the setting kept */
+    float best_ms;     /* its device time for the sample */
+    float default_ms;  /* device time of the untuned default (auto, 8 warps, 8 CTAs/SM, merge 2) */
+    uint32_t tried;    /* candidates timed */
+} excl_tune_report;
+int excl_autotune(excl_ctx *ctx, excl_index *ix, const uint32_t *terms, const uint32_t *term_offsets, uint32_t nq,
+                  excl_tune_report *report);
 
 /* ---------------------------------------------------------------------------
  * Serving loop: continuous batching of single queries. No counterpart in the

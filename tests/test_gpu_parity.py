@@ -148,3 +148,48 @@ def test_graph_replay_matches_oracle(corpus, expected):
     finally:
         ix.close()
         gctx.close()
+
+
+@pytest.mark.parametrize("codec", FORMATS)
+@pytest.mark.parametrize("merge", [ex.api.MERGE_OFF, 1, 4])
+def test_merge_and_probe_paths_agree(corpus, expected, codec, merge):
+    """The shared-memory merge path (tiles whose keys span few segments of a
+    longer list) and the per-key probe path give the oracle's output."""
+    ctx = ex.Context(0, max_queries=65536, max_keys=1 << 24, merge_segs=merge)
+    ix = _index(corpus, codec, 128 if codec == "parapfd" else 256, 0.1 if codec == "parapfd" else 0.0)
+    ctx.upload(ix)
+    eoffs, edocs = expected
+    try:
+        for algo in ("bsearch", "hashseg"):
+            offs, docs = ctx.intersect(ix, corpus.terms, corpus.term_offsets, algo=algo)
+            assert np.array_equal(offs.astype(np.uint64), eoffs)
+            assert np.array_equal(docs, edocs)
+            st = ctx.stats()
+            if merge == ex.api.MERGE_OFF:
+                assert st.merges == 0
+            else:
+                assert st.merges > 0
+    finally:
+        ix.close()
+        ctx.close()
+
+
+def test_autotune_keeps_output_exact(corpus, expected):
+    """The autotuner picks a setting no slower than the default on its sample,
+    and batches run with the tuned setting still match the oracle."""
+    ctx = ex.Context(0, max_queries=65536, max_keys=1 << 24)
+    ix = _index(corpus, "seglrc")
+    ctx.upload(ix)
+    eoffs, edocs = expected
+    try:
+        rep = ctx.autotune(ix, corpus.terms[:int(corpus.term_offsets[500])], corpus.term_offsets[:501])
+        assert rep["tried"] > 10
+        assert rep["algo"] in ("bsearch", "hashseg", "learned", "auto")
+        assert rep["warps_per_cta"] in (4, 8) and rep["ctas_per_sm"] in (2, 4, 8)
+        assert 0 < rep["best_ms"] <= rep["default_ms"]
+        offs, docs = ctx.intersect(ix, corpus.terms, corpus.term_offsets, algo="auto")
+        assert np.array_equal(offs.astype(np.uint64), eoffs)
+        assert np.array_equal(docs, edocs)
+    finally:
+        ix.close()
+        ctx.close()
