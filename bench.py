@@ -32,6 +32,10 @@ sys.path.insert(0, ROOT)
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 
+# dram__bytes_read.sum + dram__bytes_write.sum of one k_probe launch (hash-directory search) on
+# the full-size workload, from one ncu --set full capture of this same bench command
+NCU_PROBE_TRAFFIC = {"zipf": 44.20e6}
+
 
 def parse():
     p = argparse.ArgumentParser()
@@ -337,6 +341,7 @@ def main():
     import torch.distributed as dist
 
     import exclucene_b200 as ex
+    from exclucene_b200 import replicas
 
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
@@ -417,10 +422,9 @@ def main():
         ms, launch_mode = per_algo_graph[best][0], "cuda graph"
     main_ctx = gctx if launch_mode == "cuda graph" else ctx
     best_algo = "auto" if best == "tuned" else best  # the tuned setting runs as algo=auto
-    if world > 1:
-        t = torch.tensor([ms, pms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, pms = float(t[0]), float(t[1])
+    # replicas: every rank ran the whole batch; the job time is the slowest rank's
+    ms = replicas.max_over_ranks(ms, device=dev)
+    pms = replicas.max_over_ranks(pms, device=dev)
     value = world * postings / (ms / 1e3)
 
     # checksum of the last device result (traceability)
@@ -443,10 +447,7 @@ def main():
         e2e_t.append(time.perf_counter() - t0)
         b.free()
     e2e_s = float(np.mean(e2e_t))
-    if world > 1:
-        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t[0])
+    e2e_s = replicas.max_over_ranks(e2e_s, device=dev)
     h2d = w.terms.nbytes + w.term_offsets.nbytes
     d2h = h_off.nbytes + 4 * tot
 
@@ -487,8 +488,10 @@ def main():
                   "compact_ms": st.compact_ms},
         "checksum": list(cs),
         "roofline": {"bound": "hbm", "kernel": "k_probe", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None, "algorithmic_bytes": algo_bytes,
-                     "peak_kind": peak_kind},
+                     "frac": achieved / peak,
+                     "traffic": NCU_PROBE_TRAFFIC.get(args.workload) if args.scale == 1.0 else None,
+                     "traffic_note": "ncu dram read+write per k_probe launch, hash-directory search",
+                     "algorithmic_bytes": algo_bytes, "peak_kind": peak_kind},
         "e2e": {"value": world * postings / e2e_s, "unit": "postings/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_s * 1e3},
         "gpu_launches": 3 * (2 * len(algos) + (1 if tune else 0) + 1) * args.steps,  # pack, probe, scatter per batch
