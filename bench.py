@@ -43,7 +43,7 @@ def parse():
     p.add_argument("--steps", type=int, default=10)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--workload", default="zipf", choices=["zipf", "pairs", "skewed"])
+    p.add_argument("--workload", default="zipf", choices=["zipf", "pairs", "skewed", "learned", "serving"])
     p.add_argument("--codec", default=None)
     p.add_argument("--algo", default=None, help="search method for `value` (default: best measured)")
     p.add_argument("--cpu-sample-s", type=float, default=15.0)
@@ -80,6 +80,21 @@ def make_workload(name: str, scale: float):
         return w, dict(codec="hs_parapfd", block=128, frac=0.10, hs_kbits=16, hs_ubits=26), (
             f"2^26 universe, 32 clustered long lists 1e6-2e7, {nq} short lists 1e3-1e4, 1-3 long per query; "
             "HS top-16-bit buckets, ParaPFD blocks of 128, FRAC 0.10")
+    if name == "learned":
+        nq = max(100, int(20_000 * scale))
+        lmin, lmax = int(10_000_000 * scale), int(100_000_000 * scale)
+        w = synth.learned(lmin=lmin, lmax=lmax, nq=nq)
+        return w, dict(codec="seglrc", block=256, frac=0.0), (
+            f"learned vs plain: 64 clustered-run lists of log-U[{lmin:.0e}, {lmax:.0e}] and 64 Zipf(1.2)-gap "
+            f"lists over 2^31; {nq} queries, each a probe-key list of log-U[1e3, 1e5] keys (half from the "
+            "target list) AND its target; SegLRC 256-entry segments, FRAC 0")
+    if name == "serving":
+        total, nterms = int(1_000_000_000 * scale), max(1000, int(2_000_000 * scale))
+        nq = max(1000, int(100_000 * min(scale * 10, 1.0)))
+        w = synth.serving(total=total, nterms=nterms, nq=nq)
+        return w, dict(codec="seglrc", block=256, frac=0.0, codecs=w.codecs), (
+            f"serving corpus: {total:.2e} postings over {nterms} terms (Zipf(1) dfs, 2^28 universe), ParaPFD "
+            f"below 1e4 postings else SegLRC; {nq} queries of 2-8 terms ~ df^0.5")
     raise ValueError(name)
 
 
@@ -95,16 +110,11 @@ def algorithmic_bytes(w, arrays) -> int:
     lists = arrays.lists
     nseg_all = len(arrays.seg_head)
     seg_rec = arrays.seg_rec
-    # words per segment
-    seg_words = np.zeros(nseg_all, dtype=np.int64)
-    for l in range(len(lists)):
-        s0, ns = int(lists[l]["seg_base"]), int(lists[l]["nseg"])
-        offs = seg_rec[s0:s0 + ns, 1].astype(np.int64)
-        end = offs[1:].tolist() + [None]
-        nxt = int(lists[l + 1]["word_base"]) - int(lists[l]["word_base"]) if l + 1 < len(lists) else None
-        if nxt is None:
-            nxt = int(offs[-1]) + 64
-        seg_words[s0:s0 + ns] = np.diff(np.append(offs, nxt))
+    # words per segment: blocks are stored list after list, segment after segment
+    nseg = lists["nseg"].astype(np.int64)
+    seg_of_list = np.repeat(np.arange(len(lists)), nseg)
+    gstart = lists["word_base"].astype(np.int64)[seg_of_list] + seg_rec[:nseg_all, 1].astype(np.int64)
+    seg_words = np.diff(np.append(gstart, len(arrays.words) - 8))
     codec_meta = {0: 12, 1: 8, 2: 12, 3: 28, 4: 28, 5: 12}
     total = 0
     lens = np.diff(w.list_offsets).astype(np.int64)
@@ -128,7 +138,9 @@ def algorithmic_bytes(w, arrays) -> int:
             hit = 4 * int(seg_words[s0 + segs].sum()) + meta * len(segs)
             whole = 4 * int(seg_words[s0:s0 + ns].sum()) + meta * ns
             total += min(hit, whole)
-            keys = np.intersect1d(keys, w.list(t), assume_unique=True)
+            lst = w.list(t)
+            pos = np.minimum(np.searchsorted(lst, keys), len(lst) - 1)
+            keys = keys[lst[pos] == keys]
         total += 4 * len(keys)
     return total
 
@@ -355,7 +367,8 @@ def main():
     ctx.upload(ix)
     learn = None
     if not args.no_learn:
-        lmin = args.learn_min or {"zipf": 1 << 16, "pairs": 1 << 20, "skewed": 1 << 20}[args.workload]
+        lmin = args.learn_min or {"zipf": 1 << 16, "pairs": 1 << 20, "skewed": 1 << 20, "learned": 1 << 20,
+                                  "serving": 1 << 20}[args.workload]
         t0 = time.perf_counter()
         learn = ctx.learn(ix, min_postings=lmin)
         learn["wall_s"] = time.perf_counter() - t0
