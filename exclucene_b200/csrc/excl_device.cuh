@@ -59,6 +59,7 @@ struct DevIndexView {
     const uint64_t *post_base;
     const uint32_t *seg_list;   // list of each segment
     const uint64_t *seg_gword;  // first word of each segment's block (nsegs + 1 entries)
+    const ProbeRec *seg_probe;  // per-segment probe records
     ModelView models;
 };
 
@@ -239,13 +240,22 @@ __device__ __forceinline__ int last_head_le(const uint32_t *head, uint32_t lo, u
     return (int)lo - 1;
 }
 
+// Last segment in [lo, hi) of a list's probe records whose head <= key, or lo - 1.
+__device__ __forceinline__ int last_head_le_rec(const ProbeRec *pr, uint32_t lo, uint32_t hi, uint32_t key) {
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(&pr[mid].head) <= key) lo = mid + 1;
+        else hi = mid;
+    }
+    return (int)lo - 1;
+}
+
 // Serial search of `key` (head <= key) in a d-gap segment, starting at the
 // segment head or at its median (ParaPFD_Intersection_kernel.cu:383-447:
 // median halves the walk; exceptions tracked with a cursor).
-__device__ __forceinline__ bool dgap_find(const uint32_t *blk, uint32_t count, uint32_t head, uint32_t median,
-                                          uint32_t key) {
+__device__ __forceinline__ bool dgap_find(const uint32_t *blk, const BlkHdr h, uint32_t count, uint32_t head,
+                                          uint32_t median, uint32_t key) {
     if (key == head || key == median) return true;
-    const BlkHdr h = blk_hdr(ldg(blk));
     uint32_t from, end, v;
     if (key > median) {
         from = count >> 1;

@@ -62,6 +62,23 @@ struct alignas(16) SegReg {
     uint32_t R;
 };
 
+// Everything a probe needs about one segment, in one 64-byte record built at
+// upload; the first 32 bytes serve a plain probe of any codec, so the
+// segment search, the record and the block header cost one memory round trip.
+constexpr uint32_t kProbeUnbounded = 0xffffu;  // window range too wide for 16 bits
+struct alignas(64) ProbeRec {
+    uint32_t head;   // first docID (seg_head)
+    uint32_t off;    // block's word offset within the list
+    uint32_t aux;    // SegRec.aux
+    uint32_t count;  // elements
+    uint32_t hdr;    // the block's descriptor word
+    float a, b;      // segment regression (SegLRC, HS_SegLRC)
+    uint32_t lr;     // regression window ranges L | R << 16, kProbeUnbounded if wider
+    uint32_t start;  // list position of the first element (second half: HS lists only)
+    uint32_t pad[7];
+};
+static_assert(sizeof(ProbeRec) == 64, "ProbeRec layout");
+
 #ifdef __CUDACC__
 #define EXCL_HD __host__ __device__ __forceinline__
 #else

@@ -55,14 +55,29 @@ __device__ __forceinline__ bool probe_key(const DevIndexView &ix, const ListDesc
         lo = codec_is_hs(L.codec) ? d0 : (d0 ? d0 - 1u : 0u);
         hi = d1;
     }
-    const int s = last_head_le(ix.seg_head + L.seg_base, lo, hi, key);
+    // segment search and record: the record holds the head, block offset,
+    // count, base/median, block descriptor and segment regression
+    const ProbeRec *pr = ix.seg_probe + L.seg_base;
+    const int s = (ALGO == EXCL_ALGO_BSEARCH && !learned) ? last_head_le(ix.seg_head + L.seg_base, lo, hi, key)
+                                                          : last_head_le_rec(pr, lo, hi, key);
     if (s < (int)lo) return false;
-    const uint32_t sg = L.seg_base + (uint32_t)s;
-    const SegRec rec = ix.seg_rec[sg];
+    const uint4 q0 = __ldg(reinterpret_cast<const uint4 *>(pr + s));
+    const uint4 q1 = __ldg(reinterpret_cast<const uint4 *>(pr + s) + 1);
+    SegRec rec;
+    rec.off = q0.y;
+    rec.aux = q0.z;
+    rec.count = q0.w;
     const uint32_t *blk = ix.words + L.word_base + rec.off;
-    if (codec_is_dgap(L.codec)) return dgap_find(blk, rec.count, ldg(ix.seg_head + sg), rec.aux, key);
-    const BlkHdr h = blk_hdr(ldg(blk));
-    const SegReg reg = ix.seg_reg[sg];
+    const BlkHdr h = blk_hdr(q1.x);
+    if (codec_is_dgap(L.codec)) return dgap_find(blk, h, rec.count, q0.x, rec.aux, key);
+    // list position of the segment: only learned windows and the LRC/LRCSeg
+    // predictors use it, and those lists have fixed blocks
+    rec.start = (uint32_t)s << L.log2_block;
+    SegReg reg;
+    reg.a = __uint_as_float(q1.y);
+    reg.b = __uint_as_float(q1.z);
+    reg.L = q1.w & 0xffffu;
+    reg.R = q1.w >> 16;
     const ResidParams rp = resid_params(L, rec, reg);
     int64_t t0 = 0, t1 = (int64_t)rec.count - 1;
     if (learned) {
@@ -85,8 +100,8 @@ __device__ __forceinline__ bool probe_key(const DevIndexView &ix, const ListDesc
         } else {
             a = reg.a;
             bb = reg.b;
-            rl = reg.L;
-            rr = reg.R;
+            rl = reg.L == kProbeUnbounded ? 0x7fffffffu : reg.L;
+            rr = reg.R == kProbeUnbounded ? 0x7fffffffu : reg.R;
             off = 0;
         }
         const float px = __fdiv_rn(__fsub_rn(__uint2float_rn(key), bb), a);
@@ -126,8 +141,11 @@ __device__ __forceinline__ int locate_segment(const DevIndexView &ix, const List
 // decodes that span into shared memory once and every key is looked up there;
 // otherwise each key is probed on its own (probe_key).
 
-template <int ALGO, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32) k_probe(DevIndexView ix, BatchView b) {
+// MINB: resident 8-warp CTAs per SM the register budget is cut for (4: 64
+// registers, no spills; 5: 48; 6: 40, a few spills), traded for more probes
+// in flight; the launch shape is an autotuner choice.
+template <int ALGO, int WARPS, int MINB>
+__global__ void __launch_bounds__(WARPS * 32, (8 / WARPS) * MINB) k_probe(DevIndexView ix, BatchView b) {
     __shared__ uint32_t s_keys[WARPS][kTileKeys];
     __shared__ uint32_t s_merge[WARPS][kMergeCap];
     __shared__ ListDesc s_list[WARPS];
@@ -267,40 +285,47 @@ __global__ void __launch_bounds__(WARPS * 32) k_probe(DevIndexView ix, BatchView
 // ---------------------------------------------------------------------------
 // Launchers.
 
-template <int ALGO, int WARPS>
-static void launch_probe_t(const DevIndexView &ix, const BatchView &b, uint32_t blocks, int nsm, cudaStream_t st) {
-    // persistent grid: as many CTAs as fit on the device at once (capped by the
-    // caller's ctas_per_sm), so every resident warp pulls work items
+template <int ALGO, int WARPS, int MINB>
+static void launch_probe_t(const DevIndexView &ix, const BatchView &b, int nsm, cudaStream_t st) {
+    // persistent grid: as many CTAs as fit on the device at once, so every
+    // resident warp pulls work items
     static int occ[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
     int per_sm = dev >= 0 && dev < 64 ? occ[dev] : 0;
     if (!per_sm) {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_probe<ALGO, WARPS>, WARPS * 32, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_probe<ALGO, WARPS, MINB>, WARPS * 32, 0);
         per_sm = per_sm > 0 ? per_sm : 1;
         if (dev >= 0 && dev < 64) occ[dev] = per_sm;
     }
-    const uint32_t grid = std::min<uint32_t>(blocks, (uint32_t)(per_sm * nsm));
-    k_probe<ALGO, WARPS><<<grid, WARPS * 32, 0, st>>>(ix, b);
+    const uint32_t grid = (uint32_t)std::max(1, std::min(per_sm, (8 / WARPS) * MINB) * nsm);
+    k_probe<ALGO, WARPS, MINB><<<grid, WARPS * 32, 0, st>>>(ix, b);
+}
+
+template <int WARPS, int MINB>
+static void launch_probe_a(const DevIndexView &ix, const BatchView &b, int algo, int nsm, cudaStream_t st) {
+    switch (algo) {
+        case EXCL_ALGO_BSEARCH: launch_probe_t<EXCL_ALGO_BSEARCH, WARPS, MINB>(ix, b, nsm, st); break;
+        case EXCL_ALGO_HASHSEG: launch_probe_t<EXCL_ALGO_HASHSEG, WARPS, MINB>(ix, b, nsm, st); break;
+        case EXCL_ALGO_LEARNED: launch_probe_t<EXCL_ALGO_LEARNED, WARPS, MINB>(ix, b, nsm, st); break;
+        default: launch_probe_t<EXCL_ALGO_AUTO, WARPS, MINB>(ix, b, nsm, st); break;
+    }
 }
 
 template <int WARPS>
-static void launch_probe_w(const DevIndexView &ix, const BatchView &b, int algo, uint32_t blocks, int nsm,
+static void launch_probe_w(const DevIndexView &ix, const BatchView &b, int algo, int ctas_per_sm, int nsm,
                            cudaStream_t st) {
-    switch (algo) {
-        case EXCL_ALGO_BSEARCH: launch_probe_t<EXCL_ALGO_BSEARCH, WARPS>(ix, b, blocks, nsm, st); break;
-        case EXCL_ALGO_HASHSEG: launch_probe_t<EXCL_ALGO_HASHSEG, WARPS>(ix, b, blocks, nsm, st); break;
-        case EXCL_ALGO_LEARNED: launch_probe_t<EXCL_ALGO_LEARNED, WARPS>(ix, b, blocks, nsm, st); break;
-        default: launch_probe_t<EXCL_ALGO_AUTO, WARPS>(ix, b, blocks, nsm, st); break;
-    }
+    // ctas_per_sm is counted in 8-warp CTAs
+    if (ctas_per_sm <= 4) launch_probe_a<WARPS, 4>(ix, b, algo, nsm, st);
+    else if (ctas_per_sm == 5) launch_probe_a<WARPS, 5>(ix, b, algo, nsm, st);
+    else launch_probe_a<WARPS, 6>(ix, b, algo, nsm, st);
 }
 
 int launch_probe(const DevIndexView &ix, const BatchView &b, int algo, int warps, int ctas_per_sm, int nsm,
                  cudaStream_t st) {
-    const uint32_t blocks = (uint32_t)std::max(1, nsm * ctas_per_sm);
     switch (warps) {
-        case 4: launch_probe_w<4>(ix, b, algo, blocks, nsm, st); break;
-        default: launch_probe_w<8>(ix, b, algo, blocks, nsm, st); break;
+        case 4: launch_probe_w<4>(ix, b, algo, ctas_per_sm, nsm, st); break;
+        default: launch_probe_w<8>(ix, b, algo, ctas_per_sm, nsm, st); break;
     }
     return (int)cudaGetLastError();
 }

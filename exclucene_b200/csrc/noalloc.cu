@@ -134,7 +134,7 @@ extern "C" int excl_intersect_device_noalloc(excl_index *ix, const uint32_t *d_t
     L.cap = cap;
     L.algo = (int)algo;
     L.warps = 8;
-    L.ctas_per_sm = 8;
+    L.ctas_per_sm = 5;
     L.nsm = nsm;
     L.ev = nullptr;
 

@@ -164,8 +164,10 @@ void DeviceIndex::release() {
     cudaFree(post_base);
     cudaFree(seg_list);
     cudaFree(seg_gword);
+    cudaFree(seg_probe);
     seg_list = nullptr;
     seg_gword = nullptr;
+    seg_probe = nullptr;
     lists = nullptr;
     words = seg_head = dir = nullptr;
     seg_rec = nullptr;
@@ -185,6 +187,7 @@ DevIndexView DeviceIndex::view(const ModelView &mv) const {
     v.post_base = post_base;
     v.seg_list = seg_list;
     v.seg_gword = seg_gword;
+    v.seg_probe = seg_probe;
     v.models = mv;
     return v;
 }
@@ -361,7 +364,7 @@ extern "C" int excl_ctx_create(int device, const excl_ctx_config *cfg, excl_ctx 
     if (c.max_keys == 0) c.max_keys = 1ull << 26;
     ctx->cfg = c;
     ctx->warps = c.warps_per_cta ? (int)c.warps_per_cta : 8;
-    ctx->ctas_per_sm = c.ctas_per_sm ? (int)c.ctas_per_sm : 8;
+    ctx->ctas_per_sm = c.ctas_per_sm ? (int)c.ctas_per_sm : 5;
     ctx->use_graphs = c.use_graphs != 0;
     ctx->merge_segs = c.merge_segs == 0 ? 2u : c.merge_segs == EXCL_MERGE_OFF ? 0u : std::min(c.merge_segs, 4u);
     int st = cuda_status(ctx, cudaSetDevice(device), "cudaSetDevice");
@@ -428,6 +431,22 @@ extern "C" int excl_index_upload(excl_ctx *ctx, excl_index *ix) {
             sgw[g] = ix->lists[l].word_base + ix->seg_rec[g].off;
         }
     sgw[nsegs] = ix->words.size() - kWordPad;
+    std::vector<ProbeRec> prec(nsegs);
+    for (size_t g = 0; g < nsegs; ++g) {
+        const SegRec &r = ix->seg_rec[g];
+        const SegReg &rg = ix->seg_reg[g];
+        ProbeRec &p = prec[g];
+        std::memset(&p, 0, sizeof p);
+        p.head = ix->seg_head[g];
+        p.off = r.off;
+        p.aux = r.aux;
+        p.count = r.count;
+        p.hdr = ix->words[sgw[g]];
+        p.a = rg.a;
+        p.b = rg.b;
+        p.lr = std::min<uint32_t>(rg.L, kProbeUnbounded) | std::min<uint32_t>(rg.R, kProbeUnbounded) << 16;
+        p.start = r.start;
+    }
     int st = 0;
     st |= dalloc(ctx, &d->lists, ix->lists.size(), "index lists");
     st |= dalloc(ctx, &d->words, ix->words.size(), "index words");
@@ -439,6 +458,7 @@ extern "C" int excl_index_upload(excl_ctx *ctx, excl_index *ix) {
     st |= dalloc(ctx, &d->post_base, pb.size(), "index post base");
     st |= dalloc(ctx, &d->seg_list, slist.size(), "index seg list");
     st |= dalloc(ctx, &d->seg_gword, sgw.size(), "index seg words");
+    st |= dalloc(ctx, &d->seg_probe, prec.size(), "index probe records");
     if (st) {
         d->release();
         delete d;
@@ -457,6 +477,7 @@ extern "C" int excl_index_upload(excl_ctx *ctx, excl_index *ix) {
     up(d->post_base, pb.data(), pb.size() * 8);
     up(d->seg_list, slist.data(), slist.size() * 4);
     up(d->seg_gword, sgw.data(), sgw.size() * 8);
+    up(d->seg_probe, prec.data(), prec.size() * sizeof(ProbeRec));
     if (st) {
         d->release();
         delete d;
@@ -464,7 +485,8 @@ extern "C" int excl_index_upload(excl_ctx *ctx, excl_index *ix) {
     }
     d->bytes = ix->lists.size() * sizeof(ListDesc) + ix->words.size() * 4 + ix->seg_head.size() * 4 +
                ix->seg_rec.size() * sizeof(SegRec) + ix->seg_reg.size() * sizeof(SegReg) + ix->dir.size() * 4 +
-               ix->tilemap.size() * 8 + pb.size() * 8 + slist.size() * 4 + sgw.size() * 8;
+               ix->tilemap.size() * 8 + pb.size() * 8 + slist.size() * 4 + sgw.size() * 8 +
+               prec.size() * sizeof(ProbeRec);
     d->device = ctx->device;
     ix->dev = d;
     if (ix->models) st = models_upload(ctx, ix);
@@ -608,12 +630,12 @@ extern "C" int excl_autotune(excl_ctx *ctx, excl_index *ix, const uint32_t *term
         return EXCL_OK;
     };
     std::memset(rep, 0, sizeof *rep);
-    s = time_one(EXCL_ALGO_AUTO, 8, 8, 2, &rep->default_ms);
+    s = time_one(EXCL_ALGO_AUTO, 8, 5, 2, &rep->default_ms);
     float best = rep->default_ms;
     uint32_t ba = EXCL_ALGO_AUTO, bm = 2;
-    int bw = 8, bc = 8;
+    int bw = 8, bc = 5;
     const uint32_t algos[3] = {EXCL_ALGO_BSEARCH, EXCL_ALGO_HASHSEG, EXCL_ALGO_LEARNED};
-    const int warps[2] = {4, 8}, ctas[3] = {2, 4, 8};
+    const int warps[2] = {4, 8}, ctas[3] = {4, 5, 6};
     const uint32_t merges[4] = {0u, 1u, 2u, 4u};
     uint32_t tried = 1;
     for (uint32_t a : algos) {

@@ -21,6 +21,7 @@ struct DeviceIndex {
     uint64_t *post_base = nullptr;
     uint32_t *seg_list = nullptr;
     uint64_t *seg_gword = nullptr;
+    ProbeRec *seg_probe = nullptr;
     size_t bytes = 0;
     int device = 0;
     void release();

@@ -268,7 +268,7 @@ int launch_on_slot(excl_server *s, Slot *sl, uint64_t nterms, uint64_t tiles, ui
     bl.cap = s->cfg.max_batch_keys;
     bl.algo = (int)s->cfg.algo;
     bl.warps = s->cfg.warps_per_cta ? (int)s->cfg.warps_per_cta : 8;
-    bl.ctas_per_sm = s->cfg.ctas_per_sm ? (int)s->cfg.ctas_per_sm : 8;
+    bl.ctas_per_sm = s->cfg.ctas_per_sm ? (int)s->cfg.ctas_per_sm : 5;
     bl.nsm = s->nsm;
     bl.ev = nullptr;
     if (launch_batch(bl, st)) return EXCL_E_CUDA;

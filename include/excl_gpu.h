@@ -119,8 +119,9 @@ typedef struct {
     uint32_t max_queries;    /* per batch (reference: 16380-word constant image, ParaPFD_Intersection_kernel.cu:134) */
     uint32_t max_terms;      /* per query, <= 32 (reference MAX_QUERY_LEN 80, of which 8 are used by the workloads) */
     uint64_t max_keys;       /* per batch, sum of shortest-list lengths (reference baseSize) */
-    uint32_t warps_per_cta;  /* probe kernel launch shape (0 = autotuned/default) */
-    uint32_t ctas_per_sm;
+    uint32_t warps_per_cta;  /* probe kernel: 4 or 8 warps per CTA (0 = 8) */
+    uint32_t ctas_per_sm;    /* probe kernel: 4, 5 or 6 resident 8-warp CTAs per SM, i.e. a register
+                                budget of 64, 48 or 40 per thread (0 = 5) */
     uint32_t use_graphs;     /* 1: excl_intersect_device replays a CUDA graph of the batch's three
                                 kernels when called again with the same arguments (per-kernel
                                 times in excl_last_stats are then 0; total_ms stays) */
@@ -215,7 +216,7 @@ int excl_last_stats(excl_ctx *ctx, excl_batch_stats *st);
 typedef struct {
     uint32_t algo, warps_per_cta, ctas_per_sm, merge_segs; /* the setting kept */
     float best_ms;     /* its device time for the sample */
-    float default_ms;  /* device time of the untuned default (auto, 8 warps, 8 CTAs/SM, merge 2) */
+    float default_ms;  /* device time of the untuned default (auto, 8 warps, 5 CTAs/SM, merge 2) */
     uint32_t tried;    /* candidates timed */
 } excl_tune_report;
 int excl_autotune(excl_ctx *ctx, excl_index *ix, const uint32_t *terms, const uint32_t *term_offsets, uint32_t nq,
