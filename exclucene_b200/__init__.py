@@ -7,8 +7,9 @@ is its ctypes binding. Importing it without the built library raises.
 """
 from .api import (ALGO_AUTO, ALGO_BSEARCH, ALGO_HASHSEG, ALGO_LEARNED, CODEC_HS_PARAPFD, CODEC_HS_SEGLRC, CODEC_LRC,
                   CODEC_LRCSEG, CODEC_PARAPFD, CODEC_SEGLRC, Batch, Context, ExclError, Index, checksum,
-                  Server, encode_array_compat, library_path, parapfd_decode, parapfd_encode)
+                  Server, encode_array_compat, library_path, parapfd_decode, parapfd_encode, query_encode,
+                  query_parse)
 
-__all__ = ["Context", "Index", "Batch", "Server", "ExclError", "checksum", "parapfd_encode", "parapfd_decode",
+__all__ = ["Context", "Index", "Batch", "Server", "query_parse", "query_encode", "ExclError", "checksum", "parapfd_encode", "parapfd_decode",
            "encode_array_compat", "library_path", "CODEC_PARAPFD", "CODEC_LRC", "CODEC_LRCSEG", "CODEC_SEGLRC",
            "CODEC_HS_SEGLRC", "CODEC_HS_PARAPFD", "ALGO_AUTO", "ALGO_BSEARCH", "ALGO_HASHSEG", "ALGO_LEARNED"]

@@ -130,6 +130,12 @@ _check = _sig("excl_ctx_check", C.c_int, C.c_void_p)
 _stats = _sig("excl_last_stats", C.c_int, C.c_void_p, C.POINTER(BatchStats))
 _checksum = _sig("excl_checksum", C.c_int, C.c_uint32, u32p, u32p, C.POINTER(C.c_uint64 * 3))
 
+_save_ref = _sig("excl_index_save_reference", C.c_int, C.c_void_p, C.c_char_p, C.c_char_p)
+_load_ref = _sig("excl_index_load_reference", C.c_int, C.c_char_p, C.c_char_p, C.c_uint32, C.POINTER(C.c_void_p))
+_qparse = _sig("excl_query_parse", C.c_int, C.c_void_p, C.c_size_t, u32p, C.c_size_t, u32p, C.c_size_t,
+               C.POINTER(C.c_uint32), C.POINTER(C.c_size_t))
+_qencode = _sig("excl_query_encode", C.c_int, u32p, u32p, C.c_uint32, C.c_void_p, C.c_size_t,
+                C.POINTER(C.c_size_t))
 _autotune = _sig("excl_autotune", C.c_int, C.c_void_p, C.c_void_p, u32p, u32p, C.c_uint32, C.POINTER(TuneReport))
 _learn = _sig("excl_learn_models", C.c_int, C.c_void_p, C.c_void_p, C.POINTER(LearnParams), C.POINTER(LearnReport))
 _mexport = _sig("excl_model_export", C.c_int, C.c_void_p, C.c_uint32, C.POINTER(C.c_float), C.POINTER(C.c_float),
@@ -239,6 +245,22 @@ class Index:
         self._codecs = None
         self.list_lengths = np.asarray(lengths, dtype=np.uint64)
         return self
+
+    def save_reference(self, directory: str, name: str) -> None:
+        """Write the reference's file set (ParaPFD or SegLRC, 256-entry segments)."""
+        _check_status(_save_ref(self._h, directory.encode(), name.encode()), what="excl_index_save_reference")
+
+    @classmethod
+    def load_reference(cls, directory: str, name: str, codec="parapfd") -> "Index":
+        """Load a reference file set (ParaPFD or SegLRC) without re-encoding."""
+        c = CODEC_NAMES[codec] if isinstance(codec, str) else int(codec)
+        h = C.c_void_p()
+        _check_status(_load_ref(directory.encode(), name.encode(), c, C.byref(h)), what="excl_index_load_reference")
+        s = IndexSizes()
+        _check_status(_isizes(h, C.byref(s)))
+        lists = (ListInfo * s.nlists)()
+        _check_status(_iexport(h, lists, None, None, None, None, None))
+        return cls.from_handle(h, s.nlists, [lists[i].n for i in range(s.nlists)])
 
     def sizes(self) -> IndexSizes:
         s = IndexSizes()
@@ -433,6 +455,29 @@ def checksum(offsets, docids) -> tuple[int, int, int]:
     return int(cs[0]), int(cs[1]), int(cs[2])
 
 
+def query_parse(data: bytes) -> tuple[np.ndarray, np.ndarray]:
+    """A reference .query stream -> (terms, term_offsets)."""
+    buf = C.create_string_buffer(bytes(data), len(data))
+    nq, nt = C.c_uint32(), C.c_size_t()
+    _check_status(_qparse(buf, len(data), None, 0, None, 0, C.byref(nq), C.byref(nt)), what="excl_query_parse")
+    terms = np.zeros(max(nt.value, 1), np.uint32)
+    toff = np.zeros(nq.value + 1, np.uint32)
+    _check_status(_qparse(buf, len(data), _p32(terms), nt.value, _p32(toff), nq.value + 1, C.byref(nq),
+                          C.byref(nt)), what="excl_query_parse")
+    return terms[:nt.value], toff
+
+
+def query_encode(terms, term_offsets) -> bytes:
+    """(terms, term_offsets) -> a reference .query stream."""
+    t = _u32(terms) if len(terms) else np.zeros(1, np.uint32)
+    o = _u32(term_offsets)
+    nb = C.c_size_t()
+    _check_status(_qencode(_p32(t), _p32(o), len(o) - 1, None, 0, C.byref(nb)))
+    buf = C.create_string_buffer(max(nb.value, 1))
+    _check_status(_qencode(_p32(t), _p32(o), len(o) - 1, buf, nb.value, C.byref(nb)))
+    return buf.raw[:nb.value]
+
+
 def library_path() -> str:
     return _LIB_PATH
 
@@ -488,7 +533,8 @@ _srv_stats = _sig("excl_server_stats_get", C.c_int, C.c_void_p, C.POINTER(Server
 _srv_reset = _sig("excl_server_stats_reset", C.c_int, C.c_void_p)
 _srv_replay = _sig("excl_server_replay", C.c_int, C.c_void_p, u32p, u32p, C.c_uint32, C.POINTER(C.c_double),
                    C.POINTER(C.c_double), C.POINTER(C.c_uint64 * 3), C.POINTER(C.c_double))
-EXPORTED += ["excl_autotune", "excl_server_create", "excl_server_destroy", "excl_server_submit", "excl_server_wait",
+EXPORTED += ["excl_index_save_reference", "excl_index_load_reference", "excl_query_parse", "excl_query_encode",
+             "excl_autotune", "excl_server_create", "excl_server_destroy", "excl_server_submit", "excl_server_wait",
              "excl_server_stats_get", "excl_server_stats_reset", "excl_server_replay",
              "excl_intersect_device_noalloc"]
 

@@ -245,6 +245,20 @@ static inline int32_t f2i_sat(float v) {
 // ---------------------------------------------------------------------------
 // One list -> blocks + metadata.
 
+void fixed_list_directory(ListDesc &d, const uint32_t *head, uint32_t ns, std::vector<uint32_t> &dir) {
+    const int sh = (int)nbits(d.last_doc) - (int)nbits(ns);
+    d.dir_shift = (uint32_t)std::max(sh, 0);
+    d.ndir = (uint32_t)(((uint64_t)d.last_doc >> d.dir_shift) + 1);
+    dir.assign((size_t)d.ndir + 1, 0);
+    uint32_t s = 0;
+    for (uint32_t b = 0; b <= d.ndir; ++b) {
+        while (s < ns && ((uint64_t)head[s] >> d.dir_shift) < b) ++s;
+        dir[b] = s;
+    }
+}
+
+int32_t seg_pred_host(uint32_t idx, float a, float b) { return f2i_sat(std::fmaf((float)idx, a, b)); }
+
 struct ListOut {
     ListDesc d{};
     std::vector<uint32_t> words, head, dir;
@@ -409,15 +423,7 @@ static void build_list(const uint32_t *docs, uint32_t n, uint32_t codec, const e
     if (codec_is_hs(codec)) {
         o.dir = bfirst;
     } else {
-        const int sh = (int)nbits(d.last_doc) - (int)nbits(ns);
-        d.dir_shift = (uint32_t)std::max(sh, 0);
-        d.ndir = (uint32_t)(((uint64_t)d.last_doc >> d.dir_shift) + 1);
-        o.dir.assign(d.ndir + 1, 0);
-        uint32_t s = 0;
-        for (uint32_t b = 0; b <= d.ndir; ++b) {
-            while (s < ns && ((uint64_t)o.head[s] >> d.dir_shift) < b) ++s;
-            o.dir[b] = s;
-        }
+        fixed_list_directory(d, o.head.data(), ns, o.dir);
     }
 
     // Tiles (when this list is a query's shortest): one per fixed segment, or

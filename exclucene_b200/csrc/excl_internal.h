@@ -112,6 +112,11 @@ uint32_t pfd_decode_block(const uint32_t *in, uint32_t n, uint32_t *out);
 uint32_t pfd_block_words(const uint32_t *in, uint32_t n);
 int build_index(const uint32_t *docs, const uint64_t *loff, uint32_t nlists, const excl_build_params &p,
                 HostIndex &ix, std::string &err);
+// Top-bits directory of a fixed-block list (about one segment per bucket);
+// sets d.dir_shift / d.ndir from d.last_doc.
+void fixed_list_directory(ListDesc &d, const uint32_t *head, uint32_t ns, std::vector<uint32_t> &dir);
+// SegLRC/LRCSeg/HS prediction (int)(idx * a + b) with one rounding, saturating.
+int32_t seg_pred_host(uint32_t idx, float a, float b);
 
 }  // namespace excl
 

@@ -112,6 +112,31 @@ int excl_index_export(const excl_index *ix, excl_list_info *lists, uint32_t *wor
                       uint32_t *dir);
 
 /* ---------------------------------------------------------------------------
+ * The reference's on-disk files. An index in the ParaPFD or SegLRC format with
+ * 256-entry segments (SegmentSize of the reference encoders) is written as the
+ * file set its intersection binaries read, and such a file set is loaded
+ * without re-encoding: `<dir>/<name>` + .ind1 .ind2 .segNum .segHead .segOffset
+ * and, for ParaPFD, .segMedian (ParaPFD_Compression/main.cpp:81-232); for
+ * SegLRC, .ind2_distance_base .regression_info .regression_info_list
+ * (SegLRC_Compression/main.cpp:80-207, SegLRC_Generator.cu:338-412; the
+ * reference keeps these three in a second directory). .ind1 records are
+ * {u32 length; u64 byte offset}, 16 bytes (main.cpp:32-35). Loading checks
+ * that lists, segments and blocks are consistent and in bounds
+ * (EXCL_E_FORMAT otherwise). */
+int excl_index_save_reference(const excl_index *ix, const char *dir, const char *name);
+int excl_index_load_reference(const char *dir, const char *name, uint32_t codec /* PARAPFD or SEGLRC */,
+                              excl_index **out);
+
+/* The reference's .query stream (ParaPFD_Intersection.cu:139-142): per query a
+ * u32 term count, then the term ids. Parse into CSR form; with null outputs it
+ * only counts (nq, nterms), so a caller can size the buffers first. */
+int excl_query_parse(const void *buf, size_t bytes, uint32_t *terms, size_t terms_cap, uint32_t *term_offsets,
+                     size_t queries_cap, uint32_t *nq, size_t *nterms);
+/* Encode CSR queries as a .query stream; with buf = NULL only *bytes is set. */
+int excl_query_encode(const uint32_t *terms, const uint32_t *term_offsets, uint32_t nq, void *buf, size_t cap,
+                      size_t *bytes);
+
+/* ---------------------------------------------------------------------------
  * Context and device residency. One context per device; its own streams. */
 typedef struct excl_ctx excl_ctx;
 

@@ -79,10 +79,76 @@ def inverted_list_digest():
             f.write(f"frac {frac} words {nw} sha256 {h}\n")
 
 
+def reference_file_sets():
+    """The reference's compressed file sets for a small seeded corpus, laid out
+    as its compressors write them (ParaPFD_Compression/main.cpp:81-232,
+    SegLRC_Compression/main.cpp:80-207), every block encoded by the reference's
+    own ParaPFor.cpp. ParaPFD: d-gaps over the whole list, FRAC 0.12. SegLRC:
+    per-segment and per-list fits from the reference's getRegressionInfo (the
+    oracle's restated fit is pinned to it by regression_fits.npz), residuals
+    doc - (int)(i * a + b) minus the segment minimum, FRAC 0."""
+    import struct
+
+    rng = np.random.default_rng(0xF11E5)
+    lens = [1, 100, 255, 256, 257, 700, 2000, 5000]
+    lists = [np.sort(rng.choice(1 << 22, size=n, replace=False)).astype(np.uint32) for n in lens]
+    out = {"docs": np.concatenate(lists), "lens": np.array(lens, np.uint32)}
+    for codec, name, frac in ((0, "parapfd", 0.12), (3, "seglrc", 0.0)):
+        ind1, ind2, seg_num, heads, offs, aux, reg, listreg = b"", [], [], [], [], [], [], []
+        words_total = 0
+        for d in lists:
+            n = len(d)
+            seg_num.append(len(heads))
+            if codec == 0:
+                gaps = np.empty_like(d)
+                gaps[0] = d[0]
+                gaps[1:] = np.diff(d)
+                vals, med = gaps, [int(d[s + min(256, n - s) // 2]) for s in range(0, n, 256)]
+                segvals = [vals[s:s + 256] for s in range(0, n, 256)]
+            else:
+                enc = oracle.encode_list(d, 3, 256, 0.0)
+                segvals = [oracle.decode_block(enc["words"][o:], int(c))[0] for o, c in zip(enc["off"], enc["counts"])]
+                med = [int(x) for x in enc["aux"]]
+                reg.append(enc["reg"].astype(np.uint32))
+                listreg.append(enc["listreg"].astype(np.uint32))
+                for k, (s0, c) in enumerate(zip(enc["starts"], enc["counts"])):
+                    raw = oracle.ref_fit_seg_raw(d[s0:s0 + c])
+                    assert np.array_equal(raw, enc["reg"][k]), "oracle segment fit differs from the reference's"
+                assert np.array_equal(oracle.ref_fit_seg_raw(d), enc["listreg"]), "list fit differs"
+            ind1 += struct.pack("<IIQ", n, 0, 4 * words_total)
+            nw = 0
+            for k, v in enumerate(segvals):
+                heads.append(int(d[256 * k]))
+                offs.append(nw)
+                w = oracle.ref_encode(np.ascontiguousarray(v, np.uint32), frac)
+                ind2.append(w)
+                nw += len(w)
+            aux.extend(med)
+            words_total += nw
+        files = {".ind1": np.frombuffer(ind1, np.uint8),
+                 ".ind2": np.concatenate(ind2).view(np.uint8),
+                 ".segNum": np.array(seg_num, np.uint32).view(np.uint8),
+                 ".segHead": np.array(heads, np.uint32).view(np.uint8),
+                 ".segOffset": np.array(offs, np.uint32).view(np.uint8)}
+        if codec == 0:
+            files[".segMedian"] = np.array(aux, np.uint32).view(np.uint8)
+        else:
+            files[".ind2_distance_base"] = np.array(aux, np.uint32).view(np.uint8)
+            files[".regression_info"] = np.concatenate(reg).reshape(-1).view(np.uint8)
+            files[".regression_info_list"] = np.stack(listreg).reshape(-1).view(np.uint8)
+        for suffix, data in files.items():
+            out[name + suffix] = data
+    # a .query stream over the corpus (ParaPFD_Intersection.cu:139-142)
+    q = [[6, 7], [5, 6, 7], [0, 7], [7, 4, 3], [2, 2], [1]]
+    out["queries"] = np.array([x for t in q for x in [len(t)] + t], np.uint32).view(np.uint8)
+    np.savez_compressed(os.path.join(OUT, "reference_files.npz"), **out)
+
+
 if __name__ == "__main__":
     assert oracle.have_ref_codec() and oracle.have_ref_fit(), "build the reference first: make -C oracle ref"
     codec_vectors()
     fit_vectors()
+    reference_file_sets()
     if os.path.exists(INVERTED_LIST):
         inverted_list_digest()
     print("golden fixtures written to", OUT)

@@ -193,3 +193,30 @@ def test_autotune_keeps_output_exact(corpus, expected):
     finally:
         ix.close()
         ctx.close()
+
+
+@pytest.mark.parametrize("codec", ["parapfd", "seglrc"])
+def test_reference_file_set_runs_unchanged(gpu_ctx, tmp_path, codec):
+    """A file set written as the reference's compressors write it (blocks from
+    its own encoder) loads without re-encoding, decodes to its lists and
+    answers its .query stream as the oracle does."""
+    import os
+
+    g = dict(np.load(os.path.join(os.path.dirname(__file__), "golden", "reference_files.npz")))
+    sets = {"parapfd": (".ind1", ".ind2", ".segNum", ".segHead", ".segOffset", ".segMedian"),
+            "seglrc": (".ind1", ".ind2", ".segNum", ".segHead", ".segOffset", ".ind2_distance_base",
+                       ".regression_info", ".regression_info_list")}
+    for suffix in sets[codec]:
+        g[codec + suffix].tofile(os.path.join(tmp_path, "g" + suffix))
+    ix = ex.Index.load_reference(str(tmp_path), "g", codec)
+    gpu_ctx.upload(ix)
+    docs = g["docs"]
+    loff = np.concatenate([[0], np.cumsum(g["lens"].astype(np.uint64))]).astype(np.uint64)
+    assert np.array_equal(gpu_ctx.decode_lists(ix), docs)
+    terms, toff = ex.query_parse(g["queries"].tobytes())
+    eoffs, edocs = oracle.answer(docs, loff, terms, toff)
+    for algo in ("bsearch", "hashseg"):
+        offs, got = gpu_ctx.intersect(ix, terms, toff, algo=algo)
+        assert np.array_equal(offs.astype(np.uint64), eoffs)
+        assert np.array_equal(got, edocs)
+    ix.close()
