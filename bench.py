@@ -360,7 +360,9 @@ def main():
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
 
+    t_build = time.perf_counter()
     ix = ex.Index(w.docs, w.list_offsets, **params)
+    host_build_s = time.perf_counter() - t_build
     lens = np.diff(w.list_offsets).astype(np.int64)
     shortest = sum(int(min(lens[w.terms[w.term_offsets[q]:w.term_offsets[q + 1]]], default=0)) for q in range(w.nq))
     ctx = ex.Context(local, max_queries=max(w.nq, 1024), max_keys=max(1 << 20, 2 * shortest))
@@ -375,6 +377,25 @@ def main():
         learn["min_postings"] = lmin
     sizes = ix.sizes()
     arrays = ix.export()
+    index_build = None
+    if params["codec"] in ("parapfd", "seglrc") and "codecs" not in params:
+        # the same index built by the device kernels, from the docIDs in HBM
+        d_all = torch.from_numpy(w.docs.view(np.int32)).to(dev)
+        torch.cuda.synchronize()
+        ctx.build_index(d_all.data_ptr(), w.list_offsets, codec=params["codec"], block=params["block"],
+                        frac=params["frac"]).close()  # warm-up
+        t_build = time.perf_counter()
+        dix = ctx.build_index(d_all.data_ptr(), w.list_offsets, codec=params["codec"], block=params["block"],
+                              frac=params["frac"])
+        dev_build_s = time.perf_counter() - t_build
+        da = dix.export()
+        same = all(np.array_equal(getattr(da, k), getattr(arrays, k)) for k in ("words", "seg_head", "seg_rec",
+                                                                                 "seg_reg", "dir"))
+        dix.close()
+        del d_all
+        index_build = {"host_s": host_build_s, "host_threads": os.cpu_count(), "device_s": dev_build_s,
+                       "device_image_identical": bool(same),
+                       "device_note": "fits, residuals, blocks on the GPU; includes copying the image to the host"}
     stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
 
     d_terms = torch.from_numpy(w.terms.astype(np.int32)).to(dev)
@@ -493,6 +514,7 @@ def main():
                                  min(per_algo["learned"][0], per_algo_graph["learned"][0]))
         if "learned" in per_algo and "bsearch" in per_algo else None,
         "learned_models": learn,
+        "index_build": index_build,
         "autotune": tune,
         "per_algo_postings_per_s": {a: world * postings / (min(per_algo[a][0], per_algo_graph[a][0]) / 1e3)
                                     for a in per_algo},

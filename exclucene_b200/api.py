@@ -130,6 +130,8 @@ _check = _sig("excl_ctx_check", C.c_int, C.c_void_p)
 _stats = _sig("excl_last_stats", C.c_int, C.c_void_p, C.POINTER(BatchStats))
 _checksum = _sig("excl_checksum", C.c_int, C.c_uint32, u32p, u32p, C.POINTER(C.c_uint64 * 3))
 
+_build_dev = _sig("excl_index_build_device", C.c_int, C.c_void_p, C.c_void_p, u64p, C.c_uint32, C.POINTER(BuildParams),
+                  C.POINTER(C.c_void_p))
 _save_ref = _sig("excl_index_save_reference", C.c_int, C.c_void_p, C.c_char_p, C.c_char_p)
 _load_ref = _sig("excl_index_load_reference", C.c_int, C.c_char_p, C.c_char_p, C.c_uint32, C.POINTER(C.c_void_p))
 _qparse = _sig("excl_query_parse", C.c_int, C.c_void_p, C.c_size_t, u32p, C.c_size_t, u32p, C.c_size_t,
@@ -396,6 +398,20 @@ class Context:
                              g.ctypes.data_as(fp), C.byref(loss)), self, "excl_model_grad")
         return g, loss.value
 
+    def build_index(self, d_docs: int, list_offsets, codec="seglrc", block: int = 256, frac: float = 0.0) -> Index:
+        """Build a ParaPFD or SegLRC index on this context's GPU from a device
+        docID array (pointer; list l = d_docs[list_offsets[l] .. list_offsets[l+1])).
+        Byte-identical to Index(docs, list_offsets, ...); upload it before use."""
+        loff = np.ascontiguousarray(list_offsets, dtype=np.uint64)
+        p = BuildParams()
+        p.codec = CODEC_NAMES[codec] if isinstance(codec, str) else int(codec)
+        p.block = block
+        p.frac = frac
+        h = C.c_void_p()
+        _check_status(_build_dev(self._h, C.c_void_p(d_docs), loff.ctypes.data_as(u64p), len(loff) - 1, C.byref(p),
+                                 C.byref(h)), self, "excl_index_build_device")
+        return Index.from_handle(h, len(loff) - 1, np.diff(loff))
+
     def autotune(self, ix: Index, terms, term_offsets) -> dict:
         """Times the sample batch under every candidate setting and keeps the
         fastest for later batches run with algo="auto"."""
@@ -533,7 +549,7 @@ _srv_stats = _sig("excl_server_stats_get", C.c_int, C.c_void_p, C.POINTER(Server
 _srv_reset = _sig("excl_server_stats_reset", C.c_int, C.c_void_p)
 _srv_replay = _sig("excl_server_replay", C.c_int, C.c_void_p, u32p, u32p, C.c_uint32, C.POINTER(C.c_double),
                    C.POINTER(C.c_double), C.POINTER(C.c_uint64 * 3), C.POINTER(C.c_double))
-EXPORTED += ["excl_index_save_reference", "excl_index_load_reference", "excl_query_parse", "excl_query_encode",
+EXPORTED += ["excl_index_build_device", "excl_index_save_reference", "excl_index_load_reference", "excl_query_parse", "excl_query_encode",
              "excl_autotune", "excl_server_create", "excl_server_destroy", "excl_server_submit", "excl_server_wait",
              "excl_server_stats_get", "excl_server_stats_reset", "excl_server_replay",
              "excl_intersect_device_noalloc"]

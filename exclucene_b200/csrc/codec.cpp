@@ -259,6 +259,11 @@ void fixed_list_directory(ListDesc &d, const uint32_t *head, uint32_t ns, std::v
 
 int32_t seg_pred_host(uint32_t idx, float a, float b) { return f2i_sat(std::fmaf((float)idx, a, b)); }
 
+SegReg fit_host(const uint32_t *y, uint32_t n) {
+    const Fit f = fit_segment(y, n);
+    return SegReg{f.a, f.b, f.L, f.R};
+}
+
 struct ListOut {
     ListDesc d{};
     std::vector<uint32_t> words, head, dir;

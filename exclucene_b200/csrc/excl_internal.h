@@ -117,6 +117,8 @@ int build_index(const uint32_t *docs, const uint64_t *loff, uint32_t nlists, con
 void fixed_list_directory(ListDesc &d, const uint32_t *head, uint32_t ns, std::vector<uint32_t> &dir);
 // SegLRC/LRCSeg/HS prediction (int)(idx * a + b) with one rounding, saturating.
 int32_t seg_pred_host(uint32_t idx, float a, float b);
+// The least-squares fit of SegLRC/LRCSeg (segment or list level) on the host.
+SegReg fit_host(const uint32_t *y, uint32_t n);
 
 }  // namespace excl
 

@@ -88,6 +88,19 @@ int excl_index_build(const uint32_t *docs, const uint64_t *list_offsets, uint32_
                      const excl_build_params *params, excl_index **out);
 int excl_index_free(excl_index *ix);
 
+/* The same build on the GPU, for the ParaPFD and SegLRC formats (one codec for
+ * all lists, `codecs` = NULL): regression fits, residuals and segment minima,
+ * d-gaps and medians, and the ParaPFD blocks are computed by kernels on the
+ * context's device (SegLRC_Generator.cu:94-436, ParaPFD_Compression/main.cpp:
+ * 163-189, ParaPFor.cpp:31-113, there run on the host). d_docs is the CSR docID
+ * array in device memory; list l is d_docs[list_offsets[l] .. list_offsets[l+1])
+ * (list_offsets on the host, nlists + 1 entries). The result
+ * is byte-identical to excl_index_build's and still has to be uploaded.
+ * Scratch: about 4 bytes per posting plus 100 bytes per segment, freed on return. */
+struct excl_ctx;
+int excl_index_build_device(struct excl_ctx *ctx, const uint32_t *d_docs, const uint64_t *list_offsets,
+                            uint32_t nlists, const excl_build_params *params, excl_index **out);
+
 /* Sizes and host arrays of a built index (for checkers and the file writers).
  * Layout per list: see excl_list_info. Per segment: head, rec {start, word
  * offset, aux (ParaPFD: median docID; residual codecs: base)}, reg {a, b, L, R}. */

@@ -1,0 +1,97 @@
+"""Index build on the GPU: for the ParaPFD and SegLRC formats the device build
+gives the host build's arrays bit for bit (fits, residual bases, medians,
+blocks, directories), rejects unordered lists, and the index it builds answers
+queries as the oracle does."""
+import numpy as np
+import pytest
+
+import exclucene_b200 as ex
+import oracle
+from exclucene_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ("word_base", "n", "seg_base", "nseg", "codec", "log2_block", "first_doc", "last_doc", "reg", "dir_shift",
+          "dir_base", "ndir", "tile_base", "ntiles", "model")
+
+
+def _same_index(a: ex.Index, b: ex.Index):
+    ea, eb = a.export(), b.export()
+    for k in ("words", "seg_head", "seg_rec", "seg_reg", "dir"):
+        assert np.array_equal(getattr(ea, k), getattr(eb, k)), k
+    for f in FIELDS:
+        assert np.array_equal(ea.lists[f], eb.lists[f]), f
+
+
+def _edge_lists():
+    rng = np.random.default_rng(3)
+    lists = [np.array([7], np.uint32), np.arange(1000, 1300, dtype=np.uint32),          # gaps of 1
+             np.array([0, 1, 2 ** 31, 2 ** 32 - 2], np.uint32),                          # huge gaps
+             np.sort(rng.choice(2 ** 32 - 1, 5000, replace=False)).astype(np.uint32),   # wide residuals
+             np.arange(0, 256 * 3, 3, dtype=np.uint32), np.arange(5, 5 + 257, dtype=np.uint32)]
+    docs = np.concatenate(lists)
+    return docs, np.concatenate([[0], np.cumsum([len(x) for x in lists])]).astype(np.uint64)
+
+
+@pytest.fixture(scope="module")
+def corpus():
+    return synth.zipf_corpus(seed=21, ndocs=1 << 20, nterms=2500, cap=150_000, nq=800, qmin=2, qmax=5)
+
+
+@pytest.mark.parametrize("codec,block,frac", [("parapfd", 256, 0.0), ("parapfd", 128, 0.12), ("parapfd", 256, 0.64),
+                                              ("seglrc", 256, 0.0), ("seglrc", 128, 0.1)])
+def test_device_build_equals_host_build(gpu_ctx, corpus, codec, block, frac):
+    import torch
+
+    for docs, loff in ((corpus.docs, corpus.list_offsets), _edge_lists()):
+        d = torch.from_numpy(docs.view(np.int32)).cuda()
+        torch.cuda.synchronize()
+        try:
+            got = gpu_ctx.build_index(d.data_ptr(), loff, codec=codec, block=block, frac=frac)
+        except ex.ExclError as e:
+            # where the host build rejects the data (unrepresentable block), so must the device
+            with pytest.raises(ex.ExclError):
+                ex.Index(docs, loff, codec=codec, block=block, frac=frac)
+            assert e.status == ex.api.E_FORMAT
+            continue
+        want = ex.Index(docs, loff, codec=codec, block=block, frac=frac)
+        _same_index(got, want)
+        got.close()
+        want.close()
+
+
+def test_device_build_of_a_list_range_and_queries(gpu_ctx, corpus):
+    import torch
+
+    # lists 100.. of the corpus, indexed through absolute offsets into the full array
+    loff = corpus.list_offsets[100:]
+    d = torch.from_numpy(corpus.docs.view(np.int32)).cuda()
+    torch.cuda.synchronize()
+    ix = gpu_ctx.build_index(d.data_ptr(), loff, codec="seglrc")
+    sub_docs = corpus.docs[int(loff[0]):int(loff[-1])]
+    sub_off = (loff - loff[0]).astype(np.uint64)
+    _same_index(ix, ex.Index(sub_docs, sub_off, codec="seglrc"))
+    gpu_ctx.upload(ix)
+    rng = np.random.default_rng(8)
+    nl = len(sub_off) - 1
+    qs = [rng.choice(nl, size=int(rng.integers(2, 5)), replace=False) for _ in range(300)]
+    terms = np.concatenate(qs).astype(np.uint32)
+    toff = np.concatenate([[0], np.cumsum([len(q) for q in qs])]).astype(np.uint32)
+    offs, got = gpu_ctx.intersect(ix, terms, toff, algo="hashseg")
+    eo, ed = oracle.answer(sub_docs, sub_off, terms, toff)
+    assert np.array_equal(offs.astype(np.uint64), eo) and np.array_equal(got, ed)
+    ix.close()
+
+
+def test_device_build_rejects_unordered_lists(gpu_ctx):
+    import torch
+
+    docs = np.array([5, 9, 9, 12, 1, 2, 3], np.uint32)  # list 0 repeats 9
+    d = torch.from_numpy(docs.view(np.int32)).cuda()
+    torch.cuda.synchronize()
+    for codec in ("parapfd", "seglrc"):
+        with pytest.raises(ex.ExclError) as e:
+            gpu_ctx.build_index(d.data_ptr(), np.array([0, 4, 7], np.uint64), codec=codec)
+        assert e.value.status == ex.api.E_INVALID
+    with pytest.raises(ex.ExclError):
+        gpu_ctx.build_index(d.data_ptr(), np.array([0, 4, 7], np.uint64), codec="lrc")  # host build only
