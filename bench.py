@@ -115,7 +115,7 @@ def algorithmic_bytes(w, arrays) -> int:
     seg_of_list = np.repeat(np.arange(len(lists)), nseg)
     gstart = lists["word_base"].astype(np.int64)[seg_of_list] + seg_rec[:nseg_all, 1].astype(np.int64)
     seg_words = np.diff(np.append(gstart, len(arrays.words) - 8))
-    codec_meta = {0: 12, 1: 8, 2: 12, 3: 28, 4: 28, 5: 12}
+    codec_meta = {0: 12, 1: 8, 2: 12, 3: 28, 4: 28, 5: 12, 6: 12}
     total = 0
     lens = np.diff(w.list_offsets).astype(np.int64)
     for q in range(w.nq):
@@ -264,7 +264,7 @@ def decode_measure(ctx, ix, w, sizes, arrays, stream, flush, args):
     import torch
 
     n = int(sizes.postings)
-    meta_per_seg = {0: 12, 1: 8, 2: 12, 3: 28, 4: 28, 5: 12}
+    meta_per_seg = {0: 12, 1: 8, 2: 12, 3: 28, 4: 28, 5: 12, 6: 12}
     codecs = arrays.lists["codec"].astype(np.int64)
     nseg = arrays.lists["nseg"].astype(np.int64)
     meta = int(sum(meta_per_seg[int(c)] * int(s) for c, s in zip(codecs, nseg)))

@@ -28,8 +28,8 @@ u64p = C.POINTER(C.c_uint64)
 OK, E_INVALID, E_CUDA, E_CAPACITY, E_FORMAT, E_TIMEOUT, E_DEVICE_FLAG, E_NOMEM = range(8)
 STATUS_NAMES = ["OK", "INVALID", "CUDA", "CAPACITY", "FORMAT", "TIMEOUT", "DEVICE_FLAG", "NOMEM"]
 
-CODEC_PARAPFD, CODEC_LRC, CODEC_LRCSEG, CODEC_SEGLRC, CODEC_HS_SEGLRC, CODEC_HS_PARAPFD = range(6)
-CODEC_NAMES = {"parapfd": 0, "lrc": 1, "lrcseg": 2, "seglrc": 3, "hs_seglrc": 4, "hs_parapfd": 5}
+CODEC_PARAPFD, CODEC_LRC, CODEC_LRCSEG, CODEC_SEGLRC, CODEC_HS_SEGLRC, CODEC_HS_PARAPFD, CODEC_NEWPFD = range(7)
+CODEC_NAMES = {"parapfd": 0, "lrc": 1, "lrcseg": 2, "seglrc": 3, "hs_seglrc": 4, "hs_parapfd": 5, "newpfd": 6}
 ALGO_AUTO, ALGO_BSEARCH, ALGO_HASHSEG, ALGO_LEARNED = range(4)
 ALGO_NAMES = {"auto": 0, "bsearch": 1, "hashseg": 2, "learned": 3}
 
@@ -107,6 +107,8 @@ def _sig(name, res, *args):
 _encode = _sig("excl_parapfd_encode", C.c_int, u32p, C.c_uint32, C.c_float, u32p, C.c_size_t, C.POINTER(C.c_size_t))
 _decode = _sig("excl_parapfd_decode", C.c_int, u32p, C.c_size_t, C.c_uint32, u32p, C.POINTER(C.c_size_t))
 _set_frac = _sig("excl_set_frac", None, C.c_float)
+_nencode = _sig("excl_newpfd_encode", C.c_int, u32p, C.c_uint32, C.c_float, u32p, C.c_size_t, C.POINTER(C.c_size_t))
+_ndecode = _sig("excl_newpfd_decode", C.c_int, u32p, C.c_size_t, C.c_uint32, u32p, C.POINTER(C.c_size_t))
 _encodeArray = _sig("encodeArray", C.c_uint32, u32p, u32p, C.c_uint32)
 _decodeArray = _sig("decodeArray", C.c_uint32, u32p, u32p, C.c_uint32)
 _build = _sig("excl_index_build", C.c_int, u32p, u64p, C.c_uint32, C.POINTER(BuildParams), C.POINTER(C.c_void_p))
@@ -187,6 +189,24 @@ def parapfd_decode(words, n: int) -> tuple[np.ndarray, int]:
     out = np.zeros(max(n, 1), dtype=np.uint32)
     used = C.c_size_t(0)
     _check_status(_decode(_p32(w), len(w), n, _p32(out), C.byref(used)), what="parapfd_decode")
+    return out[:n], used.value
+
+
+def newpfd_encode(values, frac: float = 0.0) -> np.ndarray:
+    """One NewPFD block (NewPFor.cpp:52-108)."""
+    v = _u32(values)
+    cap = 3 * len(v) + 8
+    out = np.zeros(cap, dtype=np.uint32)
+    w = C.c_size_t(0)
+    _check_status(_nencode(_p32(v), len(v), frac, _p32(out), cap, C.byref(w)), what="newpfd_encode")
+    return out[: w.value].copy()
+
+
+def newpfd_decode(words, n: int) -> tuple[np.ndarray, int]:
+    w = _u32(words)
+    out = np.zeros(max(n, 1), dtype=np.uint32)
+    used = C.c_size_t(0)
+    _check_status(_ndecode(_p32(w), len(w), n, _p32(out), C.byref(used)), what="newpfd_decode")
     return out[:n], used.value
 
 
@@ -549,7 +569,7 @@ _srv_stats = _sig("excl_server_stats_get", C.c_int, C.c_void_p, C.POINTER(Server
 _srv_reset = _sig("excl_server_stats_reset", C.c_int, C.c_void_p)
 _srv_replay = _sig("excl_server_replay", C.c_int, C.c_void_p, u32p, u32p, C.c_uint32, C.POINTER(C.c_double),
                    C.POINTER(C.c_double), C.POINTER(C.c_uint64 * 3), C.POINTER(C.c_double))
-EXPORTED += ["excl_index_build_device", "excl_index_save_reference", "excl_index_load_reference", "excl_query_parse", "excl_query_encode",
+EXPORTED += ["excl_newpfd_encode", "excl_newpfd_decode", "excl_index_build_device", "excl_index_save_reference", "excl_index_load_reference", "excl_query_parse", "excl_query_encode",
              "excl_autotune", "excl_server_create", "excl_server_destroy", "excl_server_submit", "excl_server_wait",
              "excl_server_stats_get", "excl_server_stats_reset", "excl_server_replay",
              "excl_intersect_device_noalloc"]

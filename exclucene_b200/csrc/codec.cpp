@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <thread>
 
@@ -81,6 +82,90 @@ static uint32_t best_b(const uint32_t *in, uint32_t n, float frac) {
     return 32;
 }
 
+// ---------------------------------------------------------------------------
+// NewPFD blocks (NewPFor.cpp:52-139): descriptor b << 26 | en, the b-bit low
+// parts, then one Simple-16 stream holding the exception positions (first
+// absolute, then gaps minus one) followed by their high parts.
+
+// Simple-16 word layouts (Zhang, Long and Suel, WWW 2008; the same 16 cases as
+// the reference's Simple16.h): a 4-bit selector and 28 data bits split into the
+// listed runs of equal widths, low bits first.
+struct S16Run {
+    uint8_t count, width;
+};
+static const S16Run kS16Runs[16][3] = {
+    {{28, 1}, {0, 0}, {0, 0}}, {{7, 2}, {14, 1}, {0, 0}}, {{7, 1}, {7, 2}, {7, 1}}, {{14, 1}, {7, 2}, {0, 0}},
+    {{14, 2}, {0, 0}, {0, 0}}, {{1, 4}, {8, 3}, {0, 0}},  {{1, 3}, {4, 4}, {3, 3}}, {{7, 4}, {0, 0}, {0, 0}},
+    {{4, 5}, {2, 4}, {0, 0}},  {{2, 4}, {4, 5}, {0, 0}},  {{3, 6}, {2, 5}, {0, 0}}, {{2, 5}, {3, 6}, {0, 0}},
+    {{4, 7}, {0, 0}, {0, 0}},  {{1, 10}, {2, 9}, {0, 0}}, {{2, 14}, {0, 0}, {0, 0}}, {{1, 28}, {0, 0}, {0, 0}},
+};
+
+struct S16Table {
+    uint8_t count[16];
+    uint8_t width[16][28];
+    S16Table() {
+        for (int k = 0; k < 16; ++k) {
+            int c = 0, bits = 0;
+            for (const S16Run &r : kS16Runs[k])
+                for (int j = 0; j < r.count; ++j, ++c) {
+                    width[k][c] = r.width;
+                    bits += r.width;
+                }
+            count[k] = (uint8_t)c;
+            if (bits != 28) std::abort();  // every layout fills the 28 data bits
+        }
+    }
+};
+static const S16Table &s16() {
+    static const S16Table t;
+    return t;
+}
+
+// Appends v[0..n) as Simple-16 words: each word takes the first layout whose
+// widths hold the next min(count, left) values. False if a value needs more
+// than 28 bits (no layout holds it).
+static bool s16_encode(const uint32_t *v, uint32_t n, std::vector<uint32_t> &out) {
+    const S16Table &t = s16();
+    uint32_t i = 0;
+    while (i < n) {
+        bool done = false;
+        for (int k = 0; k < 16 && !done; ++k) {
+            const uint32_t vol = std::min<uint32_t>(t.count[k], n - i);
+            uint32_t j = 0;
+            while (j < vol && (uint64_t)v[i + j] < (1ull << t.width[k][j])) ++j;
+            if (j < vol) continue;
+            uint32_t w = (uint32_t)k << 28, sh = 0;
+            for (j = 0; j < vol; ++j) {
+                w |= v[i + j] << sh;
+                sh += t.width[k][j];
+            }
+            out.push_back(w);
+            i += vol;
+            done = true;
+        }
+        if (!done) return false;
+    }
+    return true;
+}
+
+// Decodes Simple-16 words from `in` until n values are out; returns words read.
+static uint32_t s16_decode(const uint32_t *in, uint32_t n, uint32_t *out) {
+    const S16Table &t = s16();
+    uint32_t r = 0, i = 0;
+    while (i < n) {
+        const uint32_t w = in[r++], k = w >> 28;
+        uint32_t sh = 0;
+        for (uint32_t j = 0; j < t.count[k] && i < n; ++j) {
+            out[i++] = (w >> sh) & ((1u << t.width[k][j]) - 1u);
+            sh += t.width[k][j];
+        }
+    }
+    return r;
+}
+
+uint32_t newpfd_encode_block(const uint32_t *in, uint32_t n, float frac, uint32_t *out, int *err);
+uint32_t newpfd_decode_block(const uint32_t *in, uint32_t n, uint32_t *out);
+
 uint32_t pfd_encode_block(const uint32_t *in, uint32_t n, float frac, uint32_t *out, int *err) {
     *err = EXCL_OK;
     const uint32_t lb = best_b(in, n, frac);
@@ -126,6 +211,79 @@ uint32_t pfd_encode_block(const uint32_t *in, uint32_t n, float frac, uint32_t *
     return w;
 }
 
+uint32_t newpfd_encode_block(const uint32_t *in, uint32_t n, float frac, uint32_t *out, int *err) {
+    *err = EXCL_OK;
+    const uint32_t b = best_b(in, n, frac);
+    if (b >= 32) {
+        *err = EXCL_E_FORMAT;
+        return 0;
+    }
+    std::vector<uint32_t> low(n), pos, high;
+    const uint32_t lim = 1u << b;
+    for (uint32_t i = 0; i < n; ++i) {
+        low[i] = in[i] & (lim - 1u);
+        if (in[i] >= lim) {
+            pos.push_back(i);
+            high.push_back(in[i] >> b);
+        }
+    }
+    const uint32_t en = (uint32_t)pos.size();
+    if (en > 65535u) {
+        *err = EXCL_E_FORMAT;
+        return 0;
+    }
+    uint32_t w = 1;
+    pack_bits(low.data(), n, b, out + w);
+    w += (uint32_t)words_for(n, b);
+    out[0] = (b << 26) + en;
+    if (en == 0) return w;
+    // positions as gaps minus one after the first, then the high parts
+    std::vector<uint32_t> all(2 * (size_t)en), s16w;
+    for (uint32_t i = 0; i < en; ++i) {
+        all[i] = i ? pos[i] - pos[i - 1] - 1 : pos[0];
+        all[en + i] = high[i];
+    }
+    if (!s16_encode(all.data(), 2 * en, s16w)) {
+        *err = EXCL_E_FORMAT;  // an exception high part of more than 28 bits
+        return 0;
+    }
+    std::memcpy(out + w, s16w.data(), s16w.size() * 4);
+    return w + (uint32_t)s16w.size();
+}
+
+uint32_t newpfd_decode_block(const uint32_t *in, uint32_t n, uint32_t *out) {
+    const uint32_t b = (in[0] >> 26) & 31u, en = in[0] & 0xffffu;
+    uint32_t w = 1;
+    unpack_bits(in + w, n, b, out);
+    w += (uint32_t)words_for(n, b);
+    if (en) {
+        std::vector<uint32_t> all(2 * (size_t)en);
+        w += s16_decode(in + w, 2 * en, all.data());
+        uint32_t p = all[0];
+        for (uint32_t i = 0; i < en; ++i) {
+            if (i) p += all[i] + 1;
+            if (p < n) out[p] += all[en + i] << b;
+        }
+    }
+    return w;
+}
+
+uint64_t newpfd_block_words(const uint32_t *in, uint32_t n, uint64_t avail) {
+    if (avail == 0) return ~0ull;
+    const uint32_t b = (in[0] >> 26) & 31u, en = in[0] & 0xffffu;
+    uint64_t w = 1 + words_for(n, b);
+    if (en) {
+        // count the Simple-16 words that hold 2 * en values, never reading past avail
+        const S16Table &t = s16();
+        uint32_t got = 0;
+        while (got < 2 * en) {
+            if (w >= avail) return ~0ull;
+            got += t.count[in[w++] >> 28];
+        }
+    }
+    return w <= avail ? w : ~0ull;
+}
+
 uint32_t pfd_block_words(const uint32_t *in, uint32_t n) {
     const uint32_t d = in[0];
     const uint32_t lb = (d >> 26) & 31u, eb = (d >> 21) & 31u, hb = (d >> 16) & 31u, en = d & 0xffffu;
@@ -151,6 +309,7 @@ uint32_t pfd_decode_block(const uint32_t *in, uint32_t n, uint32_t *out) {
     }
     return w;
 }
+
 
 // ---------------------------------------------------------------------------
 // Regression fits (reference host arithmetic, see header comment).
@@ -414,8 +573,9 @@ static void build_list(const uint32_t *docs, uint32_t n, uint32_t codec, const e
         const uint32_t c = cnt[s];
         tmp.assign((size_t)c * 3 + 8, 0u);
         int err = 0;
-        const uint32_t w = pfd_encode_block(val.data() + st[s], c, p.frac, tmp.data(), &err);
-        if (err) return fail(o, err, "block not representable in ParaPFD (b = 32 or > 65535 exceptions)");
+        const uint32_t w = codec_is_newpfd(codec) ? newpfd_encode_block(val.data() + st[s], c, p.frac, tmp.data(), &err)
+                                                   : pfd_encode_block(val.data() + st[s], c, p.frac, tmp.data(), &err);
+        if (err) return fail(o, err, "block not representable (b = 32, > 65535 exceptions, or a NewPFD high part > 28 bits)");
         o.rec[s].start = st[s];
         o.rec[s].off = (uint32_t)o.words.size();
         o.rec[s].count = c;
@@ -468,7 +628,7 @@ int build_index(const uint32_t *docs, const uint64_t *loff, uint32_t nlists, con
     }
     for (uint32_t l = 0; l < nlists; ++l) {
         const uint32_t c = p.codecs ? p.codecs[l] : p.codec;
-        if (c > EXCL_CODEC_HS_PARAPFD) {
+        if (c > EXCL_CODEC_NEWPFD) {
             err = "unknown codec";
             return EXCL_E_INVALID;
         }

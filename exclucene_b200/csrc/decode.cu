@@ -183,7 +183,14 @@ __device__ __noinline__ void decode_dgap_staged(const uint32_t *blk, const RunMe
 #pragma unroll
         for (int q = 0; q < 8; ++q)
             if (q < (int)vpl && el + q < count) vbuf[el + q] = v[q];
-        patch_exceptions(lows, h, count, vbuf, lane);
+        if (codec_is_newpfd(m.codec)) {
+            // NewPFD: exceptions from the Simple-16 stream, one lane
+            __syncwarp();
+            if (lane == 0) newpfd_patch(lows + words_for(count, h.lb), h.en, h.lb, 0, count, vbuf);
+            __syncwarp();
+        } else {
+            patch_exceptions(lows, h, count, vbuf, lane);
+        }
 #pragma unroll
         for (int q = 0; q < 8; ++q)
             if (q < (int)vpl && el + q < count) v[q] = vbuf[el + q];

@@ -166,6 +166,74 @@ __device__ __forceinline__ uint32_t block_value_ra(const uint32_t *blk, const Bl
     return v;
 }
 
+// ---------------------------------------------------------------------------
+// NewPFD exceptions: one Simple-16 stream (NewPFor.cpp:91-106) holding the
+// exception positions (first absolute, then gaps minus one) and then their
+// high parts. Two cursors walk it in step: one over the positions, one
+// started past them over the high parts.
+
+// Simple-16 word layouts (the published 16 cases; also the reference's
+// Simple16.h): up to three runs of (count, width), low bits first.
+static __constant__ uint8_t kS16Dev[16][6] = {
+    {28, 1, 0, 0, 0, 0}, {7, 2, 14, 1, 0, 0}, {7, 1, 7, 2, 7, 1}, {14, 1, 7, 2, 0, 0},
+    {14, 2, 0, 0, 0, 0}, {1, 4, 8, 3, 0, 0},  {1, 3, 4, 4, 3, 3}, {7, 4, 0, 0, 0, 0},
+    {4, 5, 2, 4, 0, 0},  {2, 4, 4, 5, 0, 0},  {3, 6, 2, 5, 0, 0}, {2, 5, 3, 6, 0, 0},
+    {4, 7, 0, 0, 0, 0},  {1, 10, 2, 9, 0, 0}, {2, 14, 0, 0, 0, 0}, {1, 28, 0, 0, 0, 0}};
+
+struct S16Cursor {
+    const uint32_t *p;  // current word (global or shared memory)
+    uint32_t word, j, sh, left, run, width;  // value j of the word; `left` values remain in the current run
+};
+
+__device__ __forceinline__ void s16_load(S16Cursor &c) {
+    c.word = *c.p;
+    const uint32_t k = c.word >> 28;
+    c.j = 0;
+    c.sh = 0;
+    c.run = 0;
+    c.left = kS16Dev[k][0];
+    c.width = kS16Dev[k][1];
+}
+
+__device__ __forceinline__ void s16_start(S16Cursor &c, const uint32_t *p) {
+    c.p = p;
+    s16_load(c);
+}
+
+__device__ __forceinline__ uint32_t s16_next(S16Cursor &c) {
+    while (c.left == 0) {  // next run of the word, or the next word
+        const uint32_t k = c.word >> 28;
+        if (++c.run < 3 && kS16Dev[k][2 * c.run]) {
+            c.left = kS16Dev[k][2 * c.run];
+            c.width = kS16Dev[k][2 * c.run + 1];
+        } else {
+            ++c.p;
+            s16_load(c);
+        }
+    }
+    const uint32_t v = (c.word >> c.sh) & ((1u << c.width) - 1u);  // widths are <= 28
+    c.sh += c.width;
+    --c.left;
+    return v;
+}
+
+// Adds the high parts of a NewPFD block's exceptions at positions in
+// [e0, e0 + kc) to buf[pos - e0] (serial: one thread).
+__device__ __forceinline__ void newpfd_patch(const uint32_t *s16, uint32_t en, uint32_t b, uint32_t e0, uint32_t kc,
+                                             uint32_t *buf) {
+    S16Cursor pc, hc;
+    s16_start(pc, s16);
+    s16_start(hc, s16);
+    for (uint32_t i = 0; i < en; ++i) s16_next(hc);
+    uint32_t p = 0;
+    for (uint32_t i = 0; i < en; ++i) {
+        const uint32_t d = s16_next(pc);
+        p = i ? p + d + 1u : d;
+        const uint32_t h = s16_next(hc);
+        if (p >= e0 && p < e0 + kc) buf[p - e0] += h << b;
+    }
+}
+
 // Warp-cooperative decode of elements [e0, e0 + kc) (kc <= 256) of one
 // segment into buf[0 .. kc). Lane l owns elements l*vpl .. l*vpl+vpl-1 so its
 // bits are contiguous; exceptions are patched through `buf`; d-gap codecs
@@ -191,10 +259,14 @@ __device__ __forceinline__ void warp_decode(const DevIndexView &ix, const ListDe
             if (j < (int)vpl && el + j < kc) buf[el + j] = v[j];
         __syncwarp();
         const uint32_t *pb = blk + 1 + words_for(rec.count, h.lb);
-        const uint32_t *hp = pb + words_for(h.en, h.eb);
-        for (uint32_t x = lane; x < h.en; x += 32) {
-            const uint32_t p = get_bits(pb, x * h.eb, h.eb);
-            if (p >= e0 && p < e0 + kc) buf[p - e0] |= get_bits(hp, x * h.hb, h.hb) << h.lb;
+        if (codec_is_newpfd(L.codec)) {
+            if (lane == 0) newpfd_patch(pb, h.en, h.lb, e0, kc, buf);
+        } else {
+            const uint32_t *hp = pb + words_for(h.en, h.eb);
+            for (uint32_t x = lane; x < h.en; x += 32) {
+                const uint32_t p = get_bits(pb, x * h.eb, h.eb);
+                if (p >= e0 && p < e0 + kc) buf[p - e0] |= get_bits(hp, x * h.hb, h.hb) << h.lb;
+            }
         }
         __syncwarp();
 #pragma unroll
@@ -298,6 +370,67 @@ __device__ __forceinline__ bool dgap_find(const uint32_t *blk, const BlkHdr h, u
             g |= get_bits(hp, x * h.hb, h.hb) << h.lb;
             ++x;
             xp = x < h.en ? get_bits(pb, x * h.eb, h.eb) : 0xffffffffu;
+        }
+        v += g;
+        if (v >= key) return v == key;
+    }
+    return false;
+}
+
+// dgap_find for a NewPFD block: the same walk, exceptions read from the
+// block's Simple-16 stream with two cursors.
+__device__ __forceinline__ bool dgap_find_newpfd(const uint32_t *blk, const BlkHdr h, uint32_t count, uint32_t head,
+                                                 uint32_t median, uint32_t key) {
+    if (key == head || key == median) return true;
+    uint32_t from, end, v;
+    if (key > median) {
+        from = count >> 1;
+        end = count;
+        v = median;
+    } else {
+        from = 0;
+        end = count >> 1;
+        v = head;
+    }
+    const uint32_t *lows = blk + 1;
+    S16Cursor pc, hc;
+    uint32_t x = 0, p = 0, xp = 0xffffffffu, xh = 0;
+    if (h.en) {
+        const uint32_t *s16 = lows + words_for(count, h.lb);
+        s16_start(pc, s16);
+        s16_start(hc, s16);
+        for (uint32_t i = 0; i < h.en; ++i) s16_next(hc);
+        // the first exception after `from`
+        do {
+            p = x ? p + s16_next(pc) + 1u : s16_next(pc);
+            xh = s16_next(hc);
+            ++x;
+        } while (p <= from && x < h.en);
+        xp = p > from ? p : 0xffffffffu;
+    }
+    uint32_t bit = (from + 1) * h.lb;
+    uint32_t wi = bit >> 5;
+    uint64_t win = ((uint64_t)ldg(lows + wi + 1) << 32) | ldg(lows + wi);
+    uint32_t sh = bit & 31u;
+    const uint32_t mask = (1u << h.lb) - 1u;
+    for (uint32_t i = from + 1; i < end; ++i) {
+        uint32_t g = (uint32_t)(win >> sh) & mask;
+        sh += h.lb;
+        if (sh >= 32) {
+            sh -= 32;
+            ++wi;
+            win = (win >> 32) | ((uint64_t)ldg(lows + wi + 1) << 32);
+        }
+        if (i == xp) {
+            g += xh << h.lb;
+            if (x < h.en) {
+                p += s16_next(pc) + 1u;
+                xh = s16_next(hc);
+                ++x;
+                xp = p;
+            } else {
+                xp = 0xffffffffu;
+            }
         }
         v += g;
         if (v >= key) return v == key;

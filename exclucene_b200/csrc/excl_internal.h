@@ -86,7 +86,10 @@ static_assert(sizeof(ProbeRec) == 64, "ProbeRec layout");
 #endif
 
 EXCL_HD bool codec_is_hs(uint32_t c) { return c == EXCL_CODEC_HS_SEGLRC || c == EXCL_CODEC_HS_PARAPFD; }
-EXCL_HD bool codec_is_dgap(uint32_t c) { return c == EXCL_CODEC_PARAPFD || c == EXCL_CODEC_HS_PARAPFD; }
+EXCL_HD bool codec_is_dgap(uint32_t c) {
+    return c == EXCL_CODEC_PARAPFD || c == EXCL_CODEC_HS_PARAPFD || c == EXCL_CODEC_NEWPFD;
+}
+EXCL_HD bool codec_is_newpfd(uint32_t c) { return c == EXCL_CODEC_NEWPFD; }
 
 struct DeviceIndex;  // runtime.cu
 struct ModelSet;     // learned.cu
@@ -110,6 +113,11 @@ struct HostIndex {
 uint32_t pfd_encode_block(const uint32_t *in, uint32_t n, float frac, uint32_t *out, int *err);
 uint32_t pfd_decode_block(const uint32_t *in, uint32_t n, uint32_t *out);
 uint32_t pfd_block_words(const uint32_t *in, uint32_t n);
+uint32_t newpfd_encode_block(const uint32_t *in, uint32_t n, float frac, uint32_t *out, int *err);
+uint32_t newpfd_decode_block(const uint32_t *in, uint32_t n, uint32_t *out);
+// Words of a NewPFD block, found by walking its Simple-16 selectors without
+// reading past `avail` words (~0 if the block does not fit in them).
+uint64_t newpfd_block_words(const uint32_t *in, uint32_t n, uint64_t avail);
 int build_index(const uint32_t *docs, const uint64_t *loff, uint32_t nlists, const excl_build_params &p,
                 HostIndex &ix, std::string &err);
 // Top-bits directory of a fixed-block list (about one segment per bucket);

@@ -69,6 +69,7 @@ __device__ __forceinline__ bool probe_key(const DevIndexView &ix, const ListDesc
     rec.count = q0.w;
     const uint32_t *blk = ix.words + L.word_base + rec.off;
     const BlkHdr h = blk_hdr(q1.x);
+    if (codec_is_newpfd(L.codec)) return dgap_find_newpfd(blk, h, rec.count, q0.x, rec.aux, key);
     if (codec_is_dgap(L.codec)) return dgap_find(blk, h, rec.count, q0.x, rec.aux, key);
     // list position of the segment: only learned windows and the LRC/LRCSeg
     // predictors use it, and those lists have fixed blocks

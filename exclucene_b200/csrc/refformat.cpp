@@ -77,7 +77,9 @@ bool read_file(const std::string &p, std::vector<T> &out) {
     return ok;
 }
 
-bool reference_codec(uint32_t c) { return c == EXCL_CODEC_PARAPFD || c == EXCL_CODEC_SEGLRC; }
+bool reference_codec(uint32_t c) {
+    return c == EXCL_CODEC_PARAPFD || c == EXCL_CODEC_SEGLRC || c == EXCL_CODEC_NEWPFD;
+}
 
 }  // namespace
 
@@ -107,7 +109,7 @@ extern "C" int excl_index_save_reference(const excl_index *ix, const char *dir, 
               write_file(path_of(dir, name, ".segNum"), seg_num.data(), seg_num.size() * 4) &&
               write_file(path_of(dir, name, ".segHead"), ix->seg_head.data(), nsegs * 4) &&
               write_file(path_of(dir, name, ".segOffset"), seg_off.data(), nsegs * 4);
-    if (ok && codec == EXCL_CODEC_PARAPFD) {
+    if (ok && codec != EXCL_CODEC_SEGLRC) {
         ok = write_file(path_of(dir, name, ".segMedian"), aux.data(), nsegs * 4);
     } else if (ok) {
         std::vector<SegReg> list_reg(ix->nlists);
@@ -130,7 +132,7 @@ extern "C" int excl_index_load_reference(const char *dir, const char *name, uint
         !read_file(path_of(dir, name, ".segNum"), seg_num) || !read_file(path_of(dir, name, ".segHead"), seg_head) ||
         !read_file(path_of(dir, name, ".segOffset"), seg_off))
         return EXCL_E_INVALID;
-    if (codec == EXCL_CODEC_PARAPFD) {
+    if (codec != EXCL_CODEC_SEGLRC) {
         if (!read_file(path_of(dir, name, ".segMedian"), aux)) return EXCL_E_INVALID;
     } else if (!read_file(path_of(dir, name, ".ind2_distance_base"), aux) ||
                !read_file(path_of(dir, name, ".regression_info"), reg) ||
@@ -182,8 +184,10 @@ extern "C" int excl_index_load_reference(const char *dir, const char *name, uint
             const uint64_t ow = seg_off[g];
             const uint64_t next = s + 1 < nseg ? seg_off[g + 1] : we - wb;
             // the block must lie inside the list's words and decode within itself
-            if (ow >= next || wb + next > we || (s && ix->seg_head[g] <= ix->seg_head[g - 1]) ||
-                pfd_block_words(ix->words.data() + wb + ow, cnt) > next - ow) {
+            const uint32_t *blk = ix->words.data() + wb + ow;
+            const uint64_t bw = codec == EXCL_CODEC_NEWPFD ? newpfd_block_words(blk, cnt, next - ow)
+                                                           : pfd_block_words(blk, cnt);
+            if (ow >= next || wb + next > we || (s && ix->seg_head[g] <= ix->seg_head[g - 1]) || bw > next - ow) {
                 st = EXCL_E_FORMAT;
                 break;
             }
@@ -198,8 +202,9 @@ extern "C" int excl_index_load_reference(const char *dir, const char *name, uint
         // last docID: decode the list's last block
         const size_t gl = (size_t)d.seg_base + nseg - 1;
         const SegRec &rl = ix->seg_rec[gl];
-        pfd_decode_block(ix->words.data() + wb + rl.off, rl.count, vals.data());
-        if (codec == EXCL_CODEC_PARAPFD) {
+        if (codec == EXCL_CODEC_NEWPFD) newpfd_decode_block(ix->words.data() + wb + rl.off, rl.count, vals.data());
+        else pfd_decode_block(ix->words.data() + wb + rl.off, rl.count, vals.data());
+        if (codec != EXCL_CODEC_SEGLRC) {
             uint32_t v = ix->seg_head[gl];
             for (uint32_t k = 1; k < rl.count; ++k) v += vals[k];
             d.last_doc = v;

@@ -43,6 +43,26 @@ extern "C" int excl_parapfd_decode(const uint32_t *in, size_t nwords, uint32_t n
     return EXCL_OK;
 }
 
+extern "C" int excl_newpfd_encode(const uint32_t *in, uint32_t n, float frac, uint32_t *out, size_t cap,
+                                  size_t *words) {
+    if ((!in && n) || !out || !words) return EXCL_E_INVALID;
+    std::vector<uint32_t> tmp((size_t)n * 3 + 8);
+    int err = 0;
+    const uint32_t w = newpfd_encode_block(in, n, frac, tmp.data(), &err);
+    if (err) return err;
+    if (w > cap) return EXCL_E_CAPACITY;
+    std::memcpy(out, tmp.data(), (size_t)w * 4);
+    *words = w;
+    return EXCL_OK;
+}
+
+extern "C" int excl_newpfd_decode(const uint32_t *in, size_t nwords, uint32_t n, uint32_t *out, size_t *consumed) {
+    if (!in || !out || !consumed || nwords == 0) return EXCL_E_INVALID;
+    if (newpfd_block_words(in, n, nwords) > nwords) return EXCL_E_FORMAT;
+    *consumed = newpfd_decode_block(in, n, out);
+    return EXCL_OK;
+}
+
 static float g_frac = 0.0f;
 extern "C" void excl_set_frac(float frac) { g_frac = frac; }
 

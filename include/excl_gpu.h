@@ -40,7 +40,9 @@ typedef enum {
     EXCL_CODEC_LRCSEG = 2,    /* list regression + per-segment base (LRCSeg_Generator*.cu) */
     EXCL_CODEC_SEGLRC = 3,    /* per-segment regression + base (SegLRC_Generator.cu:94-436) */
     EXCL_CODEC_HS_SEGLRC = 4, /* hash buckets, per-bucket regression + base (HS_SegLRC_Generator.cu) */
-    EXCL_CODEC_HS_PARAPFD = 5 /* hash buckets, d-gap ParaPFD blocks inside each bucket */
+    EXCL_CODEC_HS_PARAPFD = 5, /* hash buckets, d-gap ParaPFD blocks inside each bucket */
+    EXCL_CODEC_NEWPFD = 6      /* d-gaps, NewPFD blocks: exceptions as Simple-16 (NewPFD_Compression/main.cpp,
+                                  NewPFor.cpp:52-139); decode as NewPFD_Decompression_kernel.cu:322-488 */
 } excl_codec;
 
 /* Search method for locating a probe in a longer list. */
@@ -58,6 +60,13 @@ typedef enum {
  * blocks. `cap` is the capacity of `out` in words. */
 int excl_parapfd_encode(const uint32_t *in, uint32_t n, float frac, uint32_t *out, size_t cap, size_t *words);
 int excl_parapfd_decode(const uint32_t *in, size_t nwords, uint32_t n, uint32_t *out, size_t *consumed);
+
+/* NewPFD blocks (NewPFor.cpp:52-139): descriptor b << 26 | exception count,
+ * the b-bit low parts, then one Simple-16 stream with the exception positions
+ * (first absolute, then gaps minus one) and their high parts. A high part of
+ * more than 28 bits has no Simple-16 layout: EXCL_E_FORMAT. */
+int excl_newpfd_encode(const uint32_t *in, uint32_t n, float frac, uint32_t *out, size_t cap, size_t *words);
+int excl_newpfd_decode(const uint32_t *in, size_t nwords, uint32_t n, uint32_t *out, size_t *consumed);
 
 /* Compatibility shims with the reference's exact signatures (ParaPFor.h:15-16);
  * they use the process-wide FRAC set by excl_set_frac (default 0.0). Return 0
@@ -125,11 +134,11 @@ int excl_index_export(const excl_index *ix, excl_list_info *lists, uint32_t *wor
                       uint32_t *dir);
 
 /* ---------------------------------------------------------------------------
- * The reference's on-disk files. An index in the ParaPFD or SegLRC format with
+ * The reference's on-disk files. An index in the ParaPFD, NewPFD or SegLRC format with
  * 256-entry segments (SegmentSize of the reference encoders) is written as the
  * file set its intersection binaries read, and such a file set is loaded
  * without re-encoding: `<dir>/<name>` + .ind1 .ind2 .segNum .segHead .segOffset
- * and, for ParaPFD, .segMedian (ParaPFD_Compression/main.cpp:81-232); for
+ * and, for ParaPFD and NewPFD, .segMedian (ParaPFD_Compression/main.cpp:81-232, NewPFD_Compression/main.cpp); for
  * SegLRC, .ind2_distance_base .regression_info .regression_info_list
  * (SegLRC_Compression/main.cpp:80-207, SegLRC_Generator.cu:338-412; the
  * reference keeps these three in a second directory). .ind1 records are
@@ -137,7 +146,7 @@ int excl_index_export(const excl_index *ix, excl_list_info *lists, uint32_t *wor
  * that lists, segments and blocks are consistent and in bounds
  * (EXCL_E_FORMAT otherwise). */
 int excl_index_save_reference(const excl_index *ix, const char *dir, const char *name);
-int excl_index_load_reference(const char *dir, const char *name, uint32_t codec /* PARAPFD or SEGLRC */,
+int excl_index_load_reference(const char *dir, const char *name, uint32_t codec /* PARAPFD, NEWPFD or SEGLRC */,
                               excl_index **out);
 
 /* The reference's .query stream (ParaPFD_Intersection.cu:139-142): per query a

@@ -18,6 +18,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "liboracle.so")
 REF_CODEC = os.path.join(HERE, "_ref", "libparapfor_ref.so")
+REF_NEWPFD = os.path.join(HERE, "_ref", "libnewpfor_ref.so")
 REF_FIT = os.path.join(HERE, "_ref", "libfit_ref.so")
 
 
@@ -48,6 +49,10 @@ def _f(lib, name, res, *args):
 
 _enc_block = _f(_lib, "or_parapfd_encode_block", C.c_uint32, u32p, C.c_uint32, C.c_float, u32p, C.POINTER(C.c_int))
 _dec_block = _f(_lib, "or_parapfd_decode_block", C.c_uint32, u32p, C.c_uint32, u32p)
+_nenc_block = _f(_lib, "or_newpfd_encode_block", C.c_uint32, u32p, C.c_uint32, C.c_float, u32p, C.POINTER(C.c_int))
+_ndec_block = _f(_lib, "or_newpfd_decode_block", C.c_uint32, u32p, C.c_uint32, u32p)
+_enc_npfd = _f(_lib, "or_encode_newpfd_list", C.c_int64, u32p, C.c_uint32, C.c_uint32, C.c_float, u32p, u32p, u32p,
+               u32p)
 _fit_seg = _f(_lib, "or_fit_seg", None, u32p, C.c_uint32, C.POINTER(C.c_float), C.POINTER(C.c_float), u32p, u32p)
 _fit_lrc = _f(_lib, "or_fit_lrc", None, u32p, C.c_uint32, C.POINTER(C.c_float), i32p, C.POINTER(C.c_float))
 _enc_pfd = _f(_lib, "or_encode_parapfd_list", C.c_int64, u32p, C.c_uint32, C.c_uint32, C.c_float, u32p, u32p, u32p,
@@ -87,6 +92,24 @@ def decode_block(words, n: int) -> tuple[np.ndarray, int]:
     w[: len(words)] = words
     out = np.zeros(max(n, 1), dtype=np.uint32)
     used = _dec_block(_p(w), n, _p(out))
+    return out[:n], int(used)
+
+
+def newpfd_encode_block(values, frac: float = 0.0) -> np.ndarray:
+    v = _u32(values)
+    out = np.zeros(3 * len(v) + 8, dtype=np.uint32)
+    err = C.c_int(0)
+    w = _nenc_block(_p(v), len(v), frac, _p(out), C.byref(err))
+    if err.value:
+        raise ValueError("block not representable in NewPFD")
+    return out[:w].copy()
+
+
+def newpfd_decode_block(words, n: int) -> tuple[np.ndarray, int]:
+    w = np.zeros(len(words) + 4, dtype=np.uint32)
+    w[: len(words)] = words
+    out = np.zeros(max(n, 1), dtype=np.uint32)
+    used = _ndec_block(_p(w), n, _p(out))
     return out[:n], int(used)
 
 
@@ -157,7 +180,9 @@ def encode_list(docs, codec: int, block: int = 256, frac: float = 0.0, bucket: i
     reg = np.zeros((ns, 4), dtype=np.uint32)
     base = np.zeros(ns, dtype=np.int32)
     listreg = np.zeros(4, dtype=np.uint32)
-    if codec in (0, 5):
+    if codec == 6:
+        w = _enc_npfd(_p(d), n, block, frac, _p(words), _p(off), _p(head), _p(aux))
+    elif codec in (0, 5):
         if codec == 0:
             w = _enc_pfd(_p(d), n, block, frac, _p(words), _p(off), _p(head), _p(aux))
         else:
@@ -178,7 +203,7 @@ def decode_list(enc: dict, codec: int, n: int) -> np.ndarray:
     words = np.zeros(len(enc["words"]) + 8, dtype=np.uint32)
     words[: len(enc["words"])] = enc["words"]
     out = np.zeros(max(n, 1), dtype=np.uint32)
-    ocodec = {0: 0, 5: 0, 1: 1, 2: 2, 3: 3, 4: 3}[codec]
+    ocodec = {0: 0, 5: 0, 1: 1, 2: 2, 3: 3, 4: 3, 6: 6}[codec]
     reg = np.ascontiguousarray(enc["reg"].reshape(-1), dtype=np.uint32)
     base = np.ascontiguousarray(enc["aux"]).view(np.int32)
     _dec_list(ocodec, _p(words), n, len(enc["starts"]), _p(_u32(enc["starts"])), _p(_u32(enc["off"])),
@@ -359,6 +384,41 @@ def ref_decode(words, n: int) -> tuple[np.ndarray, int]:
     w[: len(words)] = words
     out = np.zeros(max(n, 1) + 2, dtype=np.uint32)
     used = _rc().ref_decode(_p(w), _p(out), n)
+    return out[:n].copy(), int(used)
+
+
+def have_ref_newpfd() -> bool:
+    return os.path.exists(REF_NEWPFD)
+
+
+_ref_newpfd = None
+
+
+def _rn():
+    global _ref_newpfd
+    if _ref_newpfd is None:
+        lib = C.CDLL(REF_NEWPFD)
+        _f(lib, "ref_newpfd_set_frac", None, C.c_float)
+        _f(lib, "ref_newpfd_encode", C.c_uint32, u32p, u32p, C.c_uint32)
+        _f(lib, "ref_newpfd_decode", C.c_uint32, u32p, u32p, C.c_uint32)
+        _ref_newpfd = lib
+    return _ref_newpfd
+
+
+def ref_newpfd_encode(values, frac: float) -> np.ndarray:
+    v = _u32(values)
+    out = np.zeros(3 * len(v) + 16, dtype=np.uint32)
+    lib = _rn()
+    lib.ref_newpfd_set_frac(frac)
+    w = lib.ref_newpfd_encode(_p(v), _p(out), len(v))
+    return out[:w].copy()
+
+
+def ref_newpfd_decode(words, n: int) -> tuple[np.ndarray, int]:
+    w = np.zeros(len(words) + 32, dtype=np.uint32)
+    w[: len(words)] = words
+    out = np.zeros(max(n, 1) + 2, dtype=np.uint32)
+    used = _rn().ref_newpfd_decode(_p(w), _p(out), n)
     return out[:n].copy(), int(used)
 
 

@@ -136,6 +136,119 @@ uint32_t or_parapfd_decode_block(const uint32_t *in, uint32_t n, uint32_t *out) 
 }
 
 /* ---------------------------------------------------------------------------
+ * NewPFD (NewPFor.cpp:52-139) with Simple-16 exception streams (Simple16.h).
+ * ------------------------------------------------------------------------- */
+
+/* The 16 Simple-16 layouts, each as up to three (count, width) runs; the
+ * values of one word are laid out from bit 0 up, the selector in bits 28-31. */
+static const unsigned char OR_S16[16][6] = {
+    {28, 1, 0, 0, 0, 0}, {7, 2, 14, 1, 0, 0}, {7, 1, 7, 2, 7, 1}, {14, 1, 7, 2, 0, 0},
+    {14, 2, 0, 0, 0, 0}, {1, 4, 8, 3, 0, 0},  {1, 3, 4, 4, 3, 3}, {7, 4, 0, 0, 0, 0},
+    {4, 5, 2, 4, 0, 0},  {2, 4, 4, 5, 0, 0},  {3, 6, 2, 5, 0, 0}, {2, 5, 3, 6, 0, 0},
+    {4, 7, 0, 0, 0, 0},  {1, 10, 2, 9, 0, 0}, {2, 14, 0, 0, 0, 0}, {1, 28, 0, 0, 0, 0}};
+
+static uint32_t or_s16_width(uint32_t k, uint32_t j) {
+    for (int r = 0; r < 3; ++r) {
+        if (j < OR_S16[k][2 * r]) return OR_S16[k][2 * r + 1];
+        j -= OR_S16[k][2 * r];
+    }
+    return 0;
+}
+
+static uint32_t or_s16_count(uint32_t k) { return (uint32_t)OR_S16[k][0] + OR_S16[k][2] + OR_S16[k][4]; }
+
+/* Simple16.h s16_encode: the first layout that holds the next values.
+ * Returns words written or -1 if a value exceeds 28 bits. */
+static int64_t or_s16_encode(const uint32_t *v, uint32_t n, uint32_t *out) {
+    uint64_t nw = 0;
+    uint32_t i = 0;
+    while (i < n) {
+        uint32_t k;
+        for (k = 0; k < 16; ++k) {
+            uint32_t c = or_s16_count(k), vol = c < n - i ? c : n - i, j;
+            for (j = 0; j < vol; ++j)
+                if ((uint64_t)v[i + j] >= (1ull << or_s16_width(k, j))) break;
+            if (j == vol) {
+                uint32_t word = k << 28, sh = 0;
+                for (j = 0; j < vol; ++j) { word |= v[i + j] << sh; sh += or_s16_width(k, j); }
+                out[nw++] = word;
+                i += vol;
+                break;
+            }
+        }
+        if (k == 16) return -1;
+    }
+    return (int64_t)nw;
+}
+
+/* S16_DECODE: n values from the stream; returns words read. */
+static uint32_t or_s16_decode(const uint32_t *in, uint32_t n, uint32_t *out) {
+    uint32_t r = 0, i = 0;
+    while (i < n) {
+        uint32_t word = in[r++], k = word >> 28, sh = 0;
+        for (uint32_t j = 0; j < or_s16_count(k) && i < n; ++j) {
+            uint32_t wd = or_s16_width(k, j);
+            out[i++] = (word >> sh) & (wd == 32 ? 0xffffffffu : ((1u << wd) - 1u));
+            sh += wd;
+        }
+    }
+    return r;
+}
+
+/* NewPFor.cpp:52-108 (encodeBlock). */
+uint32_t or_newpfd_encode_block(const uint32_t *in, uint32_t n, float frac, uint32_t *out, int *err) {
+    *err = OR_OK;
+    uint32_t b = or_find_best_b(in, n, frac);
+    if (b >= 32) { *err = OR_E_FORMAT; return 0; }
+    uint32_t *lower = (uint32_t *)malloc((size_t)(n ? n : 1) * 4);
+    uint32_t *all = (uint32_t *)malloc((size_t)(2 * n + 2) * 4);
+    uint32_t *pos = (uint32_t *)malloc((size_t)(n ? n : 1) * 4);
+    uint32_t en = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        lower[i] = in[i] & ((1u << b) - 1u);
+        if (in[i] >= (1u << b)) { pos[en] = i; all[n + en] = in[i] >> b; ++en; }
+    }
+    uint32_t w = 1;
+    or_pack(lower, out + w, b, n);
+    w += (uint32_t)or_roundup32((uint64_t)n * b);
+    if (en > 65535u) { *err = OR_E_FORMAT; free(lower); free(all); free(pos); return 0; }
+    out[0] = (b << 26) + en;
+    if (en) {
+        /* [first position, later positions as gaps minus one, high parts] */
+        uint32_t *seq = (uint32_t *)malloc((size_t)2 * en * 4);
+        for (uint32_t i = 0; i < en; ++i) {
+            seq[i] = i ? pos[i] - pos[i - 1] - 1u : pos[0];
+            seq[en + i] = all[n + i];
+        }
+        int64_t nw = or_s16_encode(seq, 2 * en, out + w);
+        free(seq);
+        if (nw < 0) { *err = OR_E_FORMAT; free(lower); free(all); free(pos); return 0; }
+        w += (uint32_t)nw;
+    }
+    free(lower); free(all); free(pos);
+    return w;
+}
+
+/* NewPFor.cpp:111-132 (decodeBlock). Returns words consumed. */
+uint32_t or_newpfd_decode_block(const uint32_t *in, uint32_t n, uint32_t *out) {
+    uint32_t b = (in[0] >> 26) % 32u, en = in[0] & 65535u;
+    uint32_t w = 1;
+    or_unpack(in + w, out, b, n);
+    w += (uint32_t)or_roundup32((uint64_t)n * b);
+    if (en) {
+        uint32_t *seq = (uint32_t *)malloc((size_t)2 * en * 4);
+        w += or_s16_decode(in + w, 2 * en, seq);
+        uint32_t p = 0;
+        for (uint32_t i = 0; i < en; ++i) {
+            p = i ? p + seq[i] + 1u : seq[0];
+            if (p < n) out[p] += seq[en + i] << b;
+        }
+        free(seq);
+    }
+    return w;
+}
+
+/* ---------------------------------------------------------------------------
  * Regression fits.
  * ------------------------------------------------------------------------- */
 
@@ -251,6 +364,30 @@ int64_t or_encode_parapfd_list(const uint32_t *docs, uint32_t n, uint32_t bs, fl
         off[s] = (uint32_t)nw;
         int err;
         uint32_t w = or_parapfd_encode_block(gaps + st, cnt, frac, words + nw, &err);
+        if (err) { free(gaps); return -1; }
+        nw += w;
+    }
+    free(gaps);
+    return (int64_t)nw;
+}
+
+/* NewPFD_Compression/main.cpp: the same d-gap layout with NewPFD blocks. */
+int64_t or_encode_newpfd_list(const uint32_t *docs, uint32_t n, uint32_t bs, float frac,
+                              uint32_t *words, uint32_t *off, uint32_t *head, uint32_t *median) {
+    if (n == 0) return -1;
+    uint32_t *gaps = (uint32_t *)malloc((size_t)n * 4);
+    gaps[0] = docs[0];
+    for (uint32_t j = 1; j < n; ++j) gaps[j] = docs[j] - docs[j - 1];
+    uint32_t nseg = (n + bs - 1) / bs;
+    uint64_t nw = 0;
+    for (uint32_t s = 0; s < nseg; ++s) {
+        uint32_t st = s * bs;
+        uint32_t cnt = (s + 1 < nseg) ? bs : n - st;
+        head[s] = docs[st];
+        median[s] = docs[st + cnt / 2];
+        off[s] = (uint32_t)nw;
+        int err;
+        uint32_t w = or_newpfd_encode_block(gaps + st, cnt, frac, words + nw, &err);
         if (err) { free(gaps); return -1; }
         nw += w;
     }
@@ -407,8 +544,9 @@ int or_decode_list(int codec, const uint32_t *words, uint32_t n, uint32_t nseg, 
     for (uint32_t s = 0; s < nseg; ++s) {
         uint32_t st = start[s], en = (s + 1 < nseg) ? start[s + 1] : n;
         uint32_t cnt = en - st;
-        or_parapfd_decode_block(words + off[s], cnt, out + st);
-        if (codec == 0) {
+        if (codec == 6) or_newpfd_decode_block(words + off[s], cnt, out + st);
+        else or_parapfd_decode_block(words + off[s], cnt, out + st);
+        if (codec == 0 || codec == 6) {
             /* ParaPFD_Decompression_kernel.cu:244-263: element 0 := segHead, scan */
             out[st] = head[s];
             for (uint32_t i = st + 1; i < en; ++i) out[i] += out[i - 1];
@@ -612,8 +750,9 @@ static void or_decode_seg(const or_image *im, uint32_t l, uint32_t s, uint32_t *
     const uint32_t *r = im->rec + 4 * (size_t)sg;
     const uint32_t st = r[0], cnt = r[3];
     const uint32_t codec = im->lcodec[l];
-    or_parapfd_decode_block(im->words + im->lword[l] + r[1], cnt, out);
-    if (codec == 0 || codec == 5) {
+    if (codec == 6) or_newpfd_decode_block(im->words + im->lword[l] + r[1], cnt, out);
+    else or_parapfd_decode_block(im->words + im->lword[l] + r[1], cnt, out);
+    if (codec == 0 || codec == 5 || codec == 6) {
         out[0] = im->head[sg];
         for (uint32_t i = 1; i < cnt; ++i) out[i] += out[i - 1];
     } else if (codec == 1) {

@@ -43,6 +43,29 @@ def codec_vectors():
                         word_offsets=np.array(offs, np.uint64))
 
 
+def newpfd_vectors():
+    """NewPFD blocks from the reference's own NewPFor.cpp (Simple-16 exceptions)."""
+    rng = np.random.default_rng(0x5E16)
+    ins, ns, fr, outs, offs = [], [], [], [], [0]
+    for t in range(300):
+        n = int(rng.integers(1, 300))
+        bits = int(rng.integers(0, 29))
+        v = (rng.integers(0, 1 << bits, size=n, dtype=np.uint64).astype(np.uint32) if bits
+             else np.zeros(n, np.uint32))
+        k = int(rng.integers(0, max(1, n // 3)))
+        v[rng.integers(0, n, size=k)] = rng.integers(0, 1 << 28, size=k).astype(np.uint32)
+        f = float(FRACS[t % len(FRACS)])
+        w = oracle.ref_newpfd_encode(v, f)
+        ins.append(v)
+        ns.append(n)
+        fr.append(f)
+        outs.append(w)
+        offs.append(offs[-1] + len(w))
+    np.savez_compressed(os.path.join(OUT, "newpfd_blocks.npz"), values=np.concatenate(ins),
+                        n=np.array(ns, np.uint32), frac=np.array(fr, np.float32), words=np.concatenate(outs),
+                        word_offsets=np.array(offs, np.uint64))
+
+
 def fit_vectors():
     rng = np.random.default_rng(0xF17)
     ys, ns, seg, lrc = [], [], [], []
@@ -93,13 +116,13 @@ def reference_file_sets():
     lens = [1, 100, 255, 256, 257, 700, 2000, 5000]
     lists = [np.sort(rng.choice(1 << 22, size=n, replace=False)).astype(np.uint32) for n in lens]
     out = {"docs": np.concatenate(lists), "lens": np.array(lens, np.uint32)}
-    for codec, name, frac in ((0, "parapfd", 0.12), (3, "seglrc", 0.0)):
+    for codec, name, frac in ((0, "parapfd", 0.12), (3, "seglrc", 0.0), (6, "newpfd", 0.12)):
         ind1, ind2, seg_num, heads, offs, aux, reg, listreg = b"", [], [], [], [], [], [], []
         words_total = 0
         for d in lists:
             n = len(d)
             seg_num.append(len(heads))
-            if codec == 0:
+            if codec in (0, 6):
                 gaps = np.empty_like(d)
                 gaps[0] = d[0]
                 gaps[1:] = np.diff(d)
@@ -120,7 +143,8 @@ def reference_file_sets():
             for k, v in enumerate(segvals):
                 heads.append(int(d[256 * k]))
                 offs.append(nw)
-                w = oracle.ref_encode(np.ascontiguousarray(v, np.uint32), frac)
+                enc_fn = oracle.ref_newpfd_encode if codec == 6 else oracle.ref_encode
+                w = enc_fn(np.ascontiguousarray(v, np.uint32), frac)
                 ind2.append(w)
                 nw += len(w)
             aux.extend(med)
@@ -130,7 +154,7 @@ def reference_file_sets():
                  ".segNum": np.array(seg_num, np.uint32).view(np.uint8),
                  ".segHead": np.array(heads, np.uint32).view(np.uint8),
                  ".segOffset": np.array(offs, np.uint32).view(np.uint8)}
-        if codec == 0:
+        if codec in (0, 6):
             files[".segMedian"] = np.array(aux, np.uint32).view(np.uint8)
         else:
             files[".ind2_distance_base"] = np.array(aux, np.uint32).view(np.uint8)
@@ -145,9 +169,11 @@ def reference_file_sets():
 
 
 if __name__ == "__main__":
-    assert oracle.have_ref_codec() and oracle.have_ref_fit(), "build the reference first: make -C oracle ref"
+    assert oracle.have_ref_codec() and oracle.have_ref_fit() and oracle.have_ref_newpfd(), \
+        "build the reference first: make -C oracle ref"
     codec_vectors()
     fit_vectors()
+    newpfd_vectors()
     reference_file_sets()
     if os.path.exists(INVERTED_LIST):
         inverted_list_digest()

@@ -57,7 +57,8 @@ def test_codec_edge_cases():
         ex.parapfd_decode(w[:3], 256)
 
 
-FORMATS = [("parapfd", 0), ("lrc", 1), ("lrcseg", 2), ("seglrc", 3), ("hs_seglrc", 4), ("hs_parapfd", 5)]
+FORMATS = [("parapfd", 0), ("lrc", 1), ("lrcseg", 2), ("seglrc", 3), ("hs_seglrc", 4), ("hs_parapfd", 5),
+           ("newpfd", 6)]
 
 
 def _compare_index(w, cname, codec, block, frac, kb, ub, bucket=256):
@@ -142,3 +143,24 @@ def test_checksum_matches_oracle():
     offs = np.array([0, 3, 3, 4, 9], np.uint32)
     docs = np.array([1, 5, 9, 2, 3, 4, 8, 16, 32], np.uint32)
     assert ex.checksum(offs, docs) == oracle.checksum(offs.astype(np.uint64), docs)
+
+
+def test_newpfd_codec_matches_reference_golden_blocks():
+    """Host NewPFD blocks equal the reference NewPFor.cpp's (golden vectors), and decode back."""
+    g = np.load(os.path.join(ROOT, "tests", "golden", "newpfd_blocks.npz"))
+    vo, wo = 0, g["word_offsets"]
+    for i, n in enumerate(g["n"]):
+        v = g["values"][vo:vo + n]
+        vo += n
+        ref = g["words"][wo[i]:wo[i + 1]]
+        assert np.array_equal(ex.newpfd_encode(v, float(g["frac"][i])), ref), f"block {i}"
+        dec, used = ex.newpfd_decode(ref, int(n))
+        assert used == len(ref) and np.array_equal(dec, v)
+
+
+def test_newpfd_rejects_high_part_beyond_28_bits():
+    # with b = 0 every nonzero value is an exception; a high part needs <= 28 bits
+    with pytest.raises(ex.ExclError):
+        ex.newpfd_encode(np.array([1 << 29] + [0] * 20, np.uint32), 0.1)
+    with pytest.raises(ex.ExclError):
+        ex.newpfd_decode(np.array([(0 << 26) | 3], np.uint32), 4)  # 3 exceptions, no Simple-16 words

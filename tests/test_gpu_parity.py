@@ -9,7 +9,8 @@ from exclucene_b200 import synth
 
 pytestmark = pytest.mark.gpu
 
-FORMATS = ["parapfd", "lrc", "lrcseg", "seglrc", "hs_seglrc", "hs_parapfd"]
+FORMATS = ["parapfd", "lrc", "lrcseg", "seglrc", "hs_seglrc", "hs_parapfd", "newpfd"]
+DGAP = ("parapfd", "newpfd")  # exercised with FRAC 0.1 and 128-entry blocks (exceptions)
 ALGOS = ["bsearch", "hashseg", "auto"]
 
 
@@ -47,7 +48,7 @@ def test_decode_matches_source_lists(gpu_ctx, corpus, codec, block, frac):
 @pytest.mark.parametrize("codec", FORMATS)
 @pytest.mark.parametrize("algo", ALGOS)
 def test_intersection_matches_oracle(gpu_ctx, corpus, expected, codec, algo):
-    ix = _index(corpus, codec, 128 if codec == "parapfd" else 256, 0.1 if codec == "parapfd" else 0.0)
+    ix = _index(corpus, codec, 128 if codec in DGAP else 256, 0.1 if codec in DGAP else 0.0)
     gpu_ctx.upload(ix)
     offs, docs = gpu_ctx.intersect(ix, corpus.terms, corpus.term_offsets, algo=algo)
     eoffs, edocs = expected
@@ -156,7 +157,7 @@ def test_merge_and_probe_paths_agree(corpus, expected, codec, merge):
     """The shared-memory merge path (tiles whose keys span few segments of a
     longer list) and the per-key probe path give the oracle's output."""
     ctx = ex.Context(0, max_queries=65536, max_keys=1 << 24, merge_segs=merge)
-    ix = _index(corpus, codec, 128 if codec == "parapfd" else 256, 0.1 if codec == "parapfd" else 0.0)
+    ix = _index(corpus, codec, 128 if codec in DGAP else 256, 0.1 if codec in DGAP else 0.0)
     ctx.upload(ix)
     eoffs, edocs = expected
     try:
@@ -195,7 +196,7 @@ def test_autotune_keeps_output_exact(corpus, expected):
         ctx.close()
 
 
-@pytest.mark.parametrize("codec", ["parapfd", "seglrc"])
+@pytest.mark.parametrize("codec", ["parapfd", "seglrc", "newpfd"])
 def test_reference_file_set_runs_unchanged(gpu_ctx, tmp_path, codec):
     """A file set written as the reference's compressors write it (blocks from
     its own encoder) loads without re-encoding, decodes to its lists and
@@ -204,6 +205,7 @@ def test_reference_file_set_runs_unchanged(gpu_ctx, tmp_path, codec):
 
     g = dict(np.load(os.path.join(os.path.dirname(__file__), "golden", "reference_files.npz")))
     sets = {"parapfd": (".ind1", ".ind2", ".segNum", ".segHead", ".segOffset", ".segMedian"),
+            "newpfd": (".ind1", ".ind2", ".segNum", ".segHead", ".segOffset", ".segMedian"),
             "seglrc": (".ind1", ".ind2", ".segNum", ".segHead", ".segOffset", ".ind2_distance_base",
                        ".regression_info", ".regression_info_list")}
     for suffix in sets[codec]:

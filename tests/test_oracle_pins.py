@@ -25,6 +25,29 @@ def test_oracle_codec_matches_reference_golden_blocks():
         assert used == len(ref_words) and np.array_equal(dec, v)
 
 
+def test_oracle_newpfd_matches_reference_golden_blocks():
+    g = np.load(os.path.join(GOLD, "newpfd_blocks.npz"))
+    vo, wo = 0, g["word_offsets"]
+    for i, n in enumerate(g["n"]):
+        v = g["values"][vo:vo + n]
+        vo += n
+        ref_words = g["words"][wo[i]:wo[i + 1]]
+        assert np.array_equal(oracle.newpfd_encode_block(v, float(g["frac"][i])), ref_words), f"block {i}"
+        dec, used = oracle.newpfd_decode_block(ref_words, int(n))
+        assert used == len(ref_words) and np.array_equal(dec, v)
+
+
+@pytest.mark.skipif(not have_reference(), reason="reference tree not present")
+def test_oracle_newpfd_vs_compiled_reference_random_blocks():
+    rng = np.random.default_rng(11)
+    for _ in range(300):
+        n = int(rng.integers(1, 300))
+        bits = int(rng.integers(0, 29))
+        v = rng.integers(0, 1 << bits, size=n, dtype=np.uint64).astype(np.uint32) if bits else np.zeros(n, np.uint32)
+        frac = float(rng.choice([0.0, 0.1, 0.12, 0.5]))
+        assert np.array_equal(oracle.newpfd_encode_block(v, frac), oracle.ref_newpfd_encode(v, frac))
+
+
 def test_oracle_fits_match_reference_golden():
     g = np.load(os.path.join(GOLD, "regression_fits.npz"))
     o = 0

@@ -12,9 +12,10 @@ import exclucene_b200 as ex
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "reference_files.npz")
 SETS = {"parapfd": (".ind1", ".ind2", ".segNum", ".segHead", ".segOffset", ".segMedian"),
+        "newpfd": (".ind1", ".ind2", ".segNum", ".segHead", ".segOffset", ".segMedian"),
         "seglrc": (".ind1", ".ind2", ".segNum", ".segHead", ".segOffset", ".ind2_distance_base",
                    ".regression_info", ".regression_info_list")}
-FRAC = {"parapfd": 0.12, "seglrc": 0.0}
+FRAC = {"parapfd": 0.12, "seglrc": 0.0, "newpfd": 0.12}
 
 
 @pytest.fixture(scope="module")
@@ -32,7 +33,7 @@ def _write_golden(g, codec, d):
         g[codec + suffix].tofile(os.path.join(d, "g" + suffix))
 
 
-@pytest.mark.parametrize("codec", ["parapfd", "seglrc"])
+@pytest.mark.parametrize("codec", ["parapfd", "seglrc", "newpfd"])
 def test_writer_matches_reference_bytes(golden, tmp_path, codec):
     docs, loff = _corpus(golden)
     ix = ex.Index(docs, loff, codec=codec, block=256, frac=FRAC[codec])
@@ -42,7 +43,7 @@ def test_writer_matches_reference_bytes(golden, tmp_path, codec):
         assert np.array_equal(got, golden[codec + suffix]), suffix
 
 
-@pytest.mark.parametrize("codec", ["parapfd", "seglrc"])
+@pytest.mark.parametrize("codec", ["parapfd", "seglrc", "newpfd"])
 def test_loader_rebuilds_the_same_index(golden, tmp_path, codec):
     docs, loff = _corpus(golden)
     _write_golden(golden, codec, str(tmp_path))
