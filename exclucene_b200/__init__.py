@@ -8,9 +8,9 @@ is its ctypes binding. Importing it without the built library raises.
 from .api import (ALGO_AUTO, ALGO_BSEARCH, ALGO_HASHSEG, ALGO_LEARNED, CODEC_HS_PARAPFD, CODEC_HS_SEGLRC, CODEC_LRC,
                   CODEC_LRCSEG, CODEC_NEWPFD, CODEC_PARAPFD, CODEC_SEGLRC, Batch, Context, ExclError, Index, checksum,
                   Server, encode_array_compat, library_path, newpfd_decode, newpfd_encode, parapfd_decode,
-                  parapfd_encode, query_encode,
-                  query_parse)
+                  parapfd_encode, pinned_empty, query_encode, query_parse)
 
 __all__ = ["Context", "Index", "Batch", "Server", "query_parse", "query_encode", "ExclError", "checksum", "parapfd_encode", "parapfd_decode",
            "encode_array_compat", "library_path", "CODEC_PARAPFD", "CODEC_LRC", "CODEC_LRCSEG", "CODEC_SEGLRC",
-           "CODEC_HS_SEGLRC", "CODEC_HS_PARAPFD", "CODEC_NEWPFD", "newpfd_encode", "newpfd_decode", "ALGO_AUTO", "ALGO_BSEARCH", "ALGO_HASHSEG", "ALGO_LEARNED"]
+           "CODEC_HS_SEGLRC", "CODEC_HS_PARAPFD", "CODEC_NEWPFD", "newpfd_encode", "newpfd_decode", "ALGO_AUTO", "ALGO_BSEARCH", "ALGO_HASHSEG", "ALGO_LEARNED",
+           "pinned_empty"]

@@ -10,6 +10,7 @@ missing library raises at import time.
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 import os
 from dataclasses import dataclass
 
@@ -126,6 +127,10 @@ _submit = _sig("excl_submit", C.c_int, C.c_void_p, C.c_void_p, u32p, u32p, C.c_u
                C.POINTER(C.c_void_p))
 _wait = _sig("excl_wait", C.c_int, C.c_void_p, u32p, u32p, C.c_size_t, C.c_int, u64p)
 _bfree = _sig("excl_batch_free", C.c_int, C.c_void_p)
+_submit_into = _sig("excl_submit_into", C.c_int, C.c_void_p, C.c_void_p, u32p, u32p, C.c_uint32, C.c_uint32, u32p,
+                    u32p, C.c_uint64, C.POINTER(C.c_void_p))
+_halloc = _sig("excl_host_alloc", C.c_int, C.c_size_t, C.POINTER(C.c_void_p))
+_hfree = _sig("excl_host_free", C.c_int, C.c_void_p)
 _isect_dev = _sig("excl_intersect_device", C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
                   C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint64)
 _check = _sig("excl_ctx_check", C.c_int, C.c_void_p)
@@ -153,7 +158,8 @@ EXPORTED = ["excl_learn_models", "excl_model_export", "excl_model_grad", "excl_m
             "excl_index_build", "excl_index_free", "excl_index_sizes_get", "excl_index_export", "excl_ctx_create",
             "excl_ctx_destroy", "excl_last_error", "excl_ctx_stream", "excl_index_upload",
             "excl_decode_lists_device", "excl_decode_lists", "excl_submit", "excl_wait", "excl_batch_free",
-            "excl_intersect_device", "excl_ctx_check", "excl_last_stats", "excl_checksum"]
+            "excl_intersect_device", "excl_ctx_check", "excl_last_stats", "excl_checksum", "excl_submit_into",
+            "excl_host_alloc", "excl_host_free"]
 
 
 def _p32(a: np.ndarray):
@@ -162,6 +168,17 @@ def _p32(a: np.ndarray):
 
 def _u32(a) -> np.ndarray:
     return np.ascontiguousarray(a, dtype=np.uint32)
+
+
+def pinned_empty(n: int, dtype=np.uint32) -> np.ndarray:
+    """A numpy array in page-locked, device-mapped host memory (excl_host_alloc),
+    freed with the array; the buffers excl_submit_into reads and writes."""
+    nbytes = max(int(n), 1) * np.dtype(dtype).itemsize
+    p = C.c_void_p()
+    _check_status(_halloc(nbytes, C.byref(p)), what="excl_host_alloc")
+    buf = (C.c_uint8 * nbytes).from_address(p.value)
+    weakref.finalize(buf, _hfree, p.value)
+    return np.frombuffer(buf, dtype=dtype)[: int(n)]
 
 
 def _check_status(st: int, ctx=None, what: str = "") -> None:
@@ -381,6 +398,24 @@ class Context:
         _check_status(_submit(self._h, ix._h, _p32(t), _p32(o), nq, a, C.byref(b)), self, "excl_submit")
         return Batch(self, b, nq)
 
+    def submit_into(self, ix: Index, terms: np.ndarray, term_offsets: np.ndarray, offsets: np.ndarray,
+                    docids: np.ndarray, algo="auto") -> "Batch":
+        """Zero-copy batch (excl_submit_into): offsets[nq+1] and docids are pinned_empty
+        arrays the last kernel writes into; terms and term_offsets are read from host
+        memory (pinned_empty ones asynchronously). Keep all four alive and unchanged
+        until wait() returns the number of docIDs written."""
+        for a in (terms, term_offsets, offsets, docids):
+            if a.dtype != np.uint32 or not a.flags.c_contiguous:
+                raise ExclError(E_INVALID, "excl_submit_into: arrays must be contiguous uint32")
+        nq = len(term_offsets) - 1
+        if len(offsets) < nq + 1:
+            raise ExclError(E_INVALID, "excl_submit_into: offsets holds fewer than nq+1 entries")
+        a = ALGO_NAMES[algo] if isinstance(algo, str) else int(algo)
+        b = C.c_void_p()
+        _check_status(_submit_into(self._h, ix._h, _p32(terms), _p32(term_offsets), nq, a, _p32(offsets),
+                                   _p32(docids), len(docids), C.byref(b)), self, "excl_submit_into")
+        return Batch(self, b, nq, into=(terms, term_offsets, offsets, docids))
+
     def intersect(self, ix: Index, terms, term_offsets, algo="auto") -> tuple[np.ndarray, np.ndarray]:
         """Runs one batch and returns (offsets[nq+1], docids) — each query's docIDs sorted."""
         b = self.submit(ix, terms, term_offsets, algo)
@@ -459,10 +494,17 @@ class Context:
 
 
 class Batch:
-    def __init__(self, ctx: Context, h: C.c_void_p, nq: int):
+    def __init__(self, ctx: Context, h: C.c_void_p, nq: int, into=None):
         self.ctx, self._h, self.nq = ctx, h, nq
+        self._into = into  # the arrays of an excl_submit_into batch, kept alive until it is freed
 
-    def wait(self, timeout_ms: int = -1) -> tuple[np.ndarray, np.ndarray]:
+    def wait(self, timeout_ms: int = -1):
+        """(offsets, docids) of an excl_submit batch; the number of docIDs written
+        for an excl_submit_into one."""
+        if self._into is not None:
+            tot = C.c_uint64(0)
+            _check_status(_wait(self._h, None, None, 0, timeout_ms, C.byref(tot)), self.ctx, "excl_wait")
+            return int(tot.value)
         offs = np.zeros(self.nq + 1, dtype=np.uint32)
         tot = C.c_uint64(0)
         _check_status(_wait(self._h, _p32(offs), None, 0, timeout_ms, C.byref(tot)), self.ctx, "excl_wait")

@@ -32,7 +32,7 @@ constexpr uint32_t kMergeMinKeys = 32;   // fewer keys than this: always probe
 
 // pipeline.cu
 constexpr uint32_t kPackThreads = 256;
-constexpr uint32_t kPackMaxCtas = 256;
+constexpr uint32_t kPackMaxCtas = 1024;
 constexpr uint32_t kPackMaxQueries = kPackThreads * kPackMaxCtas;
 constexpr uint32_t kSSThreads = 256;
 constexpr uint32_t kSSChunk = 512;

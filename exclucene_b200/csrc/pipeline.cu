@@ -34,6 +34,11 @@ __device__ __forceinline__ uint32_t ld_acquire(const uint32_t *p) {
     asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
+__device__ __forceinline__ uint32_t ld_relaxed(const uint32_t *p) {
+    uint32_t v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
 __device__ __forceinline__ void st_release64(uint64_t *p, uint64_t v) {
     asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
@@ -107,7 +112,6 @@ __global__ void __launch_bounds__(kPackThreads) k_pack_scan(const ListDesc *__re
                                                             const uint32_t *__restrict__ toff, uint32_t nq,
                                                             BatchView b, PackSync *__restrict__ sync) {
     __shared__ uint32_t sa[33], sb[33], s_pre[2], s_et[kPackThreads], s_id, s_tag;
-    static_assert(kPackMaxCtas <= 32 * 8, "warp 0 reads up to 8 predecessors per lane");
     if (threadIdx.x == 0) {
         s_id = atomicAdd(&sync->ticket, 1u);
         s_tag = next_tag(*(volatile uint32_t *)&sync->epoch);
@@ -203,21 +207,41 @@ __global__ void __launch_bounds__(kPackThreads) k_pack_scan(const ListDesc *__re
         st_release(&sync->flag[bid], tag);
     }
     if (threadIdx.x < 32) {
-        // warp 0: the predecessors' totals, read in parallel; every
-        // predecessor took its ticket earlier, so it is running or done
+        // warp 0: the predecessors' totals. Every predecessor took its ticket
+        // earlier, so it is running or done. Each lane has the flags of four
+        // predecessors in flight at once; one fence then orders the totals'
+        // loads after the flags that published them.
         const uint32_t lane = threadIdx.x;
         uint32_t pt = 0, pk = 0;
-        for (uint32_t p = lane; p < bid; p += 32) {
-            uint32_t spins = 0;
-            while (ld_acquire(&sync->flag[p]) != tag) {
-                if (++spins > kSpin) {
-                    atomicOr(b.err, kErrScanSpin);
-                    break;
-                }
-                __nanosleep(32);
+        for (uint32_t p0 = 0; p0 < bid; p0 += 128) {
+            uint32_t f[4];
+#pragma unroll
+            for (uint32_t j = 0; j < 4; ++j) {
+                const uint32_t p = p0 + lane + 32u * j;
+                f[j] = p < bid ? ld_relaxed(&sync->flag[p]) : tag;
             }
-            pt += sync->agg_t[p];
-            pk += sync->agg_k[p];
+#pragma unroll
+            for (uint32_t j = 0; j < 4; ++j) {
+                const uint32_t p = p0 + lane + 32u * j;
+                uint32_t spins = 0;
+                while (f[j] != tag) {
+                    if (++spins > kSpin) {
+                        atomicOr(b.err, kErrScanSpin);
+                        break;
+                    }
+                    __nanosleep(32);
+                    f[j] = ld_relaxed(&sync->flag[p]);
+                }
+            }
+            __threadfence();
+#pragma unroll
+            for (uint32_t j = 0; j < 4; ++j) {
+                const uint32_t p = p0 + lane + 32u * j;
+                if (p < bid) {
+                    pt += ld_relaxed(&sync->agg_t[p]);
+                    pk += ld_relaxed(&sync->agg_k[p]);
+                }
+            }
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {

@@ -239,7 +239,9 @@ int ctx_alloc_batch(excl_ctx *ctx) {
     st |= cuda_status(ctx, cudaMallocHost((void **)&ctx->h_terms, (size_t)c.max_queries * kMaxTerms * 4), "pinned");
     st |= cuda_status(ctx, cudaMallocHost((void **)&ctx->h_toff, ((size_t)c.max_queries + 1) * 4), "pinned");
     st |= cuda_status(ctx, cudaMallocHost((void **)&ctx->h_offsets, ((size_t)c.max_queries + 1) * 4), "pinned");
+    st |= cuda_status(ctx, cudaMallocHost((void **)&ctx->h_flags, kFlagSlots * 4), "pinned");
     if (st) return EXCL_E_NOMEM;
+    for (uint32_t i = kFlagSlots; i-- > 0;) ctx->free_flag_slots.push_back(i);
     cudaMemsetAsync(ctx->d_misc, 0, 16 * 4, ctx->stream);
     cudaMemsetAsync(ctx->d_stats, 0, 4 * 8, ctx->stream);
     cudaMemsetAsync(ctx->d_sync, 0, sizeof(PackSync), ctx->stream);
@@ -357,8 +359,13 @@ int read_device_flags(excl_ctx *ctx) {
     uint32_t f = 0;
     cudaError_t e = cudaMemcpy(&f, ctx->d_misc + kMiscErr, 4, cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return cuda_status(ctx, e, "read error flag");
+    if (f) cudaMemset(ctx->d_misc + kMiscErr, 0, 4);
+    return flags_status(ctx, f);
+}
+
+// Maps a batch's device error word to a status (and the context's message).
+int flags_status(excl_ctx *ctx, uint32_t f) {
     if (f) {
-        cudaMemset(ctx->d_misc + kMiscErr, 0, 4);
         ctx_error(ctx, "device error flags 0x%x (%s%s%s%s%s)", f, (f & kErrTerms) ? "too many terms " : "",
                   (f & kErrScanSpin) ? "scan wait expired " : "", (f & kErrTermId) ? "term id out of range " : "",
                   (f & kErrCapacity) ? "result capacity " : "", (f & kErrModel) ? "model " : "");
@@ -379,7 +386,8 @@ extern "C" int excl_ctx_create(int device, const excl_ctx_config *cfg, excl_ctx 
     ctx->device = device;
     excl_ctx_config c{};
     if (cfg) c = *cfg;
-    if (c.max_queries == 0 || c.max_queries > kPackMaxQueries) c.max_queries = kPackMaxQueries;
+    if (c.max_queries == 0) c.max_queries = 65536;
+    if (c.max_queries > kPackMaxQueries) c.max_queries = kPackMaxQueries;
     if (c.max_terms == 0 || c.max_terms > kMaxTerms) c.max_terms = kMaxTerms;
     if (c.max_keys == 0) c.max_keys = 1ull << 26;
     ctx->cfg = c;
@@ -416,6 +424,7 @@ extern "C" int excl_ctx_destroy(excl_ctx *ctx) {
     cudaFreeHost(ctx->h_terms);
     cudaFreeHost(ctx->h_toff);
     cudaFreeHost(ctx->h_offsets);
+    cudaFreeHost(ctx->h_flags);
     for (auto &e : ctx->ev)
         if (e) cudaEventDestroy(e);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -581,6 +590,9 @@ struct excl_batch {
     uint32_t nq;
     cudaEvent_t done;
     bool waited;
+    // excl_submit_into: the caller's offsets array and this batch's error-word slot (-1 for excl_submit)
+    const uint32_t *into_offsets = nullptr;
+    int32_t slot = -1;
 };
 
 // Copies a host batch into the context's query buffers (after the previous
@@ -722,22 +734,115 @@ extern "C" int excl_submit(excl_ctx *ctx, excl_index *ix, const uint32_t *terms,
     return EXCL_OK;
 }
 
+// excl_submit_into: the inputs are copied from the caller's host arrays on the
+// context's stream (asynchronously when they are page-locked) and the scatter
+// kernel writes offsets and docIDs through the device mapping of the caller's
+// page-locked output arrays, so the results cross PCIe while the last kernel
+// runs and excl_wait has nothing left to copy. The batch's error word is
+// copied to its own pinned slot and the device word cleared behind it, so
+// batches in flight together each see their own flags.
+extern "C" int excl_submit_into(excl_ctx *ctx, excl_index *ix, const uint32_t *terms, const uint32_t *term_offsets,
+                                uint32_t nq, uint32_t algo, uint32_t *offsets, uint32_t *docids, uint64_t cap,
+                                excl_batch **ticket) {
+    if (!ctx || !ix || !term_offsets || !offsets || !ticket || (!docids && cap) || (!terms && term_offsets[nq]))
+        return EXCL_E_INVALID;
+    *ticket = nullptr;
+    if (nq > ctx->cfg.max_queries) {
+        ctx_error(ctx, "batch of %u queries exceeds max_queries %u", nq, ctx->cfg.max_queries);
+        return EXCL_E_CAPACITY;
+    }
+    // per-query term counts and term ids are checked on the device (error flags)
+    const uint32_t nterms = term_offsets[nq];
+    if (term_offsets[0] > nterms) return EXCL_E_INVALID;
+    if (nterms > (uint64_t)ctx->cfg.max_queries * kMaxTerms) {
+        ctx_error(ctx, "batch of %u terms exceeds the context's %llu", nterms,
+                  (unsigned long long)ctx->cfg.max_queries * kMaxTerms);
+        return EXCL_E_CAPACITY;
+    }
+    cudaSetDevice(ctx->device);
+    uint32_t *m_offsets = nullptr, *m_docids = nullptr;
+    for (int i = 0; i < 2; ++i) {
+        void *h = i ? (void *)docids : (void *)offsets;
+        if (!h) continue;
+        cudaPointerAttributes a{};
+        if (cudaPointerGetAttributes(&a, h) != cudaSuccess || a.type != cudaMemoryTypeHost || !a.devicePointer) {
+            cudaGetLastError();
+            ctx_error(ctx, "%s array is not page-locked, device-mapped host memory", i ? "docids" : "offsets");
+            return EXCL_E_INVALID;
+        }
+        (i ? m_docids : m_offsets) = static_cast<uint32_t *>(a.devicePointer);
+    }
+    if (ctx->free_flag_slots.empty()) {
+        ctx_error(ctx, "more than %u excl_submit_into batches in flight", kFlagSlots);
+        return EXCL_E_CAPACITY;
+    }
+    cudaStream_t st = ctx->stream;
+    int s = EXCL_OK;
+    if (nterms)
+        s = cuda_status(ctx, cudaMemcpyAsync(ctx->d_terms, terms, (size_t)nterms * 4, cudaMemcpyHostToDevice, st),
+                        "h2d terms");
+    if (!s)
+        s = cuda_status(ctx, cudaMemcpyAsync(ctx->d_toff, term_offsets, ((size_t)nq + 1) * 4, cudaMemcpyHostToDevice,
+                                             st),
+                        "h2d term offsets");
+    if (!s) s = run_pipeline(ctx, ix, ctx->d_terms, ctx->d_toff, nq, algo, m_offsets, m_docids, cap);
+    if (s) return s;
+    excl_batch *b = new (std::nothrow) excl_batch{ctx, nq, nullptr, false};
+    if (!b) return EXCL_E_NOMEM;
+    b->into_offsets = offsets;
+    b->slot = (int32_t)ctx->free_flag_slots.back();
+    uint32_t *hf = ctx->h_flags + b->slot;
+    *hf = 0;
+    s = cuda_status(ctx, cudaMemcpyAsync(hf, ctx->d_misc + kMiscErr, 4, cudaMemcpyDeviceToHost, st), "d2h flags");
+    if (!s) s = cuda_status(ctx, cudaMemsetAsync(ctx->d_misc + kMiscErr, 0, 4, st), "clear flags");
+    if (!s) s = cuda_status(ctx, cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming), "event");
+    if (!s) s = cuda_status(ctx, cudaEventRecord(b->done, st), "record");
+    if (s) {
+        // the slot is not handed out: the copies above may still land in it
+        if (b->done) cudaEventDestroy(b->done);
+        cudaStreamSynchronize(st);
+        delete b;
+        return s;
+    }
+    ctx->free_flag_slots.pop_back();
+    *ticket = b;
+    return EXCL_OK;
+}
+
+// Polls the batch's event: spins for the first 2 ms (a batch usually ends
+// within tens of microseconds of the call), then sleeps between polls.
+static int wait_event(excl_ctx *ctx, cudaEvent_t ev, int timeout_ms) {
+    const auto t0 = std::chrono::steady_clock::now();
+    for (uint32_t polls = 0;; ++polls) {
+        const cudaError_t q = cudaEventQuery(ev);
+        if (q == cudaSuccess) return EXCL_OK;
+        if (q != cudaErrorNotReady) return cuda_status(ctx, q, "batch");
+        if ((polls & 63) == 0 || timeout_ms >= 0) {
+            const auto dt = std::chrono::steady_clock::now() - t0;
+            if (timeout_ms >= 0 && dt > std::chrono::milliseconds(timeout_ms)) return EXCL_E_TIMEOUT;
+            if (dt > std::chrono::milliseconds(2)) std::this_thread::sleep_for(std::chrono::microseconds(20));
+        }
+    }
+}
+
 extern "C" int excl_wait(excl_batch *b, uint32_t *offsets, uint32_t *docids, size_t cap, int timeout_ms,
                          uint64_t *total) {
     if (!b) return EXCL_E_INVALID;
     excl_ctx *ctx = b->ctx;
     cudaSetDevice(ctx->device);
-    const auto t0 = std::chrono::steady_clock::now();
-    for (;;) {
-        const cudaError_t q = cudaEventQuery(b->done);
-        if (q == cudaSuccess) break;
-        if (q != cudaErrorNotReady) return cuda_status(ctx, q, "batch");
-        if (timeout_ms >= 0 &&
-            std::chrono::steady_clock::now() - t0 > std::chrono::milliseconds(timeout_ms))
-            return EXCL_E_TIMEOUT;
-        std::this_thread::sleep_for(std::chrono::microseconds(20));
+    if (b->slot >= 0) {
+        // excl_submit_into batch: the results are already in the caller's arrays
+        if (offsets || docids) return EXCL_E_INVALID;
+        int s = b->waited ? EXCL_OK : wait_event(ctx, b->done, timeout_ms);
+        if (s) return s;
+        b->waited = true;
+        s = flags_status(ctx, ctx->h_flags[b->slot]);
+        if (total) *total = b->into_offsets[b->nq];
+        return s;
     }
-    int s = read_device_flags(ctx);
+    int s = wait_event(ctx, b->done, timeout_ms);
+    if (s) return s;
+    s = read_device_flags(ctx);
     if (s) return s;
     const uint32_t tot = ctx->h_offsets[b->nq];
     if (total) *total = tot;
@@ -755,8 +860,30 @@ extern "C" int excl_wait(excl_batch *b, uint32_t *offsets, uint32_t *docids, siz
     return s;
 }
 
+extern "C" int excl_host_alloc(size_t bytes, void **out) {
+    if (!out) return EXCL_E_INVALID;
+    *out = nullptr;
+    if (!bytes) return EXCL_OK;
+    if (cudaHostAlloc(out, bytes, cudaHostAllocMapped | cudaHostAllocPortable) != cudaSuccess) {
+        cudaGetLastError();
+        *out = nullptr;
+        return EXCL_E_NOMEM;
+    }
+    return EXCL_OK;
+}
+
+extern "C" int excl_host_free(void *p) {
+    if (!p) return EXCL_OK;
+    return cudaFreeHost(p) == cudaSuccess ? EXCL_OK : EXCL_E_INVALID;
+}
+
 extern "C" int excl_batch_free(excl_batch *b) {
     if (!b) return EXCL_E_INVALID;
+    if (b->slot >= 0) {
+        // a slot returns to the pool only once its batch's copies have landed
+        if (!b->waited) cudaEventSynchronize(b->done);
+        b->ctx->free_flag_slots.push_back((uint32_t)b->slot);
+    }
     if (b->done) cudaEventDestroy(b->done);
     delete b;
     return EXCL_OK;

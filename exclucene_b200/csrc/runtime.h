@@ -4,6 +4,7 @@
 
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "excl_device.cuh"
 #include "kernels.h"
@@ -30,6 +31,8 @@ struct DeviceIndex {
 
 // slots of ctx->d_misc
 enum { kMiscErr = 0, kMiscTileCounter = 1, kMiscDecodeTicket = 2 /* and 3: decode work counter, CTAs done */ };
+// excl_submit_into batches that may be in flight on one context at once
+constexpr uint32_t kFlagSlots = 256;
 
 }  // namespace excl
 
@@ -62,12 +65,16 @@ struct excl_ctx {
     uint32_t *d_offsets = nullptr, *d_docids = nullptr;
     uint64_t docids_cap = 0;
     uint32_t *h_terms = nullptr, *h_toff = nullptr, *h_offsets = nullptr;
+    // error word of each excl_submit_into batch in flight (pinned; a slot per batch)
+    uint32_t *h_flags = nullptr;
+    std::vector<uint32_t> free_flag_slots;
 };
 
 namespace excl {
 void ctx_error(excl_ctx *ctx, const char *fmt, ...);
 int cuda_status(excl_ctx *ctx, cudaError_t e, const char *what);
 int read_device_flags(excl_ctx *ctx);
+int flags_status(excl_ctx *ctx, uint32_t f);
 int run_pipeline(excl_ctx *ctx, excl_index *ix, const uint32_t *d_terms, const uint32_t *d_toff, uint32_t nq,
                  uint32_t algo, uint32_t *d_offsets, uint32_t *d_docids, uint64_t cap);
 

@@ -211,6 +211,24 @@ int excl_submit(excl_ctx *ctx, excl_index *ix, const uint32_t *terms, const uint
 int excl_wait(excl_batch *ticket, uint32_t *offsets, uint32_t *docids, size_t cap, int timeout_ms, uint64_t *total);
 int excl_batch_free(excl_batch *ticket);
 
+/* Zero-copy variant of excl_submit, same results. The inputs are read from
+ * host memory (asynchronously when page-locked) and the last kernel writes
+ * offsets[nq+1] and up to cap docIDs straight into the caller's arrays, which
+ * must be page-locked, device-mapped host memory (excl_host_alloc, or
+ * cudaHostAlloc / cudaHostRegister with the mapped flag). Query q's terms are
+ * terms[term_offsets[q] .. term_offsets[q+1]) as in excl_submit. All four
+ * arrays stay untouched until excl_wait(ticket, NULL, NULL, 0, timeout, &total)
+ * returns; more than cap results give EXCL_E_CAPACITY there (the first cap are
+ * written). Up to 256 such batches may be in flight on one context; they run
+ * in submission order. excl_batch_free of an unfinished batch waits for it.
+ * Replaces the same pipeline as excl_submit, with the reference's separate
+ * dtohTransfer step (ParaPFD_Intersection.cu:306) folded into the kernel. */
+int excl_submit_into(excl_ctx *ctx, excl_index *ix, const uint32_t *terms, const uint32_t *term_offsets, uint32_t nq,
+                     uint32_t algo, uint32_t *offsets, uint32_t *docids, uint64_t cap, excl_batch **ticket);
+/* Page-locked, device-mapped host memory for excl_submit_into (cudaHostAlloc). */
+int excl_host_alloc(size_t bytes, void **out);
+int excl_host_free(void *p);
+
 /* All-device variant: queries and outputs already in device memory; no host
  * synchronisation. d_offsets has nq+1 entries; d_docids capacity `cap`.
  * Writes the total to d_offsets[nq]; a total above cap raises EXCL_E_CAPACITY
