@@ -6,10 +6,13 @@
 // loaded 32-wide, a ballot finds how many fit a 24 KB stage), and one
 // cp.async.bulk copies the run into shared memory, completing on an mbarrier,
 // while all warps decode the previous run from the other stage. Decoding works
-// from shared memory only: bit-window extraction of each lane's run of values,
-// exception patching, d-gap warp scan (ParaPFD_Decompression_kernel.cu:205-263)
+// from shared memory only: bit-window extraction of each lane's values,
+// exception patching, d-gap scan (ParaPFD_Decompression_kernel.cu:205-263)
 // or regression reconstruction (SegLRC_Decompression_kernel.cu:249-252), then
-// coalesced 128-byte stores. Hash buckets of more than 256 postings are not
+// stores. A segment of c values takes G lanes (the smallest power of two with
+// c <= 8G), so one warp decodes 32/G short segments at once: a segment's
+// fixed cost (header, scan, synchronisation) is shared instead of paid by a
+// whole warp for a handful of postings. Hash buckets of more than 256 postings are not
 // staged; their 256-slices are decoded from global memory.
 //
 // No multicast is used: each CTA copies only into its own shared memory.
@@ -20,10 +23,23 @@
 
 namespace excl {
 
-constexpr int kDecWarps = 8;
-constexpr uint32_t kStages = 2;          // ring of staged runs: one copy in flight while one is decoded
-constexpr uint32_t kStageCap = 4096;     // words per stage (16 KB; a run of 32 segments needs ~3-13 KB)
-constexpr int kDecCtasPerSm = 4;
+#ifndef EXCL_DEC_WARPS
+#define EXCL_DEC_WARPS 4
+#endif
+#ifndef EXCL_DEC_STAGES
+#define EXCL_DEC_STAGES 2
+#endif
+#ifndef EXCL_DEC_STAGE_WORDS
+#define EXCL_DEC_STAGE_WORDS 2048
+#endif
+#ifndef EXCL_DEC_CTAS_PER_SM
+#define EXCL_DEC_CTAS_PER_SM 8
+#endif
+constexpr int kDecWarps = EXCL_DEC_WARPS;
+constexpr uint32_t kStages = EXCL_DEC_STAGES;         // ring of staged runs: copies in flight while one is decoded
+constexpr uint32_t kStageCap = EXCL_DEC_STAGE_WORDS;  // words per stage (a run of 32 segments needs ~3-13 KB; longer runs are cut)
+constexpr int kDecCtasPerSm = EXCL_DEC_CTAS_PER_SM;
+static_assert(kStageCap >= 1024, "a stage holds at least one block of 256 values at 32 bits plus exceptions");
 constexpr uint32_t kDecChunk = 64;  // segments per work ticket
 constexpr uint32_t kRunSegs = 32;
 constexpr uint32_t kWaitLimit = 1u << 22;  // try_wait polls before giving up (a stage normally lands in microseconds)
@@ -40,12 +56,19 @@ struct alignas(16) RunMeta {
 struct DecodeSmem {
     uint32_t stage[kStages][kStageCap + 8];
     RunMeta meta[kStages][kRunSegs];
-    uint32_t vals[kDecWarps][kTileKeys];
+    uint32_t vals[kDecWarps][kTileKeys + kTileKeys / 32];
     unsigned long long mbar[kStages];
     uint32_t run_n[kStages];       // segments in the run
     uint32_t run_big[kStages];     // 1: a single large bucket, not staged
     uint32_t run_first[kStages];   // global index of the run's first segment
     uint32_t have[kStages];        // 1: stage holds a planned run
+    // units of the run: unit u decodes useg[u][0 .. ucnt[u]) (indexes into meta),
+    // all of width class ucls[u] (d-gap or residual, log2 of the lanes per segment)
+    uint8_t useg[kStages][kRunSegs][kRunSegs];
+    uint8_t ucls[kStages][kRunSegs];
+    uint8_t ucnt[kStages][kRunSegs];
+    uint32_t nunits[kStages];
+    uint32_t unext[kStages];  // next unit to claim
     uint32_t next_seg;       // first segment not yet planned in the current chunk
     uint32_t chunk_end;
 };
@@ -88,22 +111,24 @@ __device__ void plan_run(const DevIndexView &ix, DecodeSmem &sm, uint32_t b, uin
     uint64_t gword = 0, bw = 0, ob = 0;
     float a = 1.0f, bb = 0.0f;
     if (valid) {
-        // independent loads; only the output position waits on the list id
-        l = ix.seg_list[s];
-        const SegRec rec = ix.seg_rec[s];
+        // independent loads, one round trip: the segment's 64-byte probe
+        // record (which carries its list's codec, regression words and output
+        // position), its block's word range and its list id
+        const uint4 *pr = reinterpret_cast<const uint4 *>(ix.seg_probe + s);
+        const uint4 p0 = __ldg(pr), p1 = __ldg(pr + 1), p2 = __ldg(pr + 2), p3 = __ldg(pr + 3);
         gword = ix.seg_gword[s];
         bw = ix.seg_gword[s + 1] - gword;
-        head = ldg(ix.seg_head + s);
-        const SegReg rg = ix.seg_reg[s];
-        count = rec.count;
-        start = rec.start;
-        aux = rec.aux;
-        a = rg.a;
-        bb = rg.b;
-        ob = ix.post_base[l] - out_base0 + rec.start;
-        codec = ix.lists[l].codec;
-        r0 = ix.lists[l].reg[0];
-        r1 = ix.lists[l].reg[1];
+        l = ix.seg_list[s];
+        head = p0.x;
+        aux = p0.z;
+        count = p0.w;
+        a = __uint_as_float(p1.y);
+        bb = __uint_as_float(p1.z);
+        start = p2.x;
+        codec = p2.y;
+        ob = ((uint64_t)p2.w << 32 | p2.z) - out_base0;
+        r0 = p3.x;
+        r1 = p3.y;
     }
     const bool big = valid && count > kTileKeys;
     const uint64_t base = __shfl_sync(0xffffffffu, gword, 0) & ~3ull;  // 16-byte aligned start
@@ -129,8 +154,32 @@ __device__ void plan_run(const DevIndexView &ix, DecodeSmem &sm, uint32_t b, uin
         m.r0 = r0;
         m.r1 = r1;
     }
+    // width classes: a segment of c values takes G = 2^lg lanes, the smallest
+    // power of two with c <= 8G, and 32/G segments of one class (same kind,
+    // same G) share a warp; a lane's rank among its class's segments gives its unit
+    const uint32_t need_lanes = (count + 7u) >> 3;
+    const uint32_t lg = need_lanes <= 1u ? 0u : 32u - __clz(need_lanes - 1u);
+    const uint32_t cls = lane < n ? (codec_is_dgap(codec) ? 0u : 6u) + lg : 0xffu;
+    uint32_t nunits = 0;
+#pragma unroll
+    for (uint32_t c = 0; c < 12; ++c) {
+        const uint32_t mk = __ballot_sync(0xffffffffu, cls == c);
+        const uint32_t per = 32u >> (c % 6u), tot = __popc(mk);
+        if (cls == c) {
+            const uint32_t rank = __popc(mk & ((1u << lane) - 1u));
+            const uint32_t u = nunits + rank / per, slot = rank % per;
+            sm.useg[b][u][slot] = (uint8_t)lane;
+            if (slot == 0) {
+                sm.ucls[b][u] = (uint8_t)c;
+                sm.ucnt[b][u] = (uint8_t)min(per, tot - rank);
+            }
+        }
+        nunits += (tot + per - 1u) / per;
+    }
     const uint64_t need_last = __shfl_sync(0xffffffffu, need, n - 1);
     if (lane == 0) {
+        sm.nunits[b] = nunits;
+        sm.unext[b] = 0;
         sm.run_n[b] = n;
         sm.run_big[b] = first_big ? 1u : 0u;
         sm.run_first[b] = s0;
@@ -145,32 +194,59 @@ __device__ void plan_run(const DevIndexView &ix, DecodeSmem &sm, uint32_t b, uin
     __syncwarp();
 }
 
-// Exceptions of a staged block (ParaPFor.cpp:116-125): patch the high bits
-// of the listed positions into vbuf[0, count).
-__device__ __noinline__ void patch_exceptions(const uint32_t *lows, BlkHdr h, uint32_t count, uint32_t *vbuf,
-                                              uint32_t lane) {
-    __syncwarp();
+// Group widths are template arguments (unrolled scans and strides) or, for
+// kLgRuntime, a run-time value (one body for every width: less code).
+constexpr uint32_t kLgRuntime = 8;
+#ifndef EXCL_DEC_DGAP_FIXED
+#define EXCL_DEC_DGAP_FIXED 0
+#endif
+#ifndef EXCL_DEC_RESID_FIXED
+#define EXCL_DEC_RESID_FIXED 1
+#endif
+
+// A warp's value buffer holds warp-relative element i at word i + i/32, so
+// lanes storing runs of 2, 4 or 8 consecutive values hit distinct banks.
+__device__ __forceinline__ uint32_t sw(uint32_t i) { return i + (i >> 5); }
+
+// Exceptions of a staged block (ParaPFor.cpp:116-125): the G = 2^lg lanes of
+// a group patch the high bits of the listed positions into the group's
+// values, element i at vals[sw(base + i)]. Positions are distinct, so the
+// lanes never write the same word.
+__device__ __forceinline__ void group_patch(const uint32_t *lows, BlkHdr h, uint32_t count, uint32_t codec,
+                                            uint32_t *vals, uint32_t base, uint32_t lg, uint32_t sub) {
     const uint32_t *pb = lows + words_for(count, h.lb);
+    if (codec_is_newpfd(codec)) {
+        // NewPFD: exceptions from the Simple-16 stream, one lane of the group
+        if (sub == 0)
+            newpfd_patch_at(pb, h.en, h.lb, 0, count,
+                            [vals, base](uint32_t i) -> uint32_t & { return vals[sw(base + i)]; });
+        return;
+    }
     const uint32_t *hp = pb + words_for(h.en, h.eb);
-    for (uint32_t x = lane; x < h.en; x += 32) {
+    for (uint32_t x = sub; x < h.en; x += 1u << lg) {
         const uint32_t pbit = x * h.eb, hbit = x * h.hb;
         const uint32_t p = __funnelshift_r(pb[pbit >> 5], pb[(pbit >> 5) + 1], pbit & 31u) & ((1u << h.eb) - 1u);
         const uint32_t hv = __funnelshift_r(hp[hbit >> 5], hp[(hbit >> 5) + 1], hbit & 31u) & ((1u << h.hb) - 1u);
-        if (p < count) vbuf[p] |= hv << h.lb;
+        if (p < count) vals[sw(base + p)] |= hv << h.lb;
     }
-    __syncwarp();
 }
 
-// d-gap codecs: lane l owns a run of ceil(count/32) consecutive values; the
-// segment head replaces value 0, then a warp scan turns gaps into docIDs
-// (ParaPFD_Decompression_kernel.cu:205-263).
-__device__ __noinline__ void decode_dgap_staged(const uint32_t *blk, const RunMeta &m, uint32_t *vbuf,
-                                                uint32_t *__restrict__ out, uint32_t lane) {
+// d-gap codecs, one segment per group of G = 2^lg lanes (count <= 8G):
+// lane `sub` owns a run of ceil(count/G) consecutive values; the segment head
+// replaces value 0, then a G-wide scan turns gaps into docIDs
+// (ParaPFD_Decompression_kernel.cu:205-263) and the group stores its values
+// G-wide from the warp's buffer. Inactive groups (act false) run the same
+// warp-wide steps on count 0. Every lane of the warp passes the same lg.
+template <uint32_t LGT>
+__device__ __forceinline__ void group_dgap(const uint32_t *blk, const RunMeta &m, bool act, uint32_t lg_rt,
+                                           uint32_t sub, uint32_t *vals, uint32_t base, uint32_t *__restrict__ out) {
+    const uint32_t lg = LGT == kLgRuntime ? lg_rt : LGT;
+    const uint32_t G = 1u << lg;
     const BlkHdr h = blk_hdr(blk[0]);
     const uint32_t *lows = blk + 1;
-    const uint32_t count = m.count;
-    const uint32_t vpl = (count + 31u) >> 5;
-    const uint32_t el = lane * vpl;
+    const uint32_t count = act ? m.count : 0u;
+    const uint32_t vpl = (count + G - 1u) >> lg;
+    const uint32_t el = sub * vpl;
     const uint32_t mask = (1u << h.lb) - 1u;
     uint32_t v[8];
 #pragma unroll
@@ -179,24 +255,24 @@ __device__ __noinline__ void decode_dgap_staged(const uint32_t *blk, const RunMe
         const uint32_t wi = bit >> 5;
         v[q] = (q < (int)vpl && el + q < count) ? (__funnelshift_r(lows[wi], lows[wi + 1], bit & 31u) & mask) : 0u;
     }
-    if (h.en) {
+    const bool exc = count && h.en;
+    if (__any_sync(0xffffffffu, exc)) {
+        if (exc) {
 #pragma unroll
-        for (int q = 0; q < 8; ++q)
-            if (q < (int)vpl && el + q < count) vbuf[el + q] = v[q];
-        if (codec_is_newpfd(m.codec)) {
-            // NewPFD: exceptions from the Simple-16 stream, one lane
-            __syncwarp();
-            if (lane == 0) newpfd_patch(lows + words_for(count, h.lb), h.en, h.lb, 0, count, vbuf);
-            __syncwarp();
-        } else {
-            patch_exceptions(lows, h, count, vbuf, lane);
+            for (int q = 0; q < 8; ++q)
+                if (q < (int)vpl && el + q < count) vals[sw(base + el + q)] = v[q];
         }
+        __syncwarp();
+        if (exc) group_patch(lows, h, count, m.codec, vals, base, lg, sub);
+        __syncwarp();
+        if (exc) {
 #pragma unroll
-        for (int q = 0; q < 8; ++q)
-            if (q < (int)vpl && el + q < count) v[q] = vbuf[el + q];
+            for (int q = 0; q < 8; ++q)
+                if (q < (int)vpl && el + q < count) v[q] = vals[sw(base + el + q)];
+        }
         __syncwarp();
     }
-    if (lane == 0) v[0] = m.head;
+    if (sub == 0) v[0] = count ? m.head : 0u;
     uint32_t run = 0;
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
@@ -205,49 +281,58 @@ __device__ __noinline__ void decode_dgap_staged(const uint32_t *blk, const RunMe
     }
     uint32_t incl = run;
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= (uint32_t)o) incl += t;
+    for (uint32_t o = 1; o < G; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o, G);
+        if (sub >= o) incl += t;
     }
     const uint32_t ex = incl - run;
 #pragma unroll
     for (int q = 0; q < 8; ++q)
-        if (q < (int)vpl && el + q < count) vbuf[el + q] = v[q] + ex;
+        if (q < (int)vpl && el + q < count) vals[sw(base + el + q)] = v[q] + ex;
     __syncwarp();
     uint32_t *o = out + m.ob;
-    for (uint32_t i = lane; i < count; i += 32) o[i] = vbuf[i];
+    for (uint32_t i = sub; i < count; i += G) o[i] = vals[sw(base + i)];
     __syncwarp();
 }
 
-// Residual codecs (LRC, LRCSeg, SegLRC, HS_SegLRC): no scan; lane l owns
-// values l, l+32, ... so the 32 lanes read neighbouring words (no bank
-// conflicts) and every value goes from its register straight into a coalesced
-// 128-byte store. Reconstruction as the reference:
+// Residual codecs (LRC, LRCSeg, SegLRC, HS_SegLRC), one segment per group of
+// G lanes: no scan; lane `sub` owns values sub, sub+G, ... so the group reads
+// neighbouring words and every value goes from its register straight into a
+// G-wide store. Reconstruction as the reference:
 // LRC_Decompression_kernel.cu:254, SegLRC_Decompression_kernel.cu:252.
-__device__ __forceinline__ void decode_resid_staged(const uint32_t *blk, const RunMeta &m, uint32_t *vbuf,
-                                                    uint32_t *__restrict__ out, uint32_t lane) {
+template <uint32_t LGT>
+__device__ __forceinline__ void group_resid(const uint32_t *blk, const RunMeta &m, bool act, uint32_t lg_rt,
+                                            uint32_t sub, uint32_t *vals, uint32_t base,
+                                            uint32_t *__restrict__ out) {
+    const uint32_t lg = LGT == kLgRuntime ? lg_rt : LGT;
+    const uint32_t G = 1u << lg;
     const BlkHdr h = blk_hdr(blk[0]);
     const uint32_t *lows = blk + 1;
-    const uint32_t count = m.count;
+    const uint32_t count = act ? m.count : 0u;
     const uint32_t mask = (1u << h.lb) - 1u;
-    const int nqs = (int)((count + 31u) >> 5);  // 32-value steps this segment needs
     uint32_t v[8];
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
-        if (q >= nqs) break;
-        const uint32_t t = lane + 32u * q;
+        const uint32_t t = sub + G * q;
         const uint32_t bit = t * h.lb;
         const uint32_t wi = bit >> 5;
-        v[q] = __funnelshift_r(lows[wi], lows[wi + 1], bit & 31u) & mask;  // past count: unused
+        v[q] = t < count ? (__funnelshift_r(lows[wi], lows[wi + 1], bit & 31u) & mask) : 0u;
     }
-    if (h.en) {
+    const bool exc = count && h.en;
+    if (__any_sync(0xffffffffu, exc)) {
+        if (exc) {
 #pragma unroll
-        for (int q = 0; q < 8; ++q)
-            if (q < nqs && lane + 32u * q < count) vbuf[lane + 32u * q] = v[q];
-        patch_exceptions(lows, h, count, vbuf, lane);
+            for (int q = 0; q < 8; ++q)
+                if (sub + G * q < count) vals[sw(base + sub + G * q)] = v[q];
+        }
+        __syncwarp();
+        if (exc) group_patch(lows, h, count, m.codec, vals, base, lg, sub);
+        __syncwarp();
+        if (exc) {
 #pragma unroll
-        for (int q = 0; q < 8; ++q)
-            if (q < nqs && lane + 32u * q < count) v[q] = vbuf[lane + 32u * q];
+            for (int q = 0; q < 8; ++q)
+                if (sub + G * q < count) v[q] = vals[sw(base + sub + G * q)];
+        }
         __syncwarp();
     }
     uint32_t *o = out + m.ob;
@@ -255,8 +340,7 @@ __device__ __forceinline__ void decode_resid_staged(const uint32_t *blk, const R
         const float slope = __uint_as_float(m.r0);
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
-            if (q >= nqs) break;
-            const uint32_t t = lane + 32u * q;
+            const uint32_t t = sub + G * q;
             if (t < count) o[t] = v[q] + pred_lrc(m.start + t, slope, (int32_t)m.r1);
         }
     } else if (m.codec == EXCL_CODEC_LRCSEG) {
@@ -265,20 +349,17 @@ __device__ __forceinline__ void decode_resid_staged(const uint32_t *blk, const R
         const uint32_t aux = m.aux, i0 = m.start;
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
-            if (q >= nqs) break;
-            const uint32_t t = lane + 32u * q;
+            const uint32_t t = sub + G * q;
             if (t < count) o[t] = v[q] + pred_fma(i0 + t, a, b) + aux;
         }
     } else {
-        // segment-local index t < 256: float(lane) + 32q is exactly float(t)
-        const float a = m.a, b = m.b, lf = (float)lane;
+        // segment-local index t < 256, exact in float
+        const float a = m.a, b = m.b;
         const uint32_t aux = m.aux;
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
-            if (q >= nqs) break;
-            const uint32_t t = lane + 32u * q;
-            const float tf = __fadd_rn(lf, 32.0f * (float)q);
-            if (t < count) o[t] = v[q] + (uint32_t)__float2int_rz(__fmaf_rn(tf, a, b)) + aux;
+            const uint32_t t = sub + G * q;
+            if (t < count) o[t] = v[q] + (uint32_t)__float2int_rz(__fmaf_rn(__uint2float_rn(t), a, b)) + aux;
         }
     }
 }
@@ -335,7 +416,7 @@ __global__ void __launch_bounds__(kDecWarps * 32, kDecCtasPerSm) k_decode_tma(De
     const bool any = sm.have[0] != 0;  // this CTA got a chunk
     for (uint32_t it = 0; any; ++it) {
         const uint32_t b = it % kStages;
-        const uint32_t n = sm.run_n[b], big = sm.run_big[b], first = sm.run_first[b];
+        const uint32_t big = sm.run_big[b], first = sm.run_first[b];
         __syncthreads();  // everyone has read the run header before warp 0 refills the ring
         if (w == 0) plan_next((it + kStages - 1) % kStages);  // the stage decoded in the previous iteration
         if (big) {
@@ -357,11 +438,41 @@ __global__ void __launch_bounds__(kDecWarps * 32, kDecCtasPerSm) k_decode_tma(De
                 }
             }
             phase[b] ^= 1u;
+            // units are claimed from a shared counter, so warp 0, which planned
+            // the next run first, decodes fewer of them when planning ran long
             if (!failed)
-                for (uint32_t j = w; j < n; j += kDecWarps) {
-                    const RunMeta &m = sm.meta[b][j];
-                    if (codec_is_dgap(m.codec)) decode_dgap_staged(sm.stage[b] + m.woff, m, sm.vals[w], out, lane);
-                    else decode_resid_staged(sm.stage[b] + m.woff, m, sm.vals[w], out, lane);
+                for (;;) {
+                    uint32_t u = 0;
+                    if (lane == 0) u = atomicAdd(&sm.unext[b], 1u);
+                    u = __shfl_sync(0xffffffffu, u, 0);
+                    if (u >= sm.nunits[b]) break;
+                    // unit u: group grp of G = 2^lg lanes takes the unit's grp-th segment
+                    const uint32_t c = sm.ucls[b][u], lg = c % 6u;
+                    const uint32_t grp = lane >> lg, sub = lane & ((1u << lg) - 1u);
+                    const bool act = grp < sm.ucnt[b][u];
+                    const RunMeta &m = sm.meta[b][sm.useg[b][u][act ? grp : 0u]];
+                    const uint32_t base = grp * (8u << lg);
+                    const uint32_t *blk = sm.stage[b] + m.woff;
+                    uint32_t *vals = sm.vals[w];
+#define EXCL_DEC_CALL(F, L) F<L>(blk, m, act, lg, sub, vals, base, out)
+#define EXCL_DEC_SWITCH(F)                                  \
+    switch (lg) {                                           \
+        case 0: EXCL_DEC_CALL(F, 0); break;                 \
+        case 1: EXCL_DEC_CALL(F, 1); break;                 \
+        case 2: EXCL_DEC_CALL(F, 2); break;                 \
+        case 3: EXCL_DEC_CALL(F, 3); break;                 \
+        case 4: EXCL_DEC_CALL(F, 4); break;                 \
+        default: EXCL_DEC_CALL(F, 5); break;                \
+    }
+                    if (c < 6u) {
+                        if (EXCL_DEC_DGAP_FIXED) { EXCL_DEC_SWITCH(group_dgap) }
+                        else EXCL_DEC_CALL(group_dgap, kLgRuntime);
+                    } else {
+                        if (EXCL_DEC_RESID_FIXED) { EXCL_DEC_SWITCH(group_resid) }
+                        else EXCL_DEC_CALL(group_resid, kLgRuntime);
+                    }
+#undef EXCL_DEC_SWITCH
+#undef EXCL_DEC_CALL
                 }
         }
         __syncthreads();  // stage b and its metadata are free again; the newly planned header is visible

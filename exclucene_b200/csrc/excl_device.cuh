@@ -218,9 +218,10 @@ __device__ __forceinline__ uint32_t s16_next(S16Cursor &c) {
 }
 
 // Adds the high parts of a NewPFD block's exceptions at positions in
-// [e0, e0 + kc) to buf[pos - e0] (serial: one thread).
-__device__ __forceinline__ void newpfd_patch(const uint32_t *s16, uint32_t en, uint32_t b, uint32_t e0, uint32_t kc,
-                                             uint32_t *buf) {
+// [e0, e0 + kc) to the buffer word at(pos - e0) (serial: one thread).
+template <class At>
+__device__ __forceinline__ void newpfd_patch_at(const uint32_t *s16, uint32_t en, uint32_t b, uint32_t e0, uint32_t kc,
+                                                At at) {
     S16Cursor pc, hc;
     s16_start(pc, s16);
     s16_start(hc, s16);
@@ -230,8 +231,13 @@ __device__ __forceinline__ void newpfd_patch(const uint32_t *s16, uint32_t en, u
         const uint32_t d = s16_next(pc);
         p = i ? p + d + 1u : d;
         const uint32_t h = s16_next(hc);
-        if (p >= e0 && p < e0 + kc) buf[p - e0] += h << b;
+        if (p >= e0 && p < e0 + kc) at(p - e0) += h << b;
     }
+}
+
+__device__ __forceinline__ void newpfd_patch(const uint32_t *s16, uint32_t en, uint32_t b, uint32_t e0, uint32_t kc,
+                                             uint32_t *buf) {
+    newpfd_patch_at(s16, en, b, e0, kc, [buf](uint32_t i) -> uint32_t & { return buf[i]; });
 }
 
 // Warp-cooperative decode of elements [e0, e0 + kc) (kc <= 256) of one

@@ -75,9 +75,17 @@ struct alignas(64) ProbeRec {
     float a, b;      // segment regression (SegLRC, HS_SegLRC)
     uint32_t lr;     // regression window ranges L | R << 16, kProbeUnbounded if wider
     uint32_t start;  // list position of the first element (second half: HS lists only)
-    uint32_t pad[7];
+    // whole-list decode: the list's codec and regression words, the segment's
+    // first output position, so a decode plan needs no second dependent load
+    uint32_t codec;
+    uint64_t ob;
+    uint32_t r0, r1;
+    uint32_t pad[2];
 };
 static_assert(sizeof(ProbeRec) == 64, "ProbeRec layout");
+static_assert(offsetof(ProbeRec, a) == 20 && offsetof(ProbeRec, start) == 32 && offsetof(ProbeRec, codec) == 36 &&
+                  offsetof(ProbeRec, ob) == 40 && offsetof(ProbeRec, r0) == 48,
+              "decode plans read ProbeRec as four 16-byte vectors");
 
 #ifdef __CUDACC__
 #define EXCL_HD __host__ __device__ __forceinline__

@@ -475,6 +475,11 @@ extern "C" int excl_index_upload(excl_ctx *ctx, excl_index *ix) {
         p.b = rg.b;
         p.lr = std::min<uint32_t>(rg.L, kProbeUnbounded) | std::min<uint32_t>(rg.R, kProbeUnbounded) << 16;
         p.start = r.start;
+        const ListDesc &L = ix->lists[slist[g]];
+        p.codec = L.codec;
+        p.ob = pb[slist[g]] + r.start;
+        p.r0 = L.reg[0];
+        p.r1 = L.reg[1];
     }
     int st = 0;
     st |= dalloc(ctx, &d->lists, ix->lists.size(), "index lists");
