@@ -418,6 +418,30 @@ void fixed_list_directory(ListDesc &d, const uint32_t *head, uint32_t ns, std::v
 
 int32_t seg_pred_host(uint32_t idx, float a, float b) { return f2i_sat(std::fmaf((float)idx, a, b)); }
 
+uint32_t lrc_pred_host(uint32_t idx, float slope, int32_t icpt) {
+    return (uint32_t)f2i_sat((float)(int32_t)idx * slope) + (uint32_t)icpt;
+}
+
+int variable_list_tiles(const uint32_t *cnt, uint32_t ns, std::vector<uint64_t> &tiles) {
+    // a segment larger than a tile is cut into 256-slices; consecutive small
+    // segments are grouped while they fit in one tile
+    uint32_t s = 0;
+    while (s < ns) {
+        if (cnt[s] >= kTileKeys) {
+            if (cnt[s] > kTileMaxE0) return EXCL_E_FORMAT;
+            for (uint32_t k = 0; k < cnt[s]; k += kTileKeys) tiles.push_back(tile_pack(s, k, 1));
+            ++s;
+            continue;
+        }
+        uint32_t keys = 0, g = 0;
+        while (s + g < ns && g < kTileMaxSegs && cnt[s + g] < kTileKeys && keys + cnt[s + g] <= kTileKeys)
+            keys += cnt[s + g++];
+        tiles.push_back(tile_pack(s, 0, g));
+        s += g;
+    }
+    return EXCL_OK;
+}
+
 SegReg fit_host(const uint32_t *y, uint32_t n) {
     const Fit f = fit_segment(y, n);
     return SegReg{f.a, f.b, f.L, f.R};
@@ -514,8 +538,7 @@ static void build_list(const uint32_t *docs, uint32_t n, uint32_t codec, const e
             int32_t mn = 0;
             std::vector<int32_t> r(n);
             for (uint32_t i = 0; i < n; ++i) {
-                const float pf = (float)(int32_t)i * f.slope;
-                const int32_t y = (int32_t)((uint32_t)f2i_sat(pf) + (uint32_t)f.icpt);
+                const int32_t y = (int32_t)lrc_pred_host(i, f.slope, f.icpt);
                 r[i] = (int32_t)(docs[i] - (uint32_t)y);
                 if (i == 0 || r[i] < mn) mn = r[i];
             }
@@ -596,22 +619,7 @@ static void build_list(const uint32_t *docs, uint32_t n, uint32_t codec, const e
     if (d.log2_block) {
         d.ntiles = ns;
     } else {
-        // Variable segments: a segment larger than a tile is cut into 256-slices;
-        // consecutive small segments are grouped while they fit in one tile.
-        uint32_t s = 0;
-        while (s < ns) {
-            if (cnt[s] >= kTileKeys) {
-                if (cnt[s] > kTileMaxE0) return fail(o, EXCL_E_FORMAT, "hash bucket larger than 2^24 postings");
-                for (uint32_t k = 0; k < cnt[s]; k += kTileKeys) o.tiles.push_back(tile_pack(s, k, 1));
-                ++s;
-                continue;
-            }
-            uint32_t keys = 0, g = 0;
-            while (s + g < ns && g < kTileMaxSegs && cnt[s + g] < kTileKeys && keys + cnt[s + g] <= kTileKeys)
-                keys += cnt[s + g++];
-            o.tiles.push_back(tile_pack(s, 0, g));
-            s += g;
-        }
+        if (variable_list_tiles(cnt.data(), ns, o.tiles)) return fail(o, EXCL_E_FORMAT, "hash bucket larger than 2^24 postings");
         d.ntiles = (uint32_t)o.tiles.size();
     }
 }

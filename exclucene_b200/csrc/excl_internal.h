@@ -133,6 +133,10 @@ int build_index(const uint32_t *docs, const uint64_t *loff, uint32_t nlists, con
 void fixed_list_directory(ListDesc &d, const uint32_t *head, uint32_t ns, std::vector<uint32_t> &dir);
 // SegLRC/LRCSeg/HS prediction (int)(idx * a + b) with one rounding, saturating.
 int32_t seg_pred_host(uint32_t idx, float a, float b);
+// LRC prediction (int)((float)i * slope) + icpt (LRC_Generator_kernel.cu:70), wrapping.
+uint32_t lrc_pred_host(uint32_t idx, float slope, int32_t icpt);
+// Tile map of a variable-segment (HS) list from its segment counts.
+int variable_list_tiles(const uint32_t *cnt, uint32_t ns, std::vector<uint64_t> &tiles);
 // The least-squares fit of SegLRC/LRCSeg (segment or list level) on the host.
 SegReg fit_host(const uint32_t *y, uint32_t n);
 

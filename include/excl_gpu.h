@@ -134,19 +134,32 @@ int excl_index_export(const excl_index *ix, excl_list_info *lists, uint32_t *wor
                       uint32_t *dir);
 
 /* ---------------------------------------------------------------------------
- * The reference's on-disk files. An index in the ParaPFD, NewPFD or SegLRC format with
- * 256-entry segments (SegmentSize of the reference encoders) is written as the
- * file set its intersection binaries read, and such a file set is loaded
- * without re-encoding: `<dir>/<name>` + .ind1 .ind2 .segNum .segHead .segOffset
- * and, for ParaPFD and NewPFD, .segMedian (ParaPFD_Compression/main.cpp:81-232, NewPFD_Compression/main.cpp); for
- * SegLRC, .ind2_distance_base .regression_info .regression_info_list
- * (SegLRC_Compression/main.cpp:80-207, SegLRC_Generator.cu:338-412; the
- * reference keeps these three in a second directory). .ind1 records are
- * {u32 length; u64 byte offset}, 16 bytes (main.cpp:32-35). Loading checks
- * that lists, segments and blocks are consistent and in bounds
- * (EXCL_E_FORMAT otherwise). */
+ * The reference's on-disk files. An index in the ParaPFD, NewPFD, SegLRC, LRC
+ * or LRCSeg format with 256-entry segments (SegmentSize of the reference
+ * encoders), or in HS_SegLRC with the reference's bucketing (shift from the
+ * list length, expected bucket size 256), is written as the file set the
+ * reference's intersection binaries read, and such a file set is loaded
+ * without re-encoding. `<dir>/<name>` +
+ *   ParaPFD, NewPFD: .ind1 .ind2 .segNum .segHead .segOffset .segMedian
+ *     (ParaPFD_Compression/main.cpp:81-232)
+ *   SegLRC: .ind1 .ind2 .segNum .segHead .segOffset .ind2_distance_base
+ *     .regression_info (per segment) .regression_info_list (per list)
+ *     (SegLRC_Compression/main.cpp:80-207, SegLRC_Generator.cu:338-412)
+ *   LRC: .ind1 .ind2 .segNum .segHead .segOffset .regression_info
+ *     ({float slope; i32 intercept; float range} per list; LRC_Compression/
+ *     main.cpp:94-215, LRC_Generator.cu:96-191)
+ *   LRCSeg: .ind1 .ind2 .segNum .segHead .segOffset .ind2_distance_base
+ *     .regression_info (per list) (LRCSeg_Compression/main.cpp:78-200)
+ *   HS_SegLRC: .ind1 .ind2 .HashSeg_offset .HashSeg_info .segNum .segOffset
+ *     .ind2_distance_base .regression_info (per bucket, empty buckets included)
+ *     (HS_SegLRC_Generator.cu:180-594, HS_SegLRC_Compression/main.cpp:78-190)
+ * The reference keeps the regression and hash files in a second directory.
+ * .ind1 records are {u32 length; u64 byte offset}, 16 bytes (main.cpp:32-35).
+ * Loading checks that lists, segments and blocks are consistent and in bounds,
+ * and that every hash bucket decodes to its own docID range (EXCL_E_FORMAT
+ * otherwise). */
 int excl_index_save_reference(const excl_index *ix, const char *dir, const char *name);
-int excl_index_load_reference(const char *dir, const char *name, uint32_t codec /* PARAPFD, NEWPFD or SEGLRC */,
+int excl_index_load_reference(const char *dir, const char *name, uint32_t codec /* PARAPFD NEWPFD SEGLRC LRC LRCSEG HS_SEGLRC */,
                               excl_index **out);
 
 /* The reference's .query stream (ParaPFD_Intersection.cu:139-142): per query a

@@ -102,21 +102,89 @@ def inverted_list_digest():
             f.write(f"frac {frac} words {nw} sha256 {h}\n")
 
 
+def hash_info(d):
+    """HS_SegLRC_Generator.cu:545-581 restated: the bucket shift from the
+    length (kExceptedBucketSize 256) and each bucket's first element."""
+    n = len(d)
+    maxb = int(d[-1]).bit_length()
+    if n <= 256:
+        return maxb, [0, n]
+    shift = maxb - ((n + 255) // 256).bit_length()
+    nb = (int(d[-1]) >> shift) + 1
+    off = [int(np.searchsorted(d, b << shift)) for b in range(nb)] + [n]
+    return shift, off
+
+
+def hs_file_set(lists):
+    """HS_SegLRC file set (HS_SegLRC_Generator.cu:180-594, HS_SegLRC_Compression/
+    main.cpp:78-190): per-bucket fits from the reference's getRegressionInfo,
+    blocks from the reference's ParaPFor.cpp (FRAC 0). Residuals are computed
+    against each element's own bucket; the reference generator's lower-bound
+    search gives the first element after empty buckets to the first of them
+    (HS_SegLRC_Generator_kernel.cu:73-85), so for a list with empty buckets
+    this set differs from its output in exactly those elements' residuals and
+    their buckets' bases and blocks (the list here that has them: the third)."""
+    import struct
+
+    ind1, ind2, hoff, hinfo, bnum, boff, base, reg = b"", [], [], [], [], [], [], []
+    words_total = 0
+    for d in lists:
+        n = len(d)
+        shift, off = hash_info(d)
+        hoff.append(len(hinfo))
+        hinfo += [shift, len(off) - 1] + off
+        bnum.append(len(boff))
+        enc = oracle.encode_list(d, 4, 256, 0.0, bucket=256)
+        assert enc["shift"] == shift and np.array_equal(enc["starts"], [o for o, e in zip(off, off[1:]) if e > o])
+        ind1 += struct.pack("<IIQ", n, 0, 4 * words_total)
+        nw, k = 0, 0
+        for b in range(len(off) - 1):
+            lo, hi = off[b], off[b + 1]
+            boff.append(nw)
+            if hi == lo:
+                # an empty bucket as the generator leaves it: empty fit, next docID as base
+                reg.append(oracle.ref_fit_seg_raw(np.zeros(0, np.uint32)))
+                base.append(int(d[lo]))
+                continue
+            raw = oracle.ref_fit_seg_raw(d[lo:hi])
+            assert np.array_equal(raw, enc["reg"][k]), "oracle bucket fit differs from the reference's"
+            vals = oracle.decode_block(enc["words"][enc["off"][k]:], hi - lo)[0]
+            reg.append(raw)
+            base.append(int(enc["aux"][k]))
+            w = oracle.ref_encode(np.ascontiguousarray(vals, np.uint32), 0.0)
+            ind2.append(w)
+            nw += len(w)
+            k += 1
+        words_total += nw
+    return {".ind1": np.frombuffer(ind1, np.uint8), ".ind2": np.concatenate(ind2).view(np.uint8),
+            ".HashSeg_offset": np.array(hoff, np.uint32).view(np.uint8),
+            ".HashSeg_info": np.array(hinfo, np.uint32).view(np.uint8),
+            ".segNum": np.array(bnum, np.uint32).view(np.uint8),
+            ".segOffset": np.array(boff, np.uint32).view(np.uint8),
+            ".ind2_distance_base": np.array(base, np.uint32).view(np.uint8),
+            ".regression_info": np.stack(reg).reshape(-1).view(np.uint8)}
+
+
 def reference_file_sets():
     """The reference's compressed file sets for a small seeded corpus, laid out
     as its compressors write them (ParaPFD_Compression/main.cpp:81-232,
-    SegLRC_Compression/main.cpp:80-207), every block encoded by the reference's
-    own ParaPFor.cpp. ParaPFD: d-gaps over the whole list, FRAC 0.12. SegLRC:
-    per-segment and per-list fits from the reference's getRegressionInfo (the
-    oracle's restated fit is pinned to it by regression_fits.npz), residuals
-    doc - (int)(i * a + b) minus the segment minimum, FRAC 0."""
+    SegLRC_Compression/main.cpp:80-207, LRC_Compression/main.cpp:94-215,
+    LRCSeg_Compression/main.cpp:78-200), every block encoded by the
+    reference's own ParaPFor.cpp (NewPFor.cpp for NewPFD). ParaPFD: d-gaps
+    over the whole list, FRAC 0.12. SegLRC / LRCSeg / LRC: fits from the
+    reference's getRegressionInfo (the oracle's restated fits are pinned to it
+    by regression_fits.npz) per segment / per list, residuals
+    doc - (int)(i * a + b) (LRC: (int)((float)i * slope) + intercept) minus the
+    segment's (LRC: the list's) minimum, FRAC 0. HS_SegLRC on its own corpus
+    (hs_file_set)."""
     import struct
 
     rng = np.random.default_rng(0xF11E5)
     lens = [1, 100, 255, 256, 257, 700, 2000, 5000]
     lists = [np.sort(rng.choice(1 << 22, size=n, replace=False)).astype(np.uint32) for n in lens]
     out = {"docs": np.concatenate(lists), "lens": np.array(lens, np.uint32)}
-    for codec, name, frac in ((0, "parapfd", 0.12), (3, "seglrc", 0.0), (6, "newpfd", 0.12)):
+    for codec, name, frac in ((0, "parapfd", 0.12), (3, "seglrc", 0.0), (6, "newpfd", 0.12), (1, "lrc", 0.0),
+                              (2, "lrcseg", 0.0)):
         ind1, ind2, seg_num, heads, offs, aux, reg, listreg = b"", [], [], [], [], [], [], []
         words_total = 0
         for d in lists:
@@ -129,15 +197,21 @@ def reference_file_sets():
                 vals, med = gaps, [int(d[s + min(256, n - s) // 2]) for s in range(0, n, 256)]
                 segvals = [vals[s:s + 256] for s in range(0, n, 256)]
             else:
-                enc = oracle.encode_list(d, 3, 256, 0.0)
+                enc = oracle.encode_list(d, codec, 256, 0.0)
                 segvals = [oracle.decode_block(enc["words"][o:], int(c))[0] for o, c in zip(enc["off"], enc["counts"])]
                 med = [int(x) for x in enc["aux"]]
                 reg.append(enc["reg"].astype(np.uint32))
                 listreg.append(enc["listreg"].astype(np.uint32))
-                for k, (s0, c) in enumerate(zip(enc["starts"], enc["counts"])):
-                    raw = oracle.ref_fit_seg_raw(d[s0:s0 + c])
-                    assert np.array_equal(raw, enc["reg"][k]), "oracle segment fit differs from the reference's"
-                assert np.array_equal(oracle.ref_fit_seg_raw(d), enc["listreg"]), "list fit differs"
+                if codec == 3:
+                    for k, (s0, c) in enumerate(zip(enc["starts"], enc["counts"])):
+                        raw = oracle.ref_fit_seg_raw(d[s0:s0 + c])
+                        assert np.array_equal(raw, enc["reg"][k]), "oracle segment fit differs from the reference's"
+                if codec in (2, 3):
+                    assert np.array_equal(oracle.ref_fit_seg_raw(d), enc["listreg"]), "list fit differs"
+                else:
+                    # LRC: slope and range as the reference's fit; the intercept moved by the residual minimum
+                    raw = oracle.ref_fit_lrc_raw(d)
+                    assert raw[0] == enc["listreg"][0] and raw[2] == enc["listreg"][2], "LRC fit differs"
             ind1 += struct.pack("<IIQ", n, 0, 4 * words_total)
             nw = 0
             for k, v in enumerate(segvals):
@@ -156,12 +230,28 @@ def reference_file_sets():
                  ".segOffset": np.array(offs, np.uint32).view(np.uint8)}
         if codec in (0, 6):
             files[".segMedian"] = np.array(aux, np.uint32).view(np.uint8)
-        else:
+        elif codec == 3:
             files[".ind2_distance_base"] = np.array(aux, np.uint32).view(np.uint8)
             files[".regression_info"] = np.concatenate(reg).reshape(-1).view(np.uint8)
             files[".regression_info_list"] = np.stack(listreg).reshape(-1).view(np.uint8)
+        elif codec == 2:
+            files[".ind2_distance_base"] = np.array(aux, np.uint32).view(np.uint8)
+            files[".regression_info"] = np.stack(listreg).reshape(-1).view(np.uint8)
+        else:
+            files[".regression_info"] = np.stack(listreg)[:, :3].reshape(-1).view(np.uint8)
         for suffix, data in files.items():
             out[name + suffix] = data
+    # HS_SegLRC: uniform lists, a clustered one with empty buckets, short ones
+    hrng = np.random.default_rng(0x4A5B)
+    hl = [np.sort(hrng.choice(1 << 22, size=n, replace=False)).astype(np.uint32) for n in (3000, 700)]
+    gap = np.concatenate([hrng.choice(1 << 18, size=600, replace=False),
+                          (3 << 20) + hrng.choice(1 << 18, size=600, replace=False)])
+    hl.append(np.sort(gap).astype(np.uint32))
+    hl += [np.sort(hrng.choice(1 << 22, size=n, replace=False)).astype(np.uint32) for n in (1, 256, 257)]
+    out["hs_docs"] = np.concatenate(hl)
+    out["hs_lens"] = np.array([len(x) for x in hl], np.uint32)
+    for suffix, data in hs_file_set(hl).items():
+        out["hs_seglrc" + suffix] = data
     # a .query stream over the corpus (ParaPFD_Intersection.cu:139-142)
     q = [[6, 7], [5, 6, 7], [0, 7], [7, 4, 3], [2, 2], [1]]
     out["queries"] = np.array([x for t in q for x in [len(t)] + t], np.uint32).view(np.uint8)

@@ -196,7 +196,7 @@ def test_autotune_keeps_output_exact(corpus, expected):
         ctx.close()
 
 
-@pytest.mark.parametrize("codec", ["parapfd", "seglrc", "newpfd"])
+@pytest.mark.parametrize("codec", ["parapfd", "seglrc", "newpfd", "lrc", "lrcseg", "hs_seglrc"])
 def test_reference_file_set_runs_unchanged(gpu_ctx, tmp_path, codec):
     """A file set written as the reference's compressors write it (blocks from
     its own encoder) loads without re-encoding, decodes to its lists and
@@ -207,15 +207,26 @@ def test_reference_file_set_runs_unchanged(gpu_ctx, tmp_path, codec):
     sets = {"parapfd": (".ind1", ".ind2", ".segNum", ".segHead", ".segOffset", ".segMedian"),
             "newpfd": (".ind1", ".ind2", ".segNum", ".segHead", ".segOffset", ".segMedian"),
             "seglrc": (".ind1", ".ind2", ".segNum", ".segHead", ".segOffset", ".ind2_distance_base",
-                       ".regression_info", ".regression_info_list")}
+                       ".regression_info", ".regression_info_list"),
+            "lrc": (".ind1", ".ind2", ".segNum", ".segHead", ".segOffset", ".regression_info"),
+            "lrcseg": (".ind1", ".ind2", ".segNum", ".segHead", ".segOffset", ".ind2_distance_base",
+                       ".regression_info"),
+            "hs_seglrc": (".ind1", ".ind2", ".HashSeg_offset", ".HashSeg_info", ".segNum", ".segOffset",
+                          ".ind2_distance_base", ".regression_info")}
     for suffix in sets[codec]:
         g[codec + suffix].tofile(os.path.join(tmp_path, "g" + suffix))
     ix = ex.Index.load_reference(str(tmp_path), "g", codec)
     gpu_ctx.upload(ix)
-    docs = g["docs"]
-    loff = np.concatenate([[0], np.cumsum(g["lens"].astype(np.uint64))]).astype(np.uint64)
+    pre = "hs_" if codec == "hs_seglrc" else ""
+    docs = g[pre + "docs"]
+    loff = np.concatenate([[0], np.cumsum(g[pre + "lens"].astype(np.uint64))]).astype(np.uint64)
     assert np.array_equal(gpu_ctx.decode_lists(ix), docs)
-    terms, toff = ex.query_parse(g["queries"].tobytes())
+    if pre:
+        q = [[0, 1], [2, 0], [1, 2, 0], [3], [4, 5], [0, 1, 2, 4], [5, 5], [2, 4]]
+        terms = np.array([t for x in q for t in x], np.uint32)
+        toff = np.concatenate([[0], np.cumsum([len(x) for x in q])]).astype(np.uint32)
+    else:
+        terms, toff = ex.query_parse(g["queries"].tobytes())
     eoffs, edocs = oracle.answer(docs, loff, terms, toff)
     for algo in ("bsearch", "hashseg"):
         offs, got = gpu_ctx.intersect(ix, terms, toff, algo=algo)
