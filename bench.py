@@ -383,15 +383,16 @@ def main():
     sizes = ix.sizes()
     arrays = ix.export()
     index_build = None
-    if params["codec"] in ("parapfd", "seglrc") and "codecs" not in params:
+    if params["codec"] in ("parapfd", "seglrc", "lrc", "lrcseg", "hs_seglrc", "hs_parapfd") and "codecs" not in params:
         # the same index built by the device kernels, from the docIDs in HBM
         d_all = torch.from_numpy(w.docs.view(np.int32)).to(dev)
         torch.cuda.synchronize()
+        hs = {k: params[k] for k in ("hs_bucket", "hs_kbits", "hs_ubits") if k in params}
         ctx.build_index(d_all.data_ptr(), w.list_offsets, codec=params["codec"], block=params["block"],
-                        frac=params["frac"]).close()  # warm-up
+                        frac=params["frac"], **hs).close()  # warm-up
         t_build = time.perf_counter()
         dix = ctx.build_index(d_all.data_ptr(), w.list_offsets, codec=params["codec"], block=params["block"],
-                              frac=params["frac"])
+                              frac=params["frac"], **hs)
         dev_build_s = time.perf_counter() - t_build
         da = dix.export()
         same = all(np.array_equal(getattr(da, k), getattr(arrays, k)) for k in ("words", "seg_head", "seg_rec",

@@ -453,15 +453,20 @@ class Context:
                              g.ctypes.data_as(fp), C.byref(loss)), self, "excl_model_grad")
         return g, loss.value
 
-    def build_index(self, d_docs: int, list_offsets, codec="seglrc", block: int = 256, frac: float = 0.0) -> Index:
-        """Build a ParaPFD or SegLRC index on this context's GPU from a device
-        docID array (pointer; list l = d_docs[list_offsets[l] .. list_offsets[l+1])).
-        Byte-identical to Index(docs, list_offsets, ...); upload it before use."""
+    def build_index(self, d_docs: int, list_offsets, codec="seglrc", block: int = 256, frac: float = 0.0,
+                    hs_bucket: int = 256, hs_kbits: int = 0, hs_ubits: int = 32) -> Index:
+        """Build an index (ParaPFD, LRC, LRCSeg, SegLRC, HS_SegLRC or HS_ParaPFD)
+        on this context's GPU from a device docID array (pointer; list l =
+        d_docs[list_offsets[l] .. list_offsets[l+1])). Byte-identical to
+        Index(docs, list_offsets, ...) with the same parameters; upload it before use."""
         loff = np.ascontiguousarray(list_offsets, dtype=np.uint64)
         p = BuildParams()
         p.codec = CODEC_NAMES[codec] if isinstance(codec, str) else int(codec)
         p.block = block
         p.frac = frac
+        p.hs_bucket = hs_bucket
+        p.hs_kbits = hs_kbits
+        p.hs_ubits = hs_ubits
         h = C.c_void_p()
         _check_status(_build_dev(self._h, C.c_void_p(d_docs), loff.ctypes.data_as(u64p), len(loff) - 1, C.byref(p),
                                  C.byref(h)), self, "excl_index_build_device")

@@ -391,6 +391,13 @@ static FitLrc fit_lrc(const uint32_t *y, uint32_t n) {
     return f;
 }
 
+void fit_lrc_host(const uint32_t *y, uint32_t n, float *slope, int32_t *icpt, float *range) {
+    const FitLrc f = fit_lrc(y, n);
+    *slope = f.slope;
+    *icpt = f.icpt;
+    *range = f.range;
+}
+
 // Float -> int32 truncation as the device evaluates it (cvt.rzi.s32.f32):
 // out-of-range values saturate and NaN becomes 0. The reference's residuals
 // were computed and are decoded on the GPU, so this is the format's semantics.

@@ -139,6 +139,8 @@ uint32_t lrc_pred_host(uint32_t idx, float slope, int32_t icpt);
 int variable_list_tiles(const uint32_t *cnt, uint32_t ns, std::vector<uint64_t> &tiles);
 // The least-squares fit of SegLRC/LRCSeg (segment or list level) on the host.
 SegReg fit_host(const uint32_t *y, uint32_t n);
+// The LRC list fit on the host (LRC_Generator.cu:221-287): slope, intercept, range.
+void fit_lrc_host(const uint32_t *y, uint32_t n, float *slope, int32_t *icpt, float *range);
 
 }  // namespace excl
 

@@ -1,7 +1,8 @@
-"""Index build on the GPU: for the ParaPFD and SegLRC formats the device build
-gives the host build's arrays bit for bit (fits, residual bases, medians,
-blocks, directories), rejects unordered lists, and the index it builds answers
-queries as the oracle does."""
+"""Index build on the GPU: for the ParaPFD, LRC, LRCSeg, SegLRC, HS_SegLRC and
+HS_ParaPFD formats the device build gives the host build's arrays bit for bit
+(hash partition, fits, residual bases, medians, blocks, directories, tile
+maps), rejects unordered lists, and the index it builds answers queries as the
+oracle does."""
 import numpy as np
 import pytest
 
@@ -38,26 +39,49 @@ def corpus():
     return synth.zipf_corpus(seed=21, ndocs=1 << 20, nterms=2500, cap=150_000, nq=800, qmin=2, qmax=5)
 
 
-@pytest.mark.parametrize("codec,block,frac", [("parapfd", 256, 0.0), ("parapfd", 128, 0.12), ("parapfd", 256, 0.64),
-                                              ("seglrc", 256, 0.0), ("seglrc", 128, 0.1)])
-def test_device_build_equals_host_build(gpu_ctx, corpus, codec, block, frac):
+HS_BUCKET = dict(hs_bucket=256)          # the reference's bucketing: shift from the length
+HS_TOP = dict(hs_kbits=12, hs_ubits=32)   # top 12 bits of the docID
+CASES = [("parapfd", 256, 0.0, {}), ("parapfd", 128, 0.12, {}), ("parapfd", 256, 0.64, {}),
+         ("seglrc", 256, 0.0, {}), ("seglrc", 128, 0.1, {}), ("lrc", 256, 0.0, {}), ("lrc", 128, 0.1, {}),
+         ("lrcseg", 256, 0.0, {}), ("lrcseg", 128, 0.1, {}),
+         ("hs_seglrc", 256, 0.0, HS_BUCKET), ("hs_seglrc", 256, 0.1, HS_BUCKET), ("hs_seglrc", 256, 0.0, HS_TOP),
+         ("hs_parapfd", 128, 0.1, HS_BUCKET), ("hs_parapfd", 256, 0.0, HS_TOP)]
+
+
+@pytest.mark.parametrize("codec,block,frac,hs", CASES)
+def test_device_build_equals_host_build(gpu_ctx, corpus, codec, block, frac, hs):
     import torch
 
     for docs, loff in ((corpus.docs, corpus.list_offsets), _edge_lists()):
         d = torch.from_numpy(docs.view(np.int32)).cuda()
         torch.cuda.synchronize()
         try:
-            got = gpu_ctx.build_index(d.data_ptr(), loff, codec=codec, block=block, frac=frac)
+            got = gpu_ctx.build_index(d.data_ptr(), loff, codec=codec, block=block, frac=frac, **hs)
         except ex.ExclError as e:
             # where the host build rejects the data (unrepresentable block), so must the device
             with pytest.raises(ex.ExclError):
-                ex.Index(docs, loff, codec=codec, block=block, frac=frac)
+                ex.Index(docs, loff, codec=codec, block=block, frac=frac, **hs)
             assert e.status == ex.api.E_FORMAT
             continue
-        want = ex.Index(docs, loff, codec=codec, block=block, frac=frac)
+        want = ex.Index(docs, loff, codec=codec, block=block, frac=frac, **hs)
         _same_index(got, want)
         got.close()
         want.close()
+
+
+@pytest.mark.parametrize("codec,hs", [("lrc", {}), ("lrcseg", {}), ("hs_seglrc", HS_BUCKET)])
+def test_device_built_index_answers_queries(gpu_ctx, corpus, codec, hs):
+    import torch
+
+    d = torch.from_numpy(corpus.docs.view(np.int32)).cuda()
+    torch.cuda.synchronize()
+    ix = gpu_ctx.build_index(d.data_ptr(), corpus.list_offsets, codec=codec, **hs)
+    gpu_ctx.upload(ix)
+    assert np.array_equal(gpu_ctx.decode_lists(ix), corpus.docs)
+    offs, got = gpu_ctx.intersect(ix, corpus.terms, corpus.term_offsets, algo="hashseg")
+    eo, ed = oracle.answer(corpus.docs, corpus.list_offsets, corpus.terms, corpus.term_offsets)
+    assert np.array_equal(offs.astype(np.uint64), eo) and np.array_equal(got, ed)
+    ix.close()
 
 
 def test_device_build_of_a_list_range_and_queries(gpu_ctx, corpus):
@@ -89,9 +113,9 @@ def test_device_build_rejects_unordered_lists(gpu_ctx):
     docs = np.array([5, 9, 9, 12, 1, 2, 3], np.uint32)  # list 0 repeats 9
     d = torch.from_numpy(docs.view(np.int32)).cuda()
     torch.cuda.synchronize()
-    for codec in ("parapfd", "seglrc"):
+    for codec in ("parapfd", "seglrc", "lrc", "lrcseg", "hs_seglrc", "hs_parapfd"):
         with pytest.raises(ex.ExclError) as e:
             gpu_ctx.build_index(d.data_ptr(), np.array([0, 4, 7], np.uint64), codec=codec)
         assert e.value.status == ex.api.E_INVALID
     with pytest.raises(ex.ExclError):
-        gpu_ctx.build_index(d.data_ptr(), np.array([0, 4, 7], np.uint64), codec="lrc")  # host build only
+        gpu_ctx.build_index(d.data_ptr(), np.array([0, 4, 7], np.uint64), codec="newpfd")  # host build only
