@@ -61,7 +61,20 @@ struct DevIndexView {
     const uint64_t *seg_gword;  // first word of each segment's block (nsegs + 1 entries)
     const ProbeRec *seg_probe;  // per-segment probe records
     ModelView models;
+    uint32_t codec_mask;        // bit c set: some list of the index has codec c
 };
+
+// Codec families a kernel instance is compiled for; an index whose lists all
+// belong to one family launches the narrower instance (fewer registers).
+enum : int { kKindAny = 0, kKindResid = 1, kKindDgap = 2 };
+__host__ __device__ inline int codec_kind(uint32_t mask) {
+    const uint32_t resid = (1u << EXCL_CODEC_LRC) | (1u << EXCL_CODEC_LRCSEG) | (1u << EXCL_CODEC_SEGLRC) |
+                           (1u << EXCL_CODEC_HS_SEGLRC);
+    const uint32_t dgap = (1u << EXCL_CODEC_PARAPFD) | (1u << EXCL_CODEC_HS_PARAPFD);
+    if (mask && !(mask & ~resid)) return kKindResid;
+    if (mask && !(mask & ~dgap)) return kKindDgap;
+    return kKindAny;
+}
 
 enum : uint32_t {
     kErrTerms = 1u,      // a query has more than kMaxTerms terms
@@ -246,8 +259,11 @@ __device__ __forceinline__ void newpfd_patch(const uint32_t *s16, uint32_t en, u
 // replace element 0 by the segment head and take a warp inclusive scan
 // (ParaPFD_Decompression_kernel.cu:205-263), residual codecs add the
 // regression prediction and base (SegLRC_Decompression_kernel.cu:249-252).
+template <int KIND = kKindAny>
 __device__ __forceinline__ void warp_decode(const DevIndexView &ix, const ListDesc &L, uint32_t sg, uint32_t e0,
                                             uint32_t kc, uint32_t *buf, uint32_t lane) {
+    const bool dgap = KIND == kKindDgap || (KIND == kKindAny && codec_is_dgap(L.codec));
+    const bool newpfd = KIND == kKindAny && codec_is_newpfd(L.codec);
     const SegRec rec = ix.seg_rec[sg];
     const uint32_t *blk = ix.words + L.word_base + rec.off;
     const BlkHdr h = blk_hdr(ldg(blk));
@@ -265,7 +281,7 @@ __device__ __forceinline__ void warp_decode(const DevIndexView &ix, const ListDe
             if (j < (int)vpl && el + j < kc) buf[el + j] = v[j];
         __syncwarp();
         const uint32_t *pb = blk + 1 + words_for(rec.count, h.lb);
-        if (codec_is_newpfd(L.codec)) {
+        if (newpfd) {
             if (lane == 0) newpfd_patch(pb, h.en, h.lb, e0, kc, buf);
         } else {
             const uint32_t *hp = pb + words_for(h.en, h.eb);
@@ -280,7 +296,7 @@ __device__ __forceinline__ void warp_decode(const DevIndexView &ix, const ListDe
             if (j < (int)vpl && el + j < kc) v[j] = buf[el + j];
         __syncwarp();
     }
-    if (codec_is_dgap(L.codec)) {
+    if (dgap) {
         if (lane == 0 && e0 == 0) v[0] = ix.seg_head[sg];
         uint32_t run = 0;
 #pragma unroll

@@ -21,7 +21,7 @@ namespace excl {
 __device__ __forceinline__ int64_t imax64(int64_t a, int64_t b) { return a > b ? a : b; }
 __device__ __forceinline__ int64_t imin64(int64_t a, int64_t b) { return a < b ? a : b; }
 
-template <int ALGO>
+template <int ALGO, int KIND>
 __device__ __forceinline__ bool probe_key(const DevIndexView &ix, const ListDesc &L, uint32_t key, uint32_t &fallback) {
     if (key < L.first_doc || key > L.last_doc) return false;
     uint32_t lo, hi;
@@ -69,8 +69,9 @@ __device__ __forceinline__ bool probe_key(const DevIndexView &ix, const ListDesc
     rec.count = q0.w;
     const uint32_t *blk = ix.words + L.word_base + rec.off;
     const BlkHdr h = blk_hdr(q1.x);
-    if (codec_is_newpfd(L.codec)) return dgap_find_newpfd(blk, h, rec.count, q0.x, rec.aux, key);
-    if (codec_is_dgap(L.codec)) return dgap_find(blk, h, rec.count, q0.x, rec.aux, key);
+    if (KIND == kKindAny && codec_is_newpfd(L.codec)) return dgap_find_newpfd(blk, h, rec.count, q0.x, rec.aux, key);
+    if (KIND == kKindDgap || (KIND == kKindAny && codec_is_dgap(L.codec)))
+        return dgap_find(blk, h, rec.count, q0.x, rec.aux, key);
     // list position of the segment: only learned windows and the LRC/LRCSeg
     // predictors use it, and those lists have fixed blocks
     rec.start = (uint32_t)s << L.log2_block;
@@ -143,9 +144,11 @@ __device__ __forceinline__ int locate_segment(const DevIndexView &ix, const List
 // otherwise each key is probed on its own (probe_key).
 
 // MINB: resident 8-warp CTAs per SM the register budget is cut for (4: 64
-// registers, no spills; 5: 48; 6: 40, a few spills), traded for more probes
-// in flight; the launch shape is an autotuner choice.
-template <int ALGO, int WARPS, int MINB>
+// registers; 5: 48; 6: 40), traded for more probes in flight; the launch
+// shape is an autotuner choice. KIND: the codec family the instance handles
+// (kKindAny for mixed indexes); a one-family instance needs fewer registers
+// (residual codecs: no spills at 64, the 64-register spills at 48).
+template <int ALGO, int WARPS, int MINB, int KIND>
 __global__ void __launch_bounds__(WARPS * 32, (8 / WARPS) * MINB) k_probe(DevIndexView ix, BatchView b) {
     __shared__ uint32_t s_keys[WARPS][kTileKeys];
     __shared__ uint32_t s_merge[WARPS][kMergeCap];
@@ -175,7 +178,7 @@ __global__ void __launch_bounds__(WARPS * 32, (8 / WARPS) * MINB) k_probe(DevInd
             const uint32_t sg = L.seg_base + ti;
             kc = ix.seg_rec[sg].count;
             first_elem = ti << L.log2_block;
-            warp_decode(ix, L, sg, 0, kc, keys, lane);
+            warp_decode<KIND>(ix, L, sg, 0, kc, keys, lane);
         } else {
             const uint64_t tm = ix.tilemap[L.tile_base + ti];
             const uint32_t sg0 = L.seg_base + (uint32_t)(tm >> 32);
@@ -183,7 +186,7 @@ __global__ void __launch_bounds__(WARPS * 32, (8 / WARPS) * MINB) k_probe(DevInd
             first_elem = ix.seg_rec[sg0].start + e0;
             for (uint32_t g = 0; g < ns; ++g) {
                 const uint32_t c = min(kTileKeys - kc, ix.seg_rec[sg0 + g].count - (g ? 0u : e0));
-                warp_decode(ix, L, sg0 + g, g ? 0u : e0, c, keys + kc, lane);
+                warp_decode<KIND>(ix, L, sg0 + g, g ? 0u : e0, c, keys + kc, lane);
                 kc += c;
             }
         }
@@ -213,7 +216,7 @@ __global__ void __launch_bounds__(WARPS * 32, (8 / WARPS) * MINB) k_probe(DevInd
                             for (uint32_t sg = L.seg_base + s0; sg <= L.seg_base + (uint32_t)s1; ++sg) {
                                 const SegRec r = ix.seg_rec[sg];
                                 for (uint32_t e0 = 0; e0 < r.count; e0 += kTileKeys)
-                                    warp_decode(ix, L, sg, e0, min(kTileKeys, r.count - e0), mbuf + (r.start - a0) + e0,
+                                    warp_decode<KIND>(ix, L, sg, e0, min(kTileKeys, r.count - e0), mbuf + (r.start - a0) + e0,
                                                 lane);
                             }
                         }
@@ -240,7 +243,7 @@ __global__ void __launch_bounds__(WARPS * 32, (8 / WARPS) * MINB) k_probe(DevInd
                     }
                     f = valid && lo < span && mbuf[lo] == key;
                 } else {
-                    f = valid && probe_key<ALGO>(ix, L, key, fallbacks);
+                    f = valid && probe_key<ALGO, KIND>(ix, L, key, fallbacks);
                 }
                 probes += valid;
                 const uint32_t m = __ballot_sync(0xffffffffu, f);
@@ -286,7 +289,7 @@ __global__ void __launch_bounds__(WARPS * 32, (8 / WARPS) * MINB) k_probe(DevInd
 // ---------------------------------------------------------------------------
 // Launchers.
 
-template <int ALGO, int WARPS, int MINB>
+template <int ALGO, int WARPS, int MINB, int KIND>
 static void launch_probe_t(const DevIndexView &ix, const BatchView &b, int nsm, cudaStream_t st) {
     // persistent grid: as many CTAs as fit on the device at once, so every
     // resident warp pulls work items
@@ -295,21 +298,30 @@ static void launch_probe_t(const DevIndexView &ix, const BatchView &b, int nsm, 
     cudaGetDevice(&dev);
     int per_sm = dev >= 0 && dev < 64 ? occ[dev] : 0;
     if (!per_sm) {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_probe<ALGO, WARPS, MINB>, WARPS * 32, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_probe<ALGO, WARPS, MINB, KIND>, WARPS * 32, 0);
         per_sm = per_sm > 0 ? per_sm : 1;
         if (dev >= 0 && dev < 64) occ[dev] = per_sm;
     }
     const uint32_t grid = (uint32_t)std::max(1, std::min(per_sm, (8 / WARPS) * MINB) * nsm);
-    k_probe<ALGO, WARPS, MINB><<<grid, WARPS * 32, 0, st>>>(ix, b);
+    k_probe<ALGO, WARPS, MINB, KIND><<<grid, WARPS * 32, 0, st>>>(ix, b);
+}
+
+template <int ALGO, int WARPS, int MINB>
+static void launch_probe_k(const DevIndexView &ix, const BatchView &b, int nsm, cudaStream_t st) {
+    switch (codec_kind(ix.codec_mask)) {
+        case kKindResid: launch_probe_t<ALGO, WARPS, MINB, kKindResid>(ix, b, nsm, st); break;
+        case kKindDgap: launch_probe_t<ALGO, WARPS, MINB, kKindDgap>(ix, b, nsm, st); break;
+        default: launch_probe_t<ALGO, WARPS, MINB, kKindAny>(ix, b, nsm, st); break;
+    }
 }
 
 template <int WARPS, int MINB>
 static void launch_probe_a(const DevIndexView &ix, const BatchView &b, int algo, int nsm, cudaStream_t st) {
     switch (algo) {
-        case EXCL_ALGO_BSEARCH: launch_probe_t<EXCL_ALGO_BSEARCH, WARPS, MINB>(ix, b, nsm, st); break;
-        case EXCL_ALGO_HASHSEG: launch_probe_t<EXCL_ALGO_HASHSEG, WARPS, MINB>(ix, b, nsm, st); break;
-        case EXCL_ALGO_LEARNED: launch_probe_t<EXCL_ALGO_LEARNED, WARPS, MINB>(ix, b, nsm, st); break;
-        default: launch_probe_t<EXCL_ALGO_AUTO, WARPS, MINB>(ix, b, nsm, st); break;
+        case EXCL_ALGO_BSEARCH: launch_probe_k<EXCL_ALGO_BSEARCH, WARPS, MINB>(ix, b, nsm, st); break;
+        case EXCL_ALGO_HASHSEG: launch_probe_k<EXCL_ALGO_HASHSEG, WARPS, MINB>(ix, b, nsm, st); break;
+        case EXCL_ALGO_LEARNED: launch_probe_k<EXCL_ALGO_LEARNED, WARPS, MINB>(ix, b, nsm, st); break;
+        default: launch_probe_k<EXCL_ALGO_AUTO, WARPS, MINB>(ix, b, nsm, st); break;
     }
 }
 

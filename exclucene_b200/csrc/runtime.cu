@@ -209,6 +209,7 @@ DevIndexView DeviceIndex::view(const ModelView &mv) const {
     v.seg_gword = seg_gword;
     v.seg_probe = seg_probe;
     v.models = mv;
+    v.codec_mask = codec_mask;
     return v;
 }
 
@@ -522,6 +523,7 @@ extern "C" int excl_index_upload(excl_ctx *ctx, excl_index *ix) {
                ix->tilemap.size() * 8 + pb.size() * 8 + slist.size() * 4 + sgw.size() * 8 +
                prec.size() * sizeof(ProbeRec);
     d->device = ctx->device;
+    for (uint32_t l = 0; l < ix->nlists; ++l) d->codec_mask |= 1u << ix->lists[l].codec;
     ix->dev = d;
     if (ix->models) st = models_upload(ctx, ix);
     return st;

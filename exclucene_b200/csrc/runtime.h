@@ -23,6 +23,7 @@ struct DeviceIndex {
     uint32_t *seg_list = nullptr;
     uint64_t *seg_gword = nullptr;
     ProbeRec *seg_probe = nullptr;
+    uint32_t codec_mask = 0;  // bit c: some list has codec c
     size_t bytes = 0;
     int device = 0;
     void release();
