@@ -71,7 +71,8 @@ MERGE_OFF = 0xFFFFFFFF
 
 class TuneReport(C.Structure):
     _fields_ = [("algo", C.c_uint32), ("warps_per_cta", C.c_uint32), ("ctas_per_sm", C.c_uint32),
-                ("merge_segs", C.c_uint32), ("best_ms", C.c_float), ("default_ms", C.c_float), ("tried", C.c_uint32)]
+                ("merge_segs", C.c_uint32), ("best_ms", C.c_float), ("default_ms", C.c_float), ("tried", C.c_uint32),
+                ("tile_split", C.c_uint32)]
 
     def as_dict(self) -> dict:
         d = {k: getattr(self, k) for k, _ in self._fields_}
@@ -146,6 +147,7 @@ _qparse = _sig("excl_query_parse", C.c_int, C.c_void_p, C.c_size_t, u32p, C.c_si
 _qencode = _sig("excl_query_encode", C.c_int, u32p, u32p, C.c_uint32, C.c_void_p, C.c_size_t,
                 C.POINTER(C.c_size_t))
 _autotune = _sig("excl_autotune", C.c_int, C.c_void_p, C.c_void_p, u32p, u32p, C.c_uint32, C.POINTER(TuneReport))
+_set_tuning = _sig("excl_ctx_set_tuning", C.c_int, C.c_void_p, C.POINTER(TuneReport))
 _learn = _sig("excl_learn_models", C.c_int, C.c_void_p, C.c_void_p, C.POINTER(LearnParams), C.POINTER(LearnReport))
 _mexport = _sig("excl_model_export", C.c_int, C.c_void_p, C.c_uint32, C.POINTER(C.c_float), C.POINTER(C.c_float),
                 C.POINTER(C.c_int32), C.POINTER(C.c_uint32))
@@ -159,7 +161,7 @@ EXPORTED = ["excl_learn_models", "excl_model_export", "excl_model_grad", "excl_m
             "excl_ctx_destroy", "excl_last_error", "excl_ctx_stream", "excl_index_upload",
             "excl_decode_lists_device", "excl_decode_lists", "excl_submit", "excl_wait", "excl_batch_free",
             "excl_intersect_device", "excl_ctx_check", "excl_last_stats", "excl_checksum", "excl_submit_into",
-            "excl_host_alloc", "excl_host_free"]
+            "excl_host_alloc", "excl_host_free", "excl_ctx_set_tuning"]
 
 
 def _p32(a: np.ndarray):
@@ -471,6 +473,15 @@ class Context:
         _check_status(_build_dev(self._h, C.c_void_p(d_docs), loff.ctypes.data_as(u64p), len(loff) - 1, C.byref(p),
                                  C.byref(h)), self, "excl_index_build_device")
         return Index.from_handle(h, len(loff) - 1, np.diff(loff))
+
+    def set_tuning(self, algo="auto", warps_per_cta: int = 8, ctas_per_sm: int = 5, merge_segs: int = 2,
+                   tile_split: int = 0, **_ignored) -> None:
+        """Apply a launch setting (e.g. the dict autotune returned) without timing."""
+        r = TuneReport()
+        r.algo = ALGO_NAMES[algo] if isinstance(algo, str) else int(algo)
+        r.warps_per_cta, r.ctas_per_sm, r.tile_split = warps_per_cta, ctas_per_sm, tile_split
+        r.merge_segs = MERGE_OFF if merge_segs in (0, MERGE_OFF) else merge_segs
+        _check_status(_set_tuning(self._h, C.byref(r)), self, "excl_ctx_set_tuning")
 
     def autotune(self, ix: Index, terms, term_offsets) -> dict:
         """Times the sample batch under every candidate setting and keeps the

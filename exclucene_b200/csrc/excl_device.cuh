@@ -64,6 +64,23 @@ struct DevIndexView {
     uint32_t codec_mask;        // bit c set: some list of the index has codec c
 };
 
+// Tiles per fixed segment of a query's shortest list: 2^split, capped so a
+// tile keeps at least kMinBlock (32) keys; variable (HS) lists are not cut.
+__host__ __device__ inline uint32_t tile_split_of(uint32_t log2_block, uint32_t split) {
+    return log2_block > 5u ? (split < log2_block - 5u ? split : log2_block - 5u) : 0u;
+}
+
+// Tiles of a shortest list of n postings and ntiles whole-segment tiles when
+// fixed segments are cut: 2^s per segment, and only as many as the last
+// segment's postings fill (so no tile is empty and a list of n postings never
+// has more than n/32 + 1 tiles).
+__host__ __device__ inline uint32_t split_tiles(uint32_t n, uint32_t ntiles, uint32_t log2_block, uint32_t split) {
+    const uint32_t sp = tile_split_of(log2_block, split);
+    if (!sp || ntiles == 0) return ntiles;
+    const uint32_t last = n - ((ntiles - 1u) << log2_block), sub_log = log2_block - sp;
+    return ((ntiles - 1u) << sp) + ((last + (1u << sub_log) - 1u) >> sub_log);
+}
+
 // Codec families a kernel instance is compiled for; an index whose lists all
 // belong to one family launches the narrower instance (fewer registers).
 enum : int { kKindAny = 0, kKindResid = 1, kKindDgap = 2 };

@@ -154,7 +154,7 @@ __global__ void __launch_bounds__(WARPS * 32, (8 / WARPS) * MINB) k_probe(DevInd
     __shared__ uint32_t s_merge[WARPS][kMergeCap];
     __shared__ ListDesc s_list[WARPS];
     const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
-    uint32_t *keys = s_keys[w];
+    uint32_t *keys = s_keys[w];  // the tile's keys (a sub-range of the decoded segment when tiles are cut)
     uint32_t *mbuf = s_merge[w];
     ListDesc &L = s_list[w];
     const uint32_t T = min(b.tile_prefix[b.nq], b.max_tiles);
@@ -174,11 +174,18 @@ __global__ void __launch_bounds__(WARPS * 32, (8 / WARPS) * MINB) k_probe(DevInd
         // decode the tile's keys: one fixed segment, or 1..255 consecutive
         // variable segments / one 256-slice of a large segment
         uint32_t kc = 0, first_elem;
+        keys = s_keys[w];
         if (L.log2_block) {
-            const uint32_t sg = L.seg_base + ti;
-            kc = ix.seg_rec[sg].count;
-            first_elem = ti << L.log2_block;
-            warp_decode<KIND>(ix, L, sg, 0, kc, keys, lane);
+            // tile ti: part (ti mod 2^s) of segment ti >> s; the whole segment is
+            // decoded (d-gaps need its prefix) and the part's keys probed
+            const uint32_t sp = tile_split_of(L.log2_block, b.tile_split);
+            const uint32_t sg = L.seg_base + (ti >> sp);
+            const uint32_t cnt = ix.seg_rec[sg].count;
+            const uint32_t sub = (1u << L.log2_block) >> sp, e0 = (ti & ((1u << sp) - 1u)) * sub;
+            first_elem = ((ti >> sp) << L.log2_block) + e0;
+            warp_decode<KIND>(ix, L, sg, 0, cnt, keys, lane);
+            kc = e0 < cnt ? min(sub, cnt - e0) : 0u;
+            keys += e0;
         } else {
             const uint64_t tm = ix.tilemap[L.tile_base + ti];
             const uint32_t sg0 = L.seg_base + (uint32_t)(tm >> 32);

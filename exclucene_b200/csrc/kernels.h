@@ -21,6 +21,7 @@ struct BatchView {
     uint32_t *scratch;           // max_keys survivor slots, indexed by key position
     uint32_t max_tiles;
     uint32_t merge_segs;         // probe: merge when a tile's keys span at most this many segments (0: never)
+    uint32_t tile_split;         // fixed-block shortest lists: each segment is cut into 2^tile_split tiles
     uint64_t max_keys;
     uint32_t *err;               // error flag bits
     uint64_t *stats;             // [probes, fallbacks] or null

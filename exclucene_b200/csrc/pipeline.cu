@@ -139,7 +139,9 @@ __global__ void __launch_bounds__(kPackThreads) k_pack_scan(const ListDesc *__re
                 const bool v = j < k && id[j] < nlists;
                 bad |= j < k && id[j] >= nlists;
                 len[j] = v ? __ldg(&lists[id[j]].n) : 0xffffffffu;  // absent terms sort last
-                ntl[j] = v ? __ldg(&lists[id[j]].ntiles) : 0u;
+                ntl[j] = v ? split_tiles(len[j], __ldg(&lists[id[j]].ntiles), __ldg(&lists[id[j]].log2_block),
+                                         b.tile_split)
+                           : 0u;
             }
             if (bad) {
                 atomicOr(b.err, kErrTermId);
@@ -194,7 +196,8 @@ __global__ void __launch_bounds__(kPackThreads) k_pack_scan(const ListDesc *__re
                 len[j] = cl;
             }
             for (uint32_t i = 0; i < k; ++i) dst[i] = id[i];
-            nt = k ? __ldg(&lists[id[0]].ntiles) : 0u;
+            nt = k ? split_tiles(len[0], __ldg(&lists[id[0]].ntiles), __ldg(&lists[id[0]].log2_block), b.tile_split)
+                   : 0u;
             nk = k ? len[0] : 0u;
         }
         const_cast<uint32_t *>(b.qnterms)[q] = k;

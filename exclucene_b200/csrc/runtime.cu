@@ -280,6 +280,7 @@ int run_pipeline(excl_ctx *ctx, excl_index *ix, const uint32_t *d_terms, const u
     b.scratch = ctx->d_scratch;
     b.max_tiles = ctx->max_tiles;
     b.merge_segs = ctx->merge_segs;
+    b.tile_split = ctx->tile_split;
     b.max_keys = ctx->cfg.max_keys;
     b.err = ctx->d_misc + kMiscErr;
     b.stats = ctx->collect_stats ? ctx->d_stats : nullptr;
@@ -311,7 +312,8 @@ int run_pipeline(excl_ctx *ctx, excl_index *ix, const uint32_t *d_terms, const u
                                   (uint64_t)(uintptr_t)d_toff, nq, algo, (uint64_t)(uintptr_t)d_offsets,
                                   (uint64_t)(uintptr_t)d_docids, cap,
                                   (uint64_t)ctx->collect_stats | (uint64_t)ctx->merge_segs << 8 |
-                                      (uint64_t)ctx->warps << 16 | (uint64_t)ctx->ctas_per_sm << 32};
+                                      (uint64_t)ctx->warps << 16 | (uint64_t)ctx->ctas_per_sm << 32 |
+                                      (uint64_t)ctx->tile_split << 40};
         const bool same = ctx->gkey_seen && std::memcmp(key, ctx->gkey, sizeof key) == 0;
         if (same || ctx->gexec) {
             if (!same || !ctx->gexec) {
@@ -648,9 +650,10 @@ extern "C" int excl_autotune(excl_ctx *ctx, excl_index *ix, const uint32_t *term
     // candidates are timed without graphs, on the context's own buffers
     const bool graphs = ctx->use_graphs;
     const int w0 = ctx->warps, c0 = ctx->ctas_per_sm, t0 = ctx->tuned_algo;
-    const uint32_t m0 = ctx->merge_segs;
+    const uint32_t m0 = ctx->merge_segs, sp0 = ctx->tile_split;
     ctx->use_graphs = false;
     ctx->tuned_algo = -1;
+    ctx->tile_split = 0;
     auto time_one = [&](uint32_t algo, int warps, int ctas, uint32_t merge, float *ms) -> int {
         ctx->warps = warps;
         ctx->ctas_per_sm = ctas;
@@ -696,17 +699,32 @@ extern "C" int excl_autotune(excl_ctx *ctx, excl_index *ix, const uint32_t *term
                     }
                 }
     }
+    // then, with the best setting, fixed segments cut into 2 or 4 tiles
+    // (shorter work items: the persistent queue's tail evens out)
+    uint32_t bsp = 0;
+    for (uint32_t sp = 1; sp <= 2 && !s; ++sp) {
+        ctx->tile_split = sp;
+        float ms = 0;
+        s = time_one(ba, bw, bc, bm, &ms);
+        ++tried;
+        if (!s && ms < best) {
+            best = ms;
+            bsp = sp;
+        }
+    }
     ctx->use_graphs = graphs;
     if (s) {
         ctx->warps = w0;
         ctx->ctas_per_sm = c0;
         ctx->merge_segs = m0;
         ctx->tuned_algo = t0;
+        ctx->tile_split = sp0;
         return s;
     }
     ctx->warps = bw;
     ctx->ctas_per_sm = bc;
     ctx->merge_segs = bm;
+    ctx->tile_split = bsp;
     ctx->tuned_algo = (int)ba;
     rep->algo = ba;
     rep->warps_per_cta = (uint32_t)bw;
@@ -714,6 +732,7 @@ extern "C" int excl_autotune(excl_ctx *ctx, excl_index *ix, const uint32_t *term
     rep->merge_segs = bm ? bm : EXCL_MERGE_OFF;
     rep->best_ms = best;
     rep->tried = tried;
+    rep->tile_split = bsp;
     return EXCL_OK;
 }
 
@@ -748,6 +767,20 @@ extern "C" int excl_submit(excl_ctx *ctx, excl_index *ix, const uint32_t *terms,
 // runs and excl_wait has nothing left to copy. The batch's error word is
 // copied to its own pinned slot and the device word cleared behind it, so
 // batches in flight together each see their own flags.
+extern "C" int excl_ctx_set_tuning(excl_ctx *ctx, const excl_tune_report *rep) {
+    if (!ctx || !rep) return EXCL_E_INVALID;
+    if (rep->algo > EXCL_ALGO_LEARNED || (rep->warps_per_cta != 4 && rep->warps_per_cta != 8) ||
+        rep->ctas_per_sm < 4 || rep->ctas_per_sm > 6 || rep->tile_split > 2 ||
+        (rep->merge_segs != EXCL_MERGE_OFF && (rep->merge_segs == 0 || rep->merge_segs > 4)))
+        return EXCL_E_INVALID;
+    ctx->warps = (int)rep->warps_per_cta;
+    ctx->ctas_per_sm = (int)rep->ctas_per_sm;
+    ctx->merge_segs = rep->merge_segs == EXCL_MERGE_OFF ? 0u : rep->merge_segs;
+    ctx->tuned_algo = rep->algo == EXCL_ALGO_AUTO ? -1 : (int)rep->algo;
+    ctx->tile_split = rep->tile_split;
+    return EXCL_OK;
+}
+
 extern "C" int excl_submit_into(excl_ctx *ctx, excl_index *ix, const uint32_t *terms, const uint32_t *term_offsets,
                                 uint32_t nq, uint32_t algo, uint32_t *offsets, uint32_t *docids, uint64_t cap,
                                 excl_batch **ticket) {

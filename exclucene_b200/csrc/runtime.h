@@ -43,6 +43,7 @@ struct excl_ctx {
     int warps = 8;
     int ctas_per_sm = 4;
     uint32_t merge_segs = 2;
+    uint32_t tile_split = 0;  // log2 of the tiles each fixed segment of a shortest list is cut into
     int tuned_algo = -1;  // search method the autotuner chose for EXCL_ALGO_AUTO (-1: none)
     bool collect_stats = true;
     // CUDA graph of the last batch launched through excl_intersect_device

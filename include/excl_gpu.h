@@ -291,7 +291,8 @@ int excl_last_stats(excl_ctx *ctx, excl_batch_stats *st);
  * binary). Runs a sample batch (host arrays, as excl_submit) under every
  * candidate setting: search method (bsearch, hash directory, learned where
  * models exist), probe launch shape (warps per CTA x CTAs per SM) and merge
- * threshold (EXCL_MERGE_OFF, 1, 2, 4 segments). Each candidate is timed with
+ * threshold (EXCL_MERGE_OFF, 1, 2, 4 segments); then, for the best of those,
+ * tiles of whole segments or of halves / quarters of them. Each candidate is timed with
  * CUDA events (median of 3 after a warm-up); the fastest is kept in the
  * context and used by later batches submitted with EXCL_ALGO_AUTO. The sample
  * must fit the context's limits. */
@@ -300,9 +301,16 @@ typedef struct {
     float best_ms;     /* its device time for the sample */
     float default_ms;  /* device time of the untuned default (auto, 8 warps, 5 CTAs/SM, merge 2) */
     uint32_t tried;    /* candidates timed */
+    uint32_t tile_split; /* log2 of the tiles each fixed segment of a query's shortest list is cut into */
 } excl_tune_report;
 int excl_autotune(excl_ctx *ctx, excl_index *ix, const uint32_t *terms, const uint32_t *term_offsets, uint32_t nq,
                   excl_tune_report *report);
+/* Applies a setting (a report of an earlier excl_autotune, or one the caller
+ * fills: algo, warps_per_cta 4 or 8, ctas_per_sm 4-6, merge_segs 1-4 or
+ * EXCL_MERGE_OFF, tile_split 0-2) to the context without timing anything, so a
+ * host can keep its tuning across runs. EXCL_E_INVALID for values outside
+ * those ranges. */
+int excl_ctx_set_tuning(excl_ctx *ctx, const excl_tune_report *setting);
 
 /* ---------------------------------------------------------------------------
  * Serving loop: continuous batching of single queries. No counterpart in the

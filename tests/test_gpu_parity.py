@@ -188,9 +188,36 @@ def test_autotune_keeps_output_exact(corpus, expected):
         assert rep["algo"] in ("bsearch", "hashseg", "learned", "auto")
         assert rep["warps_per_cta"] in (4, 8) and rep["ctas_per_sm"] in (4, 5, 6)
         assert 0 < rep["best_ms"] <= rep["default_ms"]
+        assert rep["tile_split"] in (0, 1, 2)
         offs, docs = ctx.intersect(ix, corpus.terms, corpus.term_offsets, algo="auto")
         assert np.array_equal(offs.astype(np.uint64), eoffs)
         assert np.array_equal(docs, edocs)
+    finally:
+        ix.close()
+        ctx.close()
+
+
+@pytest.mark.parametrize("codec", ["parapfd", "seglrc", "hs_parapfd", "newpfd"])
+@pytest.mark.parametrize("split", [0, 1, 2])
+def test_tile_split_keeps_output_exact(corpus, expected, codec, split):
+    """Fixed segments of the shortest lists cut into 2^split tiles (the part's
+    keys probed after the whole segment is decoded) give the oracle's output,
+    with graphs and merges on; settings out of range are refused."""
+    ctx = ex.Context(0, max_queries=65536, max_keys=1 << 24, use_graphs=True)
+    ix = _index(corpus, codec, 128 if codec in DGAP else 256, 0.1 if codec in DGAP else 0.0)
+    ctx.upload(ix)
+    eoffs, edocs = expected
+    try:
+        for merge in (ex.api.MERGE_OFF, 2):
+            ctx.set_tuning(algo="hashseg", warps_per_cta=8, ctas_per_sm=4, merge_segs=merge, tile_split=split)
+            for _ in range(2):
+                offs, docs = ctx.intersect(ix, corpus.terms, corpus.term_offsets, algo="auto")
+                assert np.array_equal(offs.astype(np.uint64), eoffs)
+                assert np.array_equal(docs, edocs)
+        with pytest.raises(ex.ExclError):
+            ctx.set_tuning(tile_split=3)
+        with pytest.raises(ex.ExclError):
+            ctx.set_tuning(ctas_per_sm=7)
     finally:
         ix.close()
         ctx.close()
