@@ -456,6 +456,7 @@ using namespace excl;
 extern "C" int excl_index_build_device(excl_ctx *ctx, const uint32_t *d_docs, const uint64_t *list_offsets,
                                        uint32_t nlists, const excl_build_params *p, excl_index **out) {
     if (!ctx || !d_docs || !list_offsets || !p || !out || nlists == 0) return EXCL_E_INVALID;
+    std::lock_guard<std::recursive_mutex> g(ctx->op_mu);
     *out = nullptr;
     const uint32_t B = p->block, codec = p->codec;
     if (p->codecs || !device_codec(codec)) return EXCL_E_INVALID;

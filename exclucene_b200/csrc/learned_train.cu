@@ -500,6 +500,7 @@ using namespace excl;
 extern "C" int excl_learn_models(excl_ctx *ctx, excl_index *ix, const excl_learn_params *params,
                                  excl_learn_report *rep) {
     if (!ctx || !ix || !params) return EXCL_E_INVALID;
+    std::lock_guard<std::recursive_mutex> g(ctx->op_mu);
     if (!ix->dev) {
         ctx_error(ctx, "index not uploaded");
         return EXCL_E_INVALID;
@@ -645,6 +646,7 @@ extern "C" int excl_model_export(const excl_index *ix, uint32_t list, float *roo
 extern "C" int excl_model_grad(excl_ctx *ctx, const float *params, const float *x, const float *y, uint32_t n,
                                float *grad, float *loss) {
     if (!ctx || !params || !x || !y || !grad || n == 0) return EXCL_E_INVALID;
+    std::lock_guard<std::recursive_mutex> g(ctx->op_mu);
     cudaSetDevice(ctx->device);
     const uint32_t nb = (n + kTrainThreads - 1) / kTrainThreads;
     float *d_P = nullptr, *d_x = nullptr, *d_y = nullptr, *d_part = nullptr, *d_g = nullptr, *d_loss = nullptr;

@@ -441,6 +441,7 @@ extern "C" void *excl_ctx_stream(excl_ctx *ctx) { return ctx ? (void *)ctx->stre
 
 extern "C" int excl_index_upload(excl_ctx *ctx, excl_index *ix) {
     if (!ctx || !ix) return EXCL_E_INVALID;
+    std::lock_guard<std::recursive_mutex> g(ctx->op_mu);
     cudaSetDevice(ctx->device);
     if (ix->dev) {
         ix->dev->release();
@@ -545,6 +546,7 @@ extern "C" int excl_index_free(excl_index *ix) {
 
 extern "C" int excl_decode_lists_device(excl_ctx *ctx, excl_index *ix, uint32_t l0, uint32_t l1, uint32_t *d_out) {
     if (!ctx || !ix || !d_out || l0 >= l1 || l1 > ix->nlists) return EXCL_E_INVALID;
+    std::lock_guard<std::recursive_mutex> g(ctx->op_mu);
     if (!ix->dev) {
         ctx_error(ctx, "index not uploaded");
         return EXCL_E_INVALID;
@@ -561,6 +563,7 @@ extern "C" int excl_decode_lists_device(excl_ctx *ctx, excl_index *ix, uint32_t 
 
 extern "C" int excl_decode_lists(excl_ctx *ctx, excl_index *ix, uint32_t l0, uint32_t l1, uint32_t *out, size_t cap) {
     if (!ctx || !ix || !out || l0 >= l1 || l1 > ix->nlists) return EXCL_E_INVALID;
+    std::lock_guard<std::recursive_mutex> g(ctx->op_mu);
     uint64_t n = 0;
     for (uint32_t l = l0; l < l1; ++l) n += ix->lists[l].n;
     if (n > cap) return EXCL_E_CAPACITY;
@@ -582,12 +585,14 @@ extern "C" int excl_intersect_device(excl_ctx *ctx, excl_index *ix, const uint32
                                      const uint32_t *d_term_offsets, uint32_t nq, uint32_t algo, uint32_t *d_offsets,
                                      uint32_t *d_docids, uint64_t cap) {
     if (!ctx || !ix || !d_term_offsets || !d_offsets || (!d_docids && cap)) return EXCL_E_INVALID;
+    std::lock_guard<std::recursive_mutex> g(ctx->op_mu);
     cudaSetDevice(ctx->device);
     return run_pipeline(ctx, ix, d_terms, d_term_offsets, nq, algo, d_offsets, d_docids, cap);
 }
 
 extern "C" int excl_ctx_check(excl_ctx *ctx) {
     if (!ctx) return EXCL_E_INVALID;
+    std::lock_guard<std::recursive_mutex> g(ctx->op_mu);
     cudaSetDevice(ctx->device);
     int st = cuda_status(ctx, cudaStreamSynchronize(ctx->stream), "stream sync");
     if (st) return st;
@@ -599,10 +604,42 @@ struct excl_batch {
     uint32_t nq;
     cudaEvent_t done;
     bool waited;
-    // excl_submit_into: the caller's offsets array and this batch's error-word slot (-1 for excl_submit)
-    const uint32_t *into_offsets = nullptr;
-    int32_t slot = -1;
+    const uint32_t *into_offsets = nullptr;  // excl_submit_into: the caller's offsets array
+    int32_t slot = -1;                       // this batch's error-word slot in ctx->h_flags
+    uint64_t seq = 0;                        // excl_submit: its number among the context's excl_submit batches
 };
+
+// Ends a batch's stream work: its error word is copied to a pinned slot of
+// its own and the device word cleared behind it (so batches in flight
+// together each see their own flags), then its completion event is recorded.
+// The caller holds ctx->op_mu. On failure the batch is deleted.
+static int finish_batch(excl_ctx *ctx, excl_batch *b) {
+    using namespace excl;
+    if (ctx->free_flag_slots.empty()) {
+        ctx_error(ctx, "more than %u batches in flight", kFlagSlots);
+        cudaStreamSynchronize(ctx->stream);
+        delete b;
+        return EXCL_E_CAPACITY;
+    }
+    cudaStream_t st = ctx->stream;
+    const uint32_t slot = ctx->free_flag_slots.back();
+    uint32_t *hf = ctx->h_flags + slot;
+    *hf = 0;
+    int s = cuda_status(ctx, cudaMemcpyAsync(hf, ctx->d_misc + kMiscErr, 4, cudaMemcpyDeviceToHost, st), "d2h flags");
+    if (!s) s = cuda_status(ctx, cudaMemsetAsync(ctx->d_misc + kMiscErr, 0, 4, st), "clear flags");
+    if (!s) s = cuda_status(ctx, cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming), "event");
+    if (!s) s = cuda_status(ctx, cudaEventRecord(b->done, st), "record");
+    if (s) {
+        // the slot is not handed out: the copies above may still land in it
+        if (b->done) cudaEventDestroy(b->done);
+        cudaStreamSynchronize(st);
+        delete b;
+        return s;
+    }
+    ctx->free_flag_slots.pop_back();
+    b->slot = (int32_t)slot;
+    return EXCL_OK;
+}
 
 // Copies a host batch into the context's query buffers (after the previous
 // batch has released them). Returns the number of terms through *nterms.
@@ -644,6 +681,7 @@ static int stage_host_batch(excl_ctx *ctx, excl_index *ix, const uint32_t *terms
 extern "C" int excl_autotune(excl_ctx *ctx, excl_index *ix, const uint32_t *terms, const uint32_t *term_offsets,
                              uint32_t nq, excl_tune_report *rep) {
     if (!ctx || !ix || !term_offsets || !rep) return EXCL_E_INVALID;
+    std::lock_guard<std::recursive_mutex> g(ctx->op_mu);
     if (!ix->dev) return EXCL_E_INVALID;
     int s = stage_host_batch(ctx, ix, terms, term_offsets, nq, nullptr);
     if (s) return s;
@@ -740,6 +778,7 @@ extern "C" int excl_submit(excl_ctx *ctx, excl_index *ix, const uint32_t *terms,
                            uint32_t nq, uint32_t algo, excl_batch **ticket) {
     if (!ctx || !ix || !term_offsets || !ticket) return EXCL_E_INVALID;
     *ticket = nullptr;
+    std::lock_guard<std::recursive_mutex> g(ctx->op_mu);
     cudaStream_t st = ctx->stream;
     int s = stage_host_batch(ctx, ix, terms, term_offsets, nq, nullptr);
     if (!s) s = run_pipeline(ctx, ix, ctx->d_terms, ctx->d_toff, nq, algo, ctx->d_offsets, ctx->d_docids, ctx->docids_cap);
@@ -750,25 +789,16 @@ extern "C" int excl_submit(excl_ctx *ctx, excl_index *ix, const uint32_t *terms,
     if (s) return s;
     excl_batch *b = new (std::nothrow) excl_batch{ctx, nq, nullptr, false};
     if (!b) return EXCL_E_NOMEM;
-    s = cuda_status(ctx, cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming), "event");
-    if (!s) s = cuda_status(ctx, cudaEventRecord(b->done, st), "record");
-    if (s) {
-        delete b;
-        return s;
-    }
+    b->seq = ++ctx->submit_seq;
+    s = finish_batch(ctx, b);
+    if (s) return s;
     *ticket = b;
     return EXCL_OK;
 }
 
-// excl_submit_into: the inputs are copied from the caller's host arrays on the
-// context's stream (asynchronously when they are page-locked) and the scatter
-// kernel writes offsets and docIDs through the device mapping of the caller's
-// page-locked output arrays, so the results cross PCIe while the last kernel
-// runs and excl_wait has nothing left to copy. The batch's error word is
-// copied to its own pinned slot and the device word cleared behind it, so
-// batches in flight together each see their own flags.
 extern "C" int excl_ctx_set_tuning(excl_ctx *ctx, const excl_tune_report *rep) {
     if (!ctx || !rep) return EXCL_E_INVALID;
+    std::lock_guard<std::recursive_mutex> g(ctx->op_mu);
     if (rep->algo > EXCL_ALGO_LEARNED || (rep->warps_per_cta != 4 && rep->warps_per_cta != 8) ||
         rep->ctas_per_sm < 4 || rep->ctas_per_sm > 6 || rep->tile_split > 2 ||
         (rep->merge_segs != EXCL_MERGE_OFF && (rep->merge_segs == 0 || rep->merge_segs > 4)))
@@ -781,12 +811,18 @@ extern "C" int excl_ctx_set_tuning(excl_ctx *ctx, const excl_tune_report *rep) {
     return EXCL_OK;
 }
 
+// excl_submit_into: the inputs are copied from the caller's host arrays on the
+// context's stream (asynchronously when they are page-locked) and the scatter
+// kernel writes offsets and docIDs through the device mapping of the caller's
+// page-locked output arrays, so the results cross PCIe while the last kernel
+// runs and excl_wait has nothing left to copy.
 extern "C" int excl_submit_into(excl_ctx *ctx, excl_index *ix, const uint32_t *terms, const uint32_t *term_offsets,
                                 uint32_t nq, uint32_t algo, uint32_t *offsets, uint32_t *docids, uint64_t cap,
                                 excl_batch **ticket) {
     if (!ctx || !ix || !term_offsets || !offsets || !ticket || (!docids && cap) || (!terms && term_offsets[nq]))
         return EXCL_E_INVALID;
     *ticket = nullptr;
+    std::lock_guard<std::recursive_mutex> g(ctx->op_mu);
     if (nq > ctx->cfg.max_queries) {
         ctx_error(ctx, "batch of %u queries exceeds max_queries %u", nq, ctx->cfg.max_queries);
         return EXCL_E_CAPACITY;
@@ -813,7 +849,7 @@ extern "C" int excl_submit_into(excl_ctx *ctx, excl_index *ix, const uint32_t *t
         (i ? m_docids : m_offsets) = static_cast<uint32_t *>(a.devicePointer);
     }
     if (ctx->free_flag_slots.empty()) {
-        ctx_error(ctx, "more than %u excl_submit_into batches in flight", kFlagSlots);
+        ctx_error(ctx, "more than %u batches in flight", kFlagSlots);
         return EXCL_E_CAPACITY;
     }
     cudaStream_t st = ctx->stream;
@@ -830,21 +866,8 @@ extern "C" int excl_submit_into(excl_ctx *ctx, excl_index *ix, const uint32_t *t
     excl_batch *b = new (std::nothrow) excl_batch{ctx, nq, nullptr, false};
     if (!b) return EXCL_E_NOMEM;
     b->into_offsets = offsets;
-    b->slot = (int32_t)ctx->free_flag_slots.back();
-    uint32_t *hf = ctx->h_flags + b->slot;
-    *hf = 0;
-    s = cuda_status(ctx, cudaMemcpyAsync(hf, ctx->d_misc + kMiscErr, 4, cudaMemcpyDeviceToHost, st), "d2h flags");
-    if (!s) s = cuda_status(ctx, cudaMemsetAsync(ctx->d_misc + kMiscErr, 0, 4, st), "clear flags");
-    if (!s) s = cuda_status(ctx, cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming), "event");
-    if (!s) s = cuda_status(ctx, cudaEventRecord(b->done, st), "record");
-    if (s) {
-        // the slot is not handed out: the copies above may still land in it
-        if (b->done) cudaEventDestroy(b->done);
-        cudaStreamSynchronize(st);
-        delete b;
-        return s;
-    }
-    ctx->free_flag_slots.pop_back();
+    s = finish_batch(ctx, b);
+    if (s) return s;
     *ticket = b;
     return EXCL_OK;
 }
@@ -870,20 +893,22 @@ extern "C" int excl_wait(excl_batch *b, uint32_t *offsets, uint32_t *docids, siz
     if (!b) return EXCL_E_INVALID;
     excl_ctx *ctx = b->ctx;
     cudaSetDevice(ctx->device);
-    if (b->slot >= 0) {
+    if (b->into_offsets && (offsets || docids)) return EXCL_E_INVALID;
+    int s = b->waited ? EXCL_OK : wait_event(ctx, b->done, timeout_ms);
+    if (s) return s;
+    b->waited = true;
+    s = flags_status(ctx, ctx->h_flags[b->slot]);
+    if (b->into_offsets) {
         // excl_submit_into batch: the results are already in the caller's arrays
-        if (offsets || docids) return EXCL_E_INVALID;
-        int s = b->waited ? EXCL_OK : wait_event(ctx, b->done, timeout_ms);
-        if (s) return s;
-        b->waited = true;
-        s = flags_status(ctx, ctx->h_flags[b->slot]);
         if (total) *total = b->into_offsets[b->nq];
         return s;
     }
-    int s = wait_event(ctx, b->done, timeout_ms);
     if (s) return s;
-    s = read_device_flags(ctx);
-    if (s) return s;
+    std::lock_guard<std::recursive_mutex> g(ctx->op_mu);
+    if (b->seq != ctx->submit_seq) {
+        ctx_error(ctx, "a later excl_submit on this context replaced this batch's results");
+        return EXCL_E_INVALID;
+    }
     const uint32_t tot = ctx->h_offsets[b->nq];
     if (total) *total = tot;
     if (offsets) std::memcpy(offsets, ctx->h_offsets, ((size_t)b->nq + 1) * 4);
@@ -922,6 +947,7 @@ extern "C" int excl_batch_free(excl_batch *b) {
     if (b->slot >= 0) {
         // a slot returns to the pool only once its batch's copies have landed
         if (!b->waited) cudaEventSynchronize(b->done);
+        std::lock_guard<std::recursive_mutex> g(b->ctx->op_mu);
         b->ctx->free_flag_slots.push_back((uint32_t)b->slot);
     }
     if (b->done) cudaEventDestroy(b->done);
@@ -931,6 +957,7 @@ extern "C" int excl_batch_free(excl_batch *b) {
 
 extern "C" int excl_last_stats(excl_ctx *ctx, excl_batch_stats *stt) {
     if (!ctx || !stt) return EXCL_E_INVALID;
+    std::lock_guard<std::recursive_mutex> g(ctx->op_mu);
     cudaSetDevice(ctx->device);
     int s = cuda_status(ctx, cudaStreamSynchronize(ctx->stream), "sync");
     if (s) return s;

@@ -67,9 +67,14 @@ struct excl_ctx {
     uint32_t *d_offsets = nullptr, *d_docids = nullptr;
     uint64_t docids_cap = 0;
     uint32_t *h_terms = nullptr, *h_toff = nullptr, *h_offsets = nullptr;
-    // error word of each excl_submit_into batch in flight (pinned; a slot per batch)
+    // error word of each batch in flight (pinned; a slot per batch)
     uint32_t *h_flags = nullptr;
     std::vector<uint32_t> free_flag_slots;
+    // Entry points that use the context's stream, buffers or settings hold
+    // this lock, so host threads may share a context; excl_wait holds it only
+    // to copy an excl_submit batch's results, never while waiting.
+    std::recursive_mutex op_mu;
+    uint64_t submit_seq = 0;  // excl_submit batches so far (their results share the context's buffers)
 };
 
 namespace excl {

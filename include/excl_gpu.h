@@ -222,6 +222,13 @@ int excl_decode_lists(excl_ctx *ctx, excl_index *ix, uint32_t l0, uint32_t l1, u
  * concatenated per-query docIDs, each query sorted ascending. The output is
  * identical whatever the batching. */
 typedef struct excl_batch excl_batch;
+/* Threads: host threads may share a context. Calls that use its stream,
+ * buffers or settings are serialised by the context; excl_wait does not hold
+ * it while waiting. An excl_submit batch's results live in the context's
+ * buffers until the next excl_submit on it, and waiting on the older batch
+ * then returns EXCL_E_INVALID; excl_submit_into batches write to their own
+ * arrays and may be waited on in any order. Up to 256 batches of either kind
+ * may be in flight on one context. */
 
 int excl_submit(excl_ctx *ctx, excl_index *ix, const uint32_t *terms, const uint32_t *term_offsets, uint32_t nq,
                 uint32_t algo, excl_batch **ticket);

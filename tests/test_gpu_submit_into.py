@@ -119,3 +119,56 @@ def test_capacity_and_rejected_outputs(corpus, expected):
     finally:
         ix.close()
         ctx.close()
+
+
+def test_threads_share_a_context(corpus, expected):
+    """Four host threads submit zero-copy batches on one context at once; each
+    gets its own results. An excl_submit batch superseded by a later one is
+    refused rather than answered with the later batch's results."""
+    import threading
+
+    ctx = ex.Context(0, max_queries=8192, max_keys=1 << 23)
+    ix = ex.Index(corpus.docs, corpus.list_offsets, codec="seglrc", block=256)
+    ctx.upload(ix)
+    eoffs, edocs = expected
+    toff = corpus.term_offsets
+    errors = []
+
+    def worker(k):
+        try:
+            rng = np.random.default_rng(k)
+            for _ in range(6):
+                q0 = int(rng.integers(0, corpus.nq - 50))
+                q1 = q0 + int(rng.integers(1, 50))
+                t = _pinned_copy(corpus.terms[toff[q0]:toff[q1]])
+                o = _pinned_copy((toff[q0:q1 + 1] - toff[q0]).astype(np.uint32))
+                ob = ex.pinned_empty(q1 - q0 + 1)
+                db = ex.pinned_empty(int(eoffs[q1] - eoffs[q0]) + 1)
+                b = ctx.submit_into(ix, t, o, ob, db, "hashseg")
+                tot = b.wait()
+                b.free()
+                assert np.array_equal(ob.astype(np.uint64), eoffs[q0:q1 + 1] - eoffs[q0])
+                assert np.array_equal(db[:tot], edocs[eoffs[q0]:eoffs[q1]])
+        except Exception as e:  # reported below
+            errors.append(e)
+
+    try:
+        th = [threading.Thread(target=worker, args=(k,)) for k in range(4)]
+        for x in th:
+            x.start()
+        for x in th:
+            x.join()
+        assert not errors, errors
+        # excl_submit: the older batch's results were replaced by the newer one's
+        b1 = ctx.submit(ix, corpus.terms[:int(toff[10])], toff[:11], "hashseg")
+        b2 = ctx.submit(ix, corpus.terms[:int(toff[20])], toff[:21], "hashseg")
+        with pytest.raises(ex.ExclError) as e:
+            b1.wait()
+        assert e.value.status == ex.api.E_INVALID
+        offs, docs = b2.wait()
+        assert np.array_equal(docs, edocs[:int(eoffs[20])])
+        b1.free()
+        b2.free()
+    finally:
+        ix.close()
+        ctx.close()
