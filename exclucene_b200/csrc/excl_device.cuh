@@ -352,7 +352,19 @@ __device__ __forceinline__ int last_head_le(const uint32_t *head, uint32_t lo, u
 }
 
 // Last segment in [lo, hi) of a list's probe records whose head <= key, or lo - 1.
+// Ranges of up to four records (the directory's usual one or two) load every
+// head at once, one round trip instead of a chain of dependent loads.
 __device__ __forceinline__ int last_head_le_rec(const ProbeRec *pr, uint32_t lo, uint32_t hi, uint32_t key) {
+    if (hi - lo <= 4u && lo < hi) {
+        uint32_t h[4];
+#pragma unroll
+        for (uint32_t j = 0; j < 4; ++j) h[j] = lo + j < hi ? __ldg(&pr[lo + j].head) : 0xffffffffu;
+        int s = (int)lo - 1;
+#pragma unroll
+        for (uint32_t j = 0; j < 4; ++j)
+            if (lo + j < hi && h[j] <= key) s = (int)(lo + j);
+        return s;
+    }
     while (lo < hi) {
         const uint32_t mid = (lo + hi) >> 1;
         if (__ldg(&pr[mid].head) <= key) lo = mid + 1;
