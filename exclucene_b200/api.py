@@ -128,8 +128,8 @@ _submit = _sig("excl_submit", C.c_int, C.c_void_p, C.c_void_p, u32p, u32p, C.c_u
                C.POINTER(C.c_void_p))
 _wait = _sig("excl_wait", C.c_int, C.c_void_p, u32p, u32p, C.c_size_t, C.c_int, u64p)
 _bfree = _sig("excl_batch_free", C.c_int, C.c_void_p)
-_submit_into = _sig("excl_submit_into", C.c_int, C.c_void_p, C.c_void_p, u32p, u32p, C.c_uint32, C.c_uint32, u32p,
-                    u32p, C.c_uint64, C.POINTER(C.c_void_p))
+_submit_into = _sig("excl_submit_into", C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
+                    C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint64, C.POINTER(C.c_void_p))
 _halloc = _sig("excl_host_alloc", C.c_int, C.c_size_t, C.POINTER(C.c_void_p))
 _hfree = _sig("excl_host_free", C.c_int, C.c_void_p)
 _isect_dev = _sig("excl_intersect_device", C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
@@ -414,8 +414,10 @@ class Context:
             raise ExclError(E_INVALID, "excl_submit_into: offsets holds fewer than nq+1 entries")
         a = ALGO_NAMES[algo] if isinstance(algo, str) else int(algo)
         b = C.c_void_p()
-        _check_status(_submit_into(self._h, ix._h, _p32(terms), _p32(term_offsets), nq, a, _p32(offsets),
-                                   _p32(docids), len(docids), C.byref(b)), self, "excl_submit_into")
+        st = _submit_into(self._h, ix._h, terms.ctypes.data, term_offsets.ctypes.data, nq, a, offsets.ctypes.data,
+                          docids.ctypes.data, len(docids), C.byref(b))
+        if st != OK:
+            _check_status(st, self, "excl_submit_into")
         return Batch(self, b, nq, into=(terms, term_offsets, offsets, docids))
 
     def intersect(self, ix: Index, terms, term_offsets, algo="auto") -> tuple[np.ndarray, np.ndarray]:

@@ -24,6 +24,7 @@ struct BatchView {
     uint32_t tile_split;         // fixed-block shortest lists: each segment is cut into 2^tile_split tiles
     uint64_t max_keys;
     uint32_t *err;               // error flag bits
+    uint32_t *err_out;           // or null: device-mapped host word that receives this batch's error bits at its end (the device word is cleared)
     uint64_t *stats;             // [probes, fallbacks] or null
 };
 

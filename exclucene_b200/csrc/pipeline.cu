@@ -108,8 +108,9 @@ __device__ __forceinline__ void block_scan2(uint32_t a, uint32_t b, uint32_t &ea
 // ---------------------------------------------------------------------------
 
 __global__ void __launch_bounds__(kPackThreads) k_pack_scan(const ListDesc *__restrict__ lists, uint32_t nlists,
-                                                            const uint32_t *__restrict__ terms,
-                                                            const uint32_t *__restrict__ toff, uint32_t nq,
+                                                            const uint32_t *terms,  // device or host-mapped:
+                                                            const uint32_t *toff,   // coherent loads only
+                                                            uint32_t nq,
                                                             BatchView b, PackSync *__restrict__ sync) {
     __shared__ uint32_t sa[33], sb[33], s_pre[2], s_et[kPackThreads], s_id, s_tag;
     if (threadIdx.x == 0) {
@@ -133,7 +134,7 @@ __global__ void __launch_bounds__(kPackThreads) k_pack_scan(const ListDesc *__re
             uint32_t id[kPackRegTerms], len[kPackRegTerms], ntl[kPackRegTerms];
             bool bad = false;
 #pragma unroll
-            for (uint32_t j = 0; j < kPackRegTerms; ++j) id[j] = j < k ? __ldg(terms + t0 + j) : 0u;
+            for (uint32_t j = 0; j < kPackRegTerms; ++j) id[j] = j < k ? terms[t0 + j] : 0u;
 #pragma unroll
             for (uint32_t j = 0; j < kPackRegTerms; ++j) {
                 const bool v = j < k && id[j] < nlists;
@@ -169,7 +170,7 @@ __global__ void __launch_bounds__(kPackThreads) k_pack_scan(const ListDesc *__re
             for (uint32_t i0 = 0; i0 < k; i0 += 4) {
 #pragma unroll
                 for (uint32_t j = 0; j < 4; ++j)
-                    if (i0 + j < k) id[i0 + j] = __ldg(terms + t0 + i0 + j);
+                    if (i0 + j < k) id[i0 + j] = terms[t0 + i0 + j];
             }
             for (uint32_t i0 = 0; i0 < k; i0 += 4) {
 #pragma unroll
@@ -331,6 +332,14 @@ __device__ __forceinline__ void warp_lower_bound2(const uint32_t *a, uint32_t n,
 // published. Phase B (every warp of the grid, once all chunk tickets are
 // taken, so every chunk is owned by a running CTA): survivors copied tile by
 // tile, each tile after its chunk's prefix is out.
+// The batch's error bits to the host word the batch names (the device word is
+// cleared for the next batch); nothing when it names none.
+__device__ __forceinline__ void hand_over_flags(const BatchView &b) {
+    if (!b.err_out) return;
+    *(volatile uint32_t *)b.err_out = atomicExch(b.err, 0u);
+    __threadfence_system();
+}
+
 __global__ void __launch_bounds__(kSSThreads) k_scatter(BatchView b, PackSync *__restrict__ sync,
                                                         uint64_t *__restrict__ chunk_state,
                                                         uint32_t *__restrict__ offsets,
@@ -348,6 +357,7 @@ __global__ void __launch_bounds__(kSSThreads) k_scatter(BatchView b, PackSync *_
     uint32_t *tile_out = b.tile_q;
     if (nch == 0) {  // no tiles in the batch: every offset is 0, no ticket taken
         for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q <= nq; q += gridDim.x * blockDim.x) offsets[q] = 0u;
+        if (blockIdx.x == 0 && threadIdx.x == 0) hand_over_flags(b);  // the earlier kernels' bits
         return;
     }
     for (;;) {
@@ -459,14 +469,16 @@ __global__ void __launch_bounds__(kSSThreads) k_scatter(BatchView b, PackSync *_
             if (k < n && o + k < cap) docids[o + k] = v[i];
         }
     }
-    // the last CTA out resets the chunk ticket
-    if (threadIdx.x == 0) {
+    // the last CTA out resets the chunk ticket and hands the batch's error
+    // bits (set by this and the earlier kernels of the batch) to the host;
+    // every thread's writes are fenced before its CTA counts itself done
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0 && atomicAdd(&sync->sdone, 1u) == gridDim.x - 1) {
+        sync->sticket = 0u;
+        sync->sdone = 0u;
+        hand_over_flags(b);
         __threadfence();
-        if (atomicAdd(&sync->sdone, 1u) == gridDim.x - 1) {
-            sync->sticket = 0u;
-            sync->sdone = 0u;
-            __threadfence();
-        }
     }
 }
 

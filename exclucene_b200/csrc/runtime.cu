@@ -240,7 +240,8 @@ int ctx_alloc_batch(excl_ctx *ctx) {
     st |= cuda_status(ctx, cudaMallocHost((void **)&ctx->h_terms, (size_t)c.max_queries * kMaxTerms * 4), "pinned");
     st |= cuda_status(ctx, cudaMallocHost((void **)&ctx->h_toff, ((size_t)c.max_queries + 1) * 4), "pinned");
     st |= cuda_status(ctx, cudaMallocHost((void **)&ctx->h_offsets, ((size_t)c.max_queries + 1) * 4), "pinned");
-    st |= cuda_status(ctx, cudaMallocHost((void **)&ctx->h_flags, kFlagSlots * 4), "pinned");
+    st |= cuda_status(ctx, cudaHostAlloc((void **)&ctx->h_flags, kFlagSlots * 4, cudaHostAllocMapped), "pinned");
+    if (!st) st |= cuda_status(ctx, cudaHostGetDevicePointer((void **)&ctx->m_flags, ctx->h_flags, 0), "mapped flags");
     if (st) return EXCL_E_NOMEM;
     for (uint32_t i = kFlagSlots; i-- > 0;) ctx->free_flag_slots.push_back(i);
     cudaMemsetAsync(ctx->d_misc, 0, 16 * 4, ctx->stream);
@@ -252,7 +253,7 @@ int ctx_alloc_batch(excl_ctx *ctx) {
 
 // Runs the whole device pipeline for nq queries whose terms are in device memory.
 int run_pipeline(excl_ctx *ctx, excl_index *ix, const uint32_t *d_terms, const uint32_t *d_toff, uint32_t nq,
-                 uint32_t algo, uint32_t *d_offsets, uint32_t *d_docids, uint64_t cap) {
+                 uint32_t algo, uint32_t *d_offsets, uint32_t *d_docids, uint64_t cap, uint32_t *err_out) {
     if (!ix->dev) {
         ctx_error(ctx, "index not uploaded");
         return EXCL_E_INVALID;
@@ -283,6 +284,7 @@ int run_pipeline(excl_ctx *ctx, excl_index *ix, const uint32_t *d_terms, const u
     b.tile_split = ctx->tile_split;
     b.max_keys = ctx->cfg.max_keys;
     b.err = ctx->d_misc + kMiscErr;
+    b.err_out = err_out;
     b.stats = ctx->collect_stats ? ctx->d_stats : nullptr;
     BatchLaunch L{};
     L.ixv = ix->dev->view(ix->models ? model_view(ix->models) : ModelView{});
@@ -308,12 +310,13 @@ int run_pipeline(excl_ctx *ctx, excl_index *ix, const uint32_t *d_terms, const u
         uint64_t vh = 1469598103934665603ull;
         const unsigned char *vb = reinterpret_cast<const unsigned char *>(&L.ixv);
         for (size_t i = 0; i < sizeof L.ixv; ++i) vh = (vh ^ vb[i]) * 1099511628211ull;
-        const uint64_t key[10] = {(uint64_t)(uintptr_t)ix, vh, (uint64_t)(uintptr_t)d_terms,
+        const uint64_t key[11] = {(uint64_t)(uintptr_t)ix, vh, (uint64_t)(uintptr_t)d_terms,
                                   (uint64_t)(uintptr_t)d_toff, nq, algo, (uint64_t)(uintptr_t)d_offsets,
                                   (uint64_t)(uintptr_t)d_docids, cap,
                                   (uint64_t)ctx->collect_stats | (uint64_t)ctx->merge_segs << 8 |
                                       (uint64_t)ctx->warps << 16 | (uint64_t)ctx->ctas_per_sm << 32 |
-                                      (uint64_t)ctx->tile_split << 40};
+                                      (uint64_t)ctx->tile_split << 40,
+                                  (uint64_t)(uintptr_t)err_out};
         const bool same = ctx->gkey_seen && std::memcmp(key, ctx->gkey, sizeof key) == 0;
         if (same || ctx->gexec) {
             if (!same || !ctx->gexec) {
@@ -428,6 +431,8 @@ extern "C" int excl_ctx_destroy(excl_ctx *ctx) {
     cudaFreeHost(ctx->h_toff);
     cudaFreeHost(ctx->h_offsets);
     cudaFreeHost(ctx->h_flags);
+    for (cudaEvent_t &e : ctx->slot_ev)
+        if (e) cudaEventDestroy(e);
     for (auto &e : ctx->ev)
         if (e) cudaEventDestroy(e);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -602,42 +607,50 @@ extern "C" int excl_ctx_check(excl_ctx *ctx) {
 struct excl_batch {
     excl_ctx *ctx;
     uint32_t nq;
-    cudaEvent_t done;
+    cudaEvent_t done;  // the slot's event (owned by the context)
     bool waited;
     const uint32_t *into_offsets = nullptr;  // excl_submit_into: the caller's offsets array
-    int32_t slot = -1;                       // this batch's error-word slot in ctx->h_flags
+    int32_t slot = -1;                       // this batch's slot: error word in ctx->h_flags, event
     uint64_t seq = 0;                        // excl_submit: its number among the context's excl_submit batches
 };
 
-// Ends a batch's stream work: its error word is copied to a pinned slot of
-// its own and the device word cleared behind it (so batches in flight
-// together each see their own flags), then its completion event is recorded.
-// The caller holds ctx->op_mu. On failure the batch is deleted.
-static int finish_batch(excl_ctx *ctx, excl_batch *b) {
+// A free batch slot (its pinned error word cleared), or -1 with the context's
+// error set. The caller holds ctx->op_mu.
+static int32_t take_slot(excl_ctx *ctx) {
     using namespace excl;
     if (ctx->free_flag_slots.empty()) {
         ctx_error(ctx, "more than %u batches in flight", kFlagSlots);
-        cudaStreamSynchronize(ctx->stream);
-        delete b;
-        return EXCL_E_CAPACITY;
+        return -1;
     }
-    cudaStream_t st = ctx->stream;
     const uint32_t slot = ctx->free_flag_slots.back();
-    uint32_t *hf = ctx->h_flags + slot;
-    *hf = 0;
-    int s = cuda_status(ctx, cudaMemcpyAsync(hf, ctx->d_misc + kMiscErr, 4, cudaMemcpyDeviceToHost, st), "d2h flags");
-    if (!s) s = cuda_status(ctx, cudaMemsetAsync(ctx->d_misc + kMiscErr, 0, 4, st), "clear flags");
-    if (!s) s = cuda_status(ctx, cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming), "event");
-    if (!s) s = cuda_status(ctx, cudaEventRecord(b->done, st), "record");
-    if (s) {
-        // the slot is not handed out: the copies above may still land in it
-        if (b->done) cudaEventDestroy(b->done);
-        cudaStreamSynchronize(st);
-        delete b;
-        return s;
+    if (!ctx->slot_ev[slot] && cudaEventCreateWithFlags(&ctx->slot_ev[slot], cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        ctx->slot_ev[slot] = nullptr;
+        ctx_error(ctx, "event");
+        return -1;
     }
     ctx->free_flag_slots.pop_back();
-    b->slot = (int32_t)slot;
+    ctx->h_flags[slot] = 0;
+    return (int32_t)slot;
+}
+
+// Ends a batch whose pipeline ran with err_out = the slot's mapped word (the
+// scatter kernel hands the batch's error bits to it and clears the device
+// word, so batches in flight together each see their own flags): records the
+// slot's event and hands the batch out. On failure the slot is returned.
+static int finish_batch(excl_ctx *ctx, uint32_t nq, int32_t slot, const uint32_t *into_offsets, excl_batch **ticket) {
+    using namespace excl;
+    excl_batch *b = new (std::nothrow) excl_batch{ctx, nq, ctx->slot_ev[slot], false};
+    int s = b ? cuda_status(ctx, cudaEventRecord(ctx->slot_ev[slot], ctx->stream), "record") : EXCL_E_NOMEM;
+    if (s) {
+        delete b;
+        cudaStreamSynchronize(ctx->stream);  // the batch's kernels may still write the slot
+        ctx->free_flag_slots.push_back((uint32_t)slot);
+        return s;
+    }
+    b->slot = slot;
+    b->into_offsets = into_offsets;
+    *ticket = b;
     return EXCL_OK;
 }
 
@@ -781,19 +794,23 @@ extern "C" int excl_submit(excl_ctx *ctx, excl_index *ix, const uint32_t *terms,
     std::lock_guard<std::recursive_mutex> g(ctx->op_mu);
     cudaStream_t st = ctx->stream;
     int s = stage_host_batch(ctx, ix, terms, term_offsets, nq, nullptr);
-    if (!s) s = run_pipeline(ctx, ix, ctx->d_terms, ctx->d_toff, nq, algo, ctx->d_offsets, ctx->d_docids, ctx->docids_cap);
+    if (s) return s;
+    const int32_t slot = take_slot(ctx);
+    if (slot < 0) return EXCL_E_CAPACITY;
+    s = run_pipeline(ctx, ix, ctx->d_terms, ctx->d_toff, nq, algo, ctx->d_offsets, ctx->d_docids, ctx->docids_cap,
+                     ctx->m_flags + slot);
     if (!s)
         s = cuda_status(ctx, cudaMemcpyAsync(ctx->h_offsets, ctx->d_offsets, ((size_t)nq + 1) * 4,
                                              cudaMemcpyDeviceToHost, st),
                         "d2h offsets");
-    if (s) return s;
-    excl_batch *b = new (std::nothrow) excl_batch{ctx, nq, nullptr, false};
-    if (!b) return EXCL_E_NOMEM;
-    b->seq = ++ctx->submit_seq;
-    s = finish_batch(ctx, b);
-    if (s) return s;
-    *ticket = b;
-    return EXCL_OK;
+    if (s) {
+        cudaStreamSynchronize(st);
+        ctx->free_flag_slots.push_back((uint32_t)slot);
+        return s;
+    }
+    s = finish_batch(ctx, nq, slot, nullptr, ticket);
+    if (!s) (*ticket)->seq = ++ctx->submit_seq;
+    return s;
 }
 
 extern "C" int excl_ctx_set_tuning(excl_ctx *ctx, const excl_tune_report *rep) {
@@ -836,40 +853,48 @@ extern "C" int excl_submit_into(excl_ctx *ctx, excl_index *ix, const uint32_t *t
         return EXCL_E_CAPACITY;
     }
     cudaSetDevice(ctx->device);
-    uint32_t *m_offsets = nullptr, *m_docids = nullptr;
-    for (int i = 0; i < 2; ++i) {
-        void *h = i ? (void *)docids : (void *)offsets;
-        if (!h) continue;
+    // device addresses of the caller's arrays: the outputs must be
+    // page-locked and mapped; page-locked inputs are read in place by the pack
+    // kernel, others are copied to the context's buffers first
+    uint32_t *mapped[4] = {nullptr, nullptr, nullptr, nullptr};
+    const void *host[4] = {offsets, docids, terms, term_offsets};
+    for (int i = 0; i < 4; ++i) {
+        if (!host[i]) continue;
         cudaPointerAttributes a{};
-        if (cudaPointerGetAttributes(&a, h) != cudaSuccess || a.type != cudaMemoryTypeHost || !a.devicePointer) {
+        if (cudaPointerGetAttributes(&a, host[i]) == cudaSuccess && a.type == cudaMemoryTypeHost && a.devicePointer)
+            mapped[i] = static_cast<uint32_t *>(a.devicePointer);
+        else
             cudaGetLastError();
+        if (i < 2 && !mapped[i]) {
             ctx_error(ctx, "%s array is not page-locked, device-mapped host memory", i ? "docids" : "offsets");
             return EXCL_E_INVALID;
         }
-        (i ? m_docids : m_offsets) = static_cast<uint32_t *>(a.devicePointer);
-    }
-    if (ctx->free_flag_slots.empty()) {
-        ctx_error(ctx, "more than %u batches in flight", kFlagSlots);
-        return EXCL_E_CAPACITY;
     }
     cudaStream_t st = ctx->stream;
     int s = EXCL_OK;
-    if (nterms)
+    const uint32_t *q_terms = mapped[2], *q_toff = mapped[3];
+    if (!q_terms && nterms) {
         s = cuda_status(ctx, cudaMemcpyAsync(ctx->d_terms, terms, (size_t)nterms * 4, cudaMemcpyHostToDevice, st),
                         "h2d terms");
-    if (!s)
+        q_terms = ctx->d_terms;
+    }
+    if (!q_terms) q_terms = ctx->d_terms;  // no terms: never read
+    if (!s && !q_toff) {
         s = cuda_status(ctx, cudaMemcpyAsync(ctx->d_toff, term_offsets, ((size_t)nq + 1) * 4, cudaMemcpyHostToDevice,
                                              st),
                         "h2d term offsets");
-    if (!s) s = run_pipeline(ctx, ix, ctx->d_terms, ctx->d_toff, nq, algo, m_offsets, m_docids, cap);
+        q_toff = ctx->d_toff;
+    }
     if (s) return s;
-    excl_batch *b = new (std::nothrow) excl_batch{ctx, nq, nullptr, false};
-    if (!b) return EXCL_E_NOMEM;
-    b->into_offsets = offsets;
-    s = finish_batch(ctx, b);
-    if (s) return s;
-    *ticket = b;
-    return EXCL_OK;
+    const int32_t slot = take_slot(ctx);
+    if (slot < 0) return EXCL_E_CAPACITY;
+    s = run_pipeline(ctx, ix, q_terms, q_toff, nq, algo, mapped[0], mapped[1], cap, ctx->m_flags + slot);
+    if (s) {
+        cudaStreamSynchronize(st);
+        ctx->free_flag_slots.push_back((uint32_t)slot);
+        return s;
+    }
+    return finish_batch(ctx, nq, slot, offsets, ticket);
 }
 
 // Polls the batch's event: spins for the first 2 ms (a batch usually ends
@@ -945,12 +970,11 @@ extern "C" int excl_host_free(void *p) {
 extern "C" int excl_batch_free(excl_batch *b) {
     if (!b) return EXCL_E_INVALID;
     if (b->slot >= 0) {
-        // a slot returns to the pool only once its batch's copies have landed
+        // a slot returns to the pool only once its batch's writes have landed
         if (!b->waited) cudaEventSynchronize(b->done);
         std::lock_guard<std::recursive_mutex> g(b->ctx->op_mu);
         b->ctx->free_flag_slots.push_back((uint32_t)b->slot);
     }
-    if (b->done) cudaEventDestroy(b->done);
     delete b;
     return EXCL_OK;
 }

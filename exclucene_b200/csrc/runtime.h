@@ -49,7 +49,7 @@ struct excl_ctx {
     // CUDA graph of the last batch launched through excl_intersect_device
     bool use_graphs = false, last_was_graph = false;
     cudaGraphExec_t gexec = nullptr;
-    uint64_t gkey[10] = {};
+    uint64_t gkey[11] = {};
     bool gkey_seen = false;  // the key ran once uncaptured (first sighting)
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -67,8 +67,10 @@ struct excl_ctx {
     uint32_t *d_offsets = nullptr, *d_docids = nullptr;
     uint64_t docids_cap = 0;
     uint32_t *h_terms = nullptr, *h_toff = nullptr, *h_offsets = nullptr;
-    // error word of each batch in flight (pinned; a slot per batch)
-    uint32_t *h_flags = nullptr;
+    // error word of each batch in flight (pinned, device-mapped: the scatter
+    // kernel writes it) and the event that marks the batch done, a slot per batch
+    uint32_t *h_flags = nullptr, *m_flags = nullptr;
+    cudaEvent_t slot_ev[excl::kFlagSlots] = {};
     std::vector<uint32_t> free_flag_slots;
     // Entry points that use the context's stream, buffers or settings hold
     // this lock, so host threads may share a context; excl_wait holds it only
@@ -83,7 +85,7 @@ int cuda_status(excl_ctx *ctx, cudaError_t e, const char *what);
 int read_device_flags(excl_ctx *ctx);
 int flags_status(excl_ctx *ctx, uint32_t f);
 int run_pipeline(excl_ctx *ctx, excl_index *ix, const uint32_t *d_terms, const uint32_t *d_toff, uint32_t nq,
-                 uint32_t algo, uint32_t *d_offsets, uint32_t *d_docids, uint64_t cap);
+                 uint32_t algo, uint32_t *d_offsets, uint32_t *d_docids, uint64_t cap, uint32_t *err_out = nullptr);
 
 // learned.cu
 ModelView model_view(const ModelSet *m);
