@@ -46,12 +46,13 @@ using Clock = std::chrono::steady_clock;
 
 constexpr uint64_t up256(uint64_t b) { return (b + 255) & ~255ull; }
 
-// Byte layout of one batch's block of the pool.
+// Byte layout of one batch's block of the pool (the queries themselves stay
+// in the slot's mapped host arrays).
 struct WsLayout {
-    uint64_t terms, toff, qterms, qnterms, tile_prefix, key_base, tile_q, tile_count, tile_slot, scratch, total;
+    uint64_t qterms, qnterms, tile_prefix, key_base, tile_q, tile_count, tile_slot, scratch, total;
 };
 
-WsLayout ws_layout(uint64_t nq, uint64_t nterms, uint64_t tiles, uint64_t keys) {
+WsLayout ws_layout(uint64_t nq, uint64_t /*nterms*/, uint64_t tiles, uint64_t keys) {
     WsLayout L{};
     uint64_t o = 0;
     auto take = [&](uint64_t words) {
@@ -59,8 +60,6 @@ WsLayout ws_layout(uint64_t nq, uint64_t nterms, uint64_t tiles, uint64_t keys) 
         o += up256(std::max<uint64_t>(words, 1) * 4);
         return r;
     };
-    L.terms = take(nterms);
-    L.toff = take(nq + 1);
     L.qterms = take(nq * kMaxTerms);
     L.qnterms = take(nq);
     L.tile_prefix = take(nq + 2);
@@ -142,8 +141,9 @@ struct Slot {
     PackSync *d_sync = nullptr;
     uint64_t *d_chunk = nullptr;
     uint32_t *d_misc = nullptr;                      // error flag, probe work counter
-    uint32_t *h_terms = nullptr, *h_toff = nullptr;  // pinned staging
-    uint32_t *h_err = nullptr;                       // pinned copy of the error flag
+    uint32_t *h_terms = nullptr, *h_toff = nullptr;  // pinned, mapped: the pack kernel reads them in place
+    uint32_t *h_err = nullptr;                       // pinned, mapped: the batch's error bits, handed over by k_scatter
+    uint32_t *m_terms = nullptr, *m_toff = nullptr, *m_err = nullptr;  // their device addresses
     uint32_t *h_offsets = nullptr, *h_docids = nullptr;  // mapped pinned results
     uint32_t *m_offsets = nullptr, *m_docids = nullptr;  // their device addresses
     std::vector<ReqPtr> batch;
@@ -233,11 +233,9 @@ int launch_on_slot(excl_server *s, Slot *sl, uint64_t nterms, uint64_t tiles, ui
     uint8_t *base = s->d_pool + sl->pool_off;
     auto at = [&](uint64_t off) { return reinterpret_cast<uint32_t *>(base + off); };
     cudaStream_t st = sl->stream;
-    cudaError_t e = cudaMemcpyAsync(at(L.terms), sl->h_terms, (size_t)o * 4, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(at(L.toff), sl->h_toff, ((size_t)nq + 1) * 4, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(sl->d_misc, 0, 8, st);
-    if (e != cudaSuccess) return EXCL_E_CUDA;
+    // no copies: the pack kernel reads the batch's queries from the slot's
+    // mapped host arrays, k_pack_scan resets the tile counter, and k_scatter
+    // hands the error bits to h_err and clears the device word for the next batch
     BatchView b{};
     b.nq = nq;
     b.qterms = at(L.qterms);
@@ -253,13 +251,14 @@ int launch_on_slot(excl_server *s, Slot *sl, uint64_t nterms, uint64_t tiles, ui
     b.merge_segs = 2;
     b.max_keys = keys;
     b.err = sl->d_misc;
+    b.err_out = sl->m_err;
     b.stats = nullptr;
     BatchLaunch bl{};
     bl.ixv = s->ix->dev->view(s->ix->models ? model_view(s->ix->models) : ModelView{});
     bl.lists = s->ix->dev->lists;
     bl.nlists = s->ix->nlists;
-    bl.terms = at(L.terms);
-    bl.toff = at(L.toff);
+    bl.terms = sl->m_terms;
+    bl.toff = sl->m_toff;
     bl.b = b;
     bl.sync = sl->d_sync;
     bl.chunk_state = sl->d_chunk;
@@ -272,9 +271,7 @@ int launch_on_slot(excl_server *s, Slot *sl, uint64_t nterms, uint64_t tiles, ui
     bl.nsm = s->nsm;
     bl.ev = nullptr;
     if (launch_batch(bl, st)) return EXCL_E_CUDA;
-    e = cudaMemcpyAsync(sl->h_err, sl->d_misc, 4, cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaEventRecord(sl->done, st);
-    return e == cudaSuccess ? EXCL_OK : EXCL_E_CUDA;
+    return cudaEventRecord(sl->done, st) == cudaSuccess ? EXCL_OK : EXCL_E_CUDA;
 }
 
 void dispatch_loop(excl_server *s) {
@@ -514,14 +511,17 @@ extern "C" int excl_server_create(int device, excl_index *ix, const excl_server_
         ck(cudaMalloc(&sl->d_sync, sizeof(PackSync)));
         ck(cudaMalloc(&sl->d_chunk, nchunk * 8));
         ck(cudaMalloc(&sl->d_misc, 256));
-        ck(cudaHostAlloc(&sl->h_terms, (size_t)c.max_batch_queries * kMaxTerms * 4, cudaHostAllocDefault));
-        ck(cudaHostAlloc(&sl->h_toff, ((size_t)c.max_batch_queries + 1) * 4, cudaHostAllocDefault));
-        ck(cudaHostAlloc(&sl->h_err, 64, cudaHostAllocDefault));
+        ck(cudaHostAlloc(&sl->h_terms, (size_t)c.max_batch_queries * kMaxTerms * 4, cudaHostAllocMapped));
+        ck(cudaHostAlloc(&sl->h_toff, ((size_t)c.max_batch_queries + 1) * 4, cudaHostAllocMapped));
+        ck(cudaHostAlloc(&sl->h_err, 64, cudaHostAllocMapped));
         ck(cudaHostAlloc(&sl->h_offsets, ((size_t)c.max_batch_queries + 1) * 4, cudaHostAllocMapped));
         ck(cudaHostAlloc(&sl->h_docids, (size_t)c.max_batch_keys * 4, cudaHostAllocMapped));
         if (!st) {
             ck(cudaHostGetDevicePointer((void **)&sl->m_offsets, sl->h_offsets, 0));
             ck(cudaHostGetDevicePointer((void **)&sl->m_docids, sl->h_docids, 0));
+            ck(cudaHostGetDevicePointer((void **)&sl->m_terms, sl->h_terms, 0));
+            ck(cudaHostGetDevicePointer((void **)&sl->m_toff, sl->h_toff, 0));
+            ck(cudaHostGetDevicePointer((void **)&sl->m_err, sl->h_err, 0));
             ck(cudaMemset(sl->d_sync, 0, sizeof(PackSync)));
             ck(cudaMemset(sl->d_chunk, 0, nchunk * 8));
             ck(cudaMemset(sl->d_misc, 0, 256));
