@@ -3,14 +3,26 @@ compressed posting lists in ExCLucene's ParaPFD, LRC, LRCSeg, SegLRC and
 hash-segmentation formats.
 
 The work happens in libexcl_gpu.so (C ABI: include/excl_gpu.h); this package
-is its ctypes binding. Importing it without the built library raises.
+is its ctypes binding. Before the library is built only the build module
+(`python -m exclucene_b200.build`) is usable: any other name of the package
+raises ImportError, so no call can silently fall back to the CPU.
 """
-from .api import (ALGO_AUTO, ALGO_BSEARCH, ALGO_HASHSEG, ALGO_LEARNED, CODEC_HS_PARAPFD, CODEC_HS_SEGLRC, CODEC_LRC,
-                  CODEC_LRCSEG, CODEC_NEWPFD, CODEC_PARAPFD, CODEC_SEGLRC, Batch, Context, ExclError, Index, checksum,
-                  Server, encode_array_compat, library_path, newpfd_decode, newpfd_encode, parapfd_decode,
-                  parapfd_encode, pinned_empty, query_encode, query_parse)
+import os as _os
+
+_LIB = _os.path.join(_os.path.dirname(_os.path.abspath(__file__)), "libexcl_gpu.so")
 
 __all__ = ["Context", "Index", "Batch", "Server", "query_parse", "query_encode", "ExclError", "checksum", "parapfd_encode", "parapfd_decode",
            "encode_array_compat", "library_path", "CODEC_PARAPFD", "CODEC_LRC", "CODEC_LRCSEG", "CODEC_SEGLRC",
            "CODEC_HS_SEGLRC", "CODEC_HS_PARAPFD", "CODEC_NEWPFD", "newpfd_encode", "newpfd_decode", "ALGO_AUTO", "ALGO_BSEARCH", "ALGO_HASHSEG", "ALGO_LEARNED",
            "pinned_empty"]
+
+if _os.path.exists(_LIB):
+    from .api import (ALGO_AUTO, ALGO_BSEARCH, ALGO_HASHSEG, ALGO_LEARNED, CODEC_HS_PARAPFD, CODEC_HS_SEGLRC, CODEC_LRC,
+                      CODEC_LRCSEG, CODEC_NEWPFD, CODEC_PARAPFD, CODEC_SEGLRC, Batch, Context, ExclError, Index, checksum,
+                      Server, encode_array_compat, library_path, newpfd_decode, newpfd_encode, parapfd_decode,
+                      parapfd_encode, pinned_empty, query_encode, query_parse)
+else:
+    def __getattr__(name):
+        if name in __all__:
+            raise ImportError(f"{_LIB} is not built; run `python -m exclucene_b200.build`")
+        raise AttributeError(name)
