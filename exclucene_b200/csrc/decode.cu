@@ -311,12 +311,28 @@ __device__ __forceinline__ void group_resid(const uint32_t *blk, const RunMeta &
     const uint32_t count = act ? m.count : 0u;
     const uint32_t mask = (1u << h.lb) - 1u;
     uint32_t v[8];
+    if (LGT == 5) {
+        // G = 32: value t = sub + 32q starts at bit sub*lb + 32*q*lb, so its
+        // word is q*lb words past the lane's first one and its shift is the
+        // lane's own; a full block needs no bounds test
+        const uint32_t b0 = sub * h.lb, sh = b0 & 31u;
+        const uint32_t *p = lows + (b0 >> 5);
+        if (count == 8u * 32u) {
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
-        const uint32_t t = sub + G * q;
-        const uint32_t bit = t * h.lb;
-        const uint32_t wi = bit >> 5;
-        v[q] = t < count ? (__funnelshift_r(lows[wi], lows[wi + 1], bit & 31u) & mask) : 0u;
+            for (int q = 0; q < 8; ++q) v[q] = __funnelshift_r(p[q * h.lb], p[q * h.lb + 1], sh) & mask;
+        } else {
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+                v[q] = sub + 32u * q < count ? (__funnelshift_r(p[q * h.lb], p[q * h.lb + 1], sh) & mask) : 0u;
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const uint32_t t = sub + G * q;
+            const uint32_t bit = t * h.lb;
+            const uint32_t wi = bit >> 5;
+            v[q] = t < count ? (__funnelshift_r(lows[wi], lows[wi + 1], bit & 31u) & mask) : 0u;
+        }
     }
     const bool exc = count && h.en;
     if (__any_sync(0xffffffffu, exc)) {
@@ -353,13 +369,22 @@ __device__ __forceinline__ void group_resid(const uint32_t *blk, const RunMeta &
             if (t < count) o[t] = v[q] + pred_fma(i0 + t, a, b) + aux;
         }
     } else {
-        // segment-local index t < 256, exact in float
+        // segment-local index t < 256: float(sub) + G*q is exact, so one
+        // conversion per lane replaces one per value
         const float a = m.a, b = m.b;
         const uint32_t aux = m.aux;
+        const float tf = __uint2float_rn(sub);
+        if (LGT == 5 && count == 8u * 32u) {
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            const uint32_t t = sub + G * q;
-            if (t < count) o[t] = v[q] + (uint32_t)__float2int_rz(__fmaf_rn(__uint2float_rn(t), a, b)) + aux;
+            for (int q = 0; q < 8; ++q)
+                o[sub + 32u * q] = v[q] + (uint32_t)__float2int_rz(__fmaf_rn(__fadd_rn(tf, 32.0f * q), a, b)) + aux;
+        } else {
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const uint32_t t = sub + G * q;
+                const float tq = __fadd_rn(tf, (float)(G * q));
+                if (t < count) o[t] = v[q] + (uint32_t)__float2int_rz(__fmaf_rn(tq, a, b)) + aux;
+            }
         }
     }
 }
