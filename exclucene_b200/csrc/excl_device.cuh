@@ -54,7 +54,7 @@ struct DevIndexView {
     const uint32_t *seg_head;
     const SegRec *seg_rec;
     const SegReg *seg_reg;
-    const uint2 *dir;           // per list: {first segment whose head's bucket >= b, that segment's head}
+    const uint32_t *dir;
     const uint64_t *tilemap;
     const uint64_t *post_base;
     const uint32_t *seg_list;   // list of each segment
@@ -351,6 +351,28 @@ __device__ __forceinline__ int last_head_le(const uint32_t *head, uint32_t lo, u
     return (int)lo - 1;
 }
 
+// Last segment in [lo, hi) of a list's probe records whose head <= key, or lo - 1.
+// Ranges of up to four records (the directory's usual one or two) load every
+// head at once, one round trip instead of a chain of dependent loads.
+__device__ __forceinline__ int last_head_le_rec(const ProbeRec *pr, uint32_t lo, uint32_t hi, uint32_t key) {
+    if (hi - lo <= 4u && lo < hi) {
+        uint32_t h[4];
+#pragma unroll
+        for (uint32_t j = 0; j < 4; ++j) h[j] = lo + j < hi ? __ldg(&pr[lo + j].head) : 0xffffffffu;
+        int s = (int)lo - 1;
+#pragma unroll
+        for (uint32_t j = 0; j < 4; ++j)
+            if (lo + j < hi && h[j] <= key) s = (int)(lo + j);
+        return s;
+    }
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(&pr[mid].head) <= key) lo = mid + 1;
+        else hi = mid;
+    }
+    return (int)lo - 1;
+}
+
 // Serial search of `key` (head <= key) in a d-gap segment, starting at the
 // segment head or at its median (ParaPFD_Intersection_kernel.cu:383-447:
 // median halves the walk; exceptions tracked with a cursor).
@@ -463,6 +485,19 @@ __device__ __forceinline__ bool dgap_find_newpfd(const uint32_t *blk, const BlkH
         }
         v += g;
         if (v >= key) return v == key;
+    }
+    return false;
+}
+
+// Binary search for `key` over elements [t0, t1] of a residual-coded segment.
+__device__ __forceinline__ bool resid_find(const uint32_t *blk, const BlkHdr &h, const ResidParams &rp, uint32_t count,
+                                           int t0, int t1, uint32_t key) {
+    while (t0 <= t1) {
+        const int mid = (t0 + t1) >> 1;
+        const uint32_t v = resid_value(rp, (uint32_t)mid, block_value_ra(blk, h, count, (uint32_t)mid));
+        if (v == key) return true;
+        if (v < key) t0 = mid + 1;
+        else t1 = mid - 1;
     }
     return false;
 }

@@ -16,268 +16,105 @@
 namespace excl {
 
 // ---------------------------------------------------------------------------
+// Probe of one key against one longer list.
+
 __device__ __forceinline__ int64_t imax64(int64_t a, int64_t b) { return a > b ? a : b; }
 __device__ __forceinline__ int64_t imin64(int64_t a, int64_t b) { return a < b ? a : b; }
 
-// Probe of K keys of one lane against one longer list L. Each key walks a
-// chain of dependent loads: directory bucket (or learned model, or a binary
-// search over all heads) -> segment heads -> segment record (head, block
-// offset, count, base/median, descriptor, segment regression) -> block words
-// (a d-gap walk from the head or median, ParaPFD_Intersection_kernel.cu:
-// 383-447, or a binary search over random-access residuals inside the
-// regression window, SegLRC_Intersection_kernel.cu:366-393). Every stage
-// issues the loads of all K keys before using any, so K > 1 keeps K chains
-// in flight per lane. Bit k of `act`: key[k] is valid; bit k of the result:
-// key[k] is in L.
-template <int ALGO, int KIND, int K>
-__device__ __forceinline__ uint32_t probe_keys(const DevIndexView &ix, const ListDesc &L, const uint32_t (&key)[K],
-                                               uint32_t act, uint32_t &fallback) {
-#pragma unroll
-    for (int k = 0; k < K; ++k)
-        if (key[k] < L.first_doc || key[k] > L.last_doc) act &= ~(1u << k);
-    if (!act) return 0u;
-    uint32_t lo[K] = {}, hi[K] = {};
-    uint32_t plo[K] = {}, phi[K] = {};  // learned rank window (inclusive, within the list)
-    uint32_t lrn = 0;                   // bit k: key k is searched in its learned window
+template <int ALGO, int KIND>
+__device__ __forceinline__ bool probe_key(const DevIndexView &ix, const ListDesc &L, uint32_t key, uint32_t &fallback) {
+    if (key < L.first_doc || key > L.last_doc) return false;
+    uint32_t lo, hi;
+    int64_t plo = 0, phi = -1;  // learned rank window (inclusive), when used
+    bool learned = false;
     if ((ALGO == EXCL_ALGO_LEARNED || ALGO == EXCL_ALGO_AUTO) && L.model != kNoModel) {
         const ModelHdr m = ix.models.hdr[L.model];
-        const uint32_t *bd = ix.models.bnd + m.bnd_base;
-        // routing (model_route): the grid cell bounds the leaf, the leaf
-        // boundaries resolve it (last l in [lo, hi] with bnd[l] <= key)
-#pragma unroll
-        for (int k = 0; k < K; ++k)
-            if (act >> k & 1u) {
-                const uint32_t j = (key[k] - m.first) >> m.grid_shift;
-                lo[k] = ix.models.grid[m.grid_base + j];
-                hi[k] = ix.models.grid[m.grid_base + j + 1];
-            }
-        for (;;) {
-            uint32_t more = 0;
-#pragma unroll
-            for (int k = 0; k < K; ++k)
-                if (lo[k] < hi[k]) {
-                    const uint32_t mid = (lo[k] + hi[k] + 1) >> 1;
-                    if (__ldg(bd + mid) <= key[k]) lo[k] = mid;
-                    else hi[k] = mid - 1;
-                    more |= lo[k] < hi[k];
-                }
-            if (!more) break;
-        }
-        Leaf lf[K];
-#pragma unroll
-        for (int k = 0; k < K; ++k)
-            if (act >> k & 1u) lf[k] = ix.models.leaves[m.leaf_base + lo[k]];
-#pragma unroll
-        for (int k = 0; k < K; ++k) {
-            if (!(act >> k & 1u)) continue;
-            // no posting of the list routes to an empty leaf, and routing is deterministic
-            if (lf[k].ehi < lf[k].elo) {
-                act &= ~(1u << k);
-            } else if ((uint32_t)(lf[k].ehi - lf[k].elo) <= m.max_window) {
-                const int pr = model_pred_rank(lf[k], model_norm(m, key[k]));
-                const int64_t wl = imax64(0, (int64_t)pr + lf[k].elo);
-                const int64_t wh = imin64((int64_t)L.n - 1, (int64_t)pr + lf[k].ehi);
-                if (wl > wh) {
-                    act &= ~(1u << k);
-                } else {
-                    lrn |= 1u << k;
-                    plo[k] = (uint32_t)wl;
-                    phi[k] = (uint32_t)wh;
-                    lo[k] = plo[k] >> L.log2_block;
-                    hi[k] = (phi[k] >> L.log2_block) + 1u;
-                }
-            } else {
-                ++fallback;
-            }
+        const float x = model_norm(m, key);
+        const Leaf lf = ix.models.leaves[m.leaf_base + model_route(ix.models.grid, ix.models.bnd, m, key)];
+        // no posting of the list routes to an empty leaf, and routing is deterministic
+        if (lf.ehi < lf.elo) return false;
+        if ((uint32_t)(lf.ehi - lf.elo) <= m.max_window) {
+            const int pr = model_pred_rank(lf, x);
+            plo = imax64(0, (int64_t)pr + lf.elo);
+            phi = imin64((int64_t)L.n - 1, (int64_t)pr + lf.ehi);
+            if (plo > phi) return false;
+            learned = true;
+        } else {
+            ++fallback;
         }
     }
-    // segment: the last one whose head is <= key. s[k] is the best segment
-    // known so far (a head <= key), bit k of `hit` says it is one; [lo, hi)
-    // holds the candidates after it. Learned windows and BSEARCH start with
-    // no known segment; a directory entry carries the head of its segment,
-    // so the bucket's first candidate is settled by the directory load.
-    int s[K];
-    uint32_t hit = 0;
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-        s[k] = (int)lo[k] - 1;
-        if (!(act >> k & 1u)) {
-            lo[k] = hi[k] = 0;
-        } else if (!(lrn >> k & 1u)) {
-            if (ALGO == EXCL_ALGO_BSEARCH) {
-                lo[k] = 0;
-                hi[k] = L.nseg;
-                s[k] = -1;
-            } else {
-                const uint32_t b = (uint32_t)((uint64_t)key[k] >> L.dir_shift);
-                const uint2 e0 = ix.dir[L.dir_base + b], e1 = ix.dir[L.dir_base + b + 1];
-                // fixed blocks: the segment before the bucket's first may hold
-                // the key (it starts in an earlier bucket, so its head < key);
-                // HS: only the bucket's own segments
-                hi[k] = e1.x;
-                if (e0.x < e1.x && e0.y <= key[k]) {
-                    s[k] = (int)e0.x;
-                    lo[k] = e0.x + 1u;
-                    hit |= 1u << k;
-                } else {
-                    s[k] = (int)e0.x - 1;
-                    lo[k] = hi[k];
-                    if (!codec_is_hs(L.codec) && e0.x > 0) hit |= 1u << k;
-                }
-            }
+    if (learned) {
+        lo = (uint32_t)(plo >> L.log2_block);
+        hi = (uint32_t)(phi >> L.log2_block) + 1u;
+    } else if (ALGO == EXCL_ALGO_BSEARCH) {
+        lo = 0;
+        hi = L.nseg;
+    } else {
+        const uint32_t b = (uint32_t)((uint64_t)key >> L.dir_shift);
+        const uint32_t d0 = ldg(ix.dir + L.dir_base + b), d1 = ldg(ix.dir + L.dir_base + b + 1);
+        lo = codec_is_hs(L.codec) ? d0 : (d0 ? d0 - 1u : 0u);
+        hi = d1;
+    }
+    // segment search and record: the record holds the head, block offset,
+    // count, base/median, block descriptor and segment regression
+    const ProbeRec *pr = ix.seg_probe + L.seg_base;
+    const int s = (ALGO == EXCL_ALGO_BSEARCH && !learned) ? last_head_le(ix.seg_head + L.seg_base, lo, hi, key)
+                                                          : last_head_le_rec(pr, lo, hi, key);
+    if (s < (int)lo) return false;
+    const uint4 q0 = __ldg(reinterpret_cast<const uint4 *>(pr + s));
+    const uint4 q1 = __ldg(reinterpret_cast<const uint4 *>(pr + s) + 1);
+    SegRec rec;
+    rec.off = q0.y;
+    rec.aux = q0.z;
+    rec.count = q0.w;
+    const uint32_t *blk = ix.words + L.word_base + rec.off;
+    const BlkHdr h = blk_hdr(q1.x);
+    if (KIND == kKindAny && codec_is_newpfd(L.codec)) return dgap_find_newpfd(blk, h, rec.count, q0.x, rec.aux, key);
+    if (KIND == kKindDgap || (KIND == kKindAny && codec_is_dgap(L.codec)))
+        return dgap_find(blk, h, rec.count, q0.x, rec.aux, key);
+    // list position of the segment: only learned windows and the LRC/LRCSeg
+    // predictors use it, and those lists have fixed blocks
+    rec.start = (uint32_t)s << L.log2_block;
+    SegReg reg;
+    reg.a = __uint_as_float(q1.y);
+    reg.b = __uint_as_float(q1.z);
+    reg.L = q1.w & 0xffffu;
+    reg.R = q1.w >> 16;
+    const ResidParams rp = resid_params(L, rec, reg);
+    int64_t t0 = 0, t1 = (int64_t)rec.count - 1;
+    if (learned) {
+        t0 = imax64(t0, plo - rec.start);
+        t1 = imin64(t1, phi - rec.start);
+    } else if (L.codec == EXCL_CODEC_SEGLRC || L.codec == EXCL_CODEC_HS_SEGLRC || L.codec == EXCL_CODEC_LRCSEG) {
+        // Regression window (SegLRC_Intersection_kernel.cu:366-371): the pivot
+        // (key - b) / a in IEEE single precision, widened by the fit's safe
+        // range. The range was measured with this same expression on every
+        // element, so a present key always lies inside.
+        float a, bb;
+        uint32_t rl, rr;
+        int64_t off;
+        if (L.codec == EXCL_CODEC_LRCSEG) {
+            a = __uint_as_float(L.reg[0]);
+            bb = __uint_as_float(L.reg[1]);
+            rl = L.reg[2];
+            rr = L.reg[3];
+            off = rec.start;
+        } else {
+            a = reg.a;
+            bb = reg.b;
+            rl = reg.L == kProbeUnbounded ? 0x7fffffffu : reg.L;
+            rr = reg.R == kProbeUnbounded ? 0x7fffffffu : reg.R;
+            off = 0;
+        }
+        const float px = __fdiv_rn(__fsub_rn(__uint2float_rn(key), bb), a);
+        if (isfinite(px) && fabsf(px) < 2.0e9f) {
+            const int64_t P = (int64_t)__float2int_rz(px) - off;
+            t0 = imax64(t0, P - (int64_t)rl);
+            t1 = imin64(t1, P + (int64_t)rr);
         }
     }
-    // Binary search over the remaining candidates (the dense heads for
-    // BSEARCH, the records' heads otherwise) down to at most four, whose heads
-    // are then loaded at once.
-    const ProbeRec *prs = ix.seg_probe + L.seg_base;
-    const uint32_t *hb = ALGO == EXCL_ALGO_BSEARCH ? ix.seg_head + L.seg_base : &prs[0].head;
-    constexpr uint32_t hs = ALGO == EXCL_ALGO_BSEARCH ? 1u : (uint32_t)(sizeof(ProbeRec) / 4);
-    for (;;) {
-        uint32_t more = 0;
-#pragma unroll
-        for (int k = 0; k < K; ++k)
-            if (hi[k] > lo[k] + 4u) {
-                const uint32_t mid = (lo[k] + hi[k]) >> 1;
-                if (ldg(hb + (size_t)mid * hs) <= key[k]) {
-                    lo[k] = mid + 1;
-                    s[k] = (int)mid;
-                    hit |= 1u << k;
-                } else {
-                    hi[k] = mid;
-                }
-                more |= hi[k] > lo[k] + 4u;
-            }
-        if (!more) break;
-    }
-    // one candidate and none before it (a learned window inside one segment):
-    // its head is checked from its record instead of loaded first
-    uint32_t one = 0;
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-        if (hi[k] == lo[k] + 1u && !(hit >> k & 1u)) {
-            s[k] = (int)lo[k];
-            one |= 1u << k;
-            continue;
-        }
-        uint32_t h4[4];
-#pragma unroll
-        for (uint32_t j = 0; j < 4; ++j) h4[j] = lo[k] + j < hi[k] ? ldg(hb + (size_t)(lo[k] + j) * hs) : 0xffffffffu;
-#pragma unroll
-        for (uint32_t j = 0; j < 4; ++j)
-            if (lo[k] + j < hi[k] && h4[j] <= key[k]) {
-                s[k] = (int)(lo[k] + j);
-                hit |= 1u << k;
-            }
-    }
-    act &= hit | one;
-    if (!act) return 0u;
-    // segment records: head, block offset, aux, count | descriptor, regression
-    uint4 q0[K], q1[K];
-#pragma unroll
-    for (int k = 0; k < K; ++k)
-        if (act >> k & 1u) {
-            q0[k] = __ldg(reinterpret_cast<const uint4 *>(prs + s[k]));
-            q1[k] = __ldg(reinterpret_cast<const uint4 *>(prs + s[k]) + 1);
-        }
-#pragma unroll
-    for (int k = 0; k < K; ++k)
-        if ((act & one) >> k & 1u && key[k] < q0[k].x) act &= ~(1u << k);
-    if (!act) return 0u;
-    const uint32_t *lw = ix.words + L.word_base;
-    uint32_t found = 0;
-    if (KIND == kKindDgap || (KIND == kKindAny && codec_is_dgap(L.codec))) {
-        // d-gap walks: each is a stream over one block
-#pragma unroll
-        for (int k = 0; k < K; ++k)
-            if (act >> k & 1u) {
-                const uint32_t *blk = lw + q0[k].y;
-                const BlkHdr h = blk_hdr(q1[k].x);
-                const bool f = (KIND == kKindAny && codec_is_newpfd(L.codec))
-                                   ? dgap_find_newpfd(blk, h, q0[k].w, q0[k].x, q0[k].z, key[k])
-                                   : dgap_find(blk, h, q0[k].w, q0[k].x, q0[k].z, key[k]);
-                found |= (uint32_t)f << k;
-            }
-        return found;
-    }
-    if constexpr (KIND != kKindDgap) {
-        // residual codecs: windows, then one binary search step of every key per round
-        int t0[K], t1[K];
-#pragma unroll
-        for (int k = 0; k < K; ++k) {
-            t0[k] = 0;
-            t1[k] = -1;
-            if (!(act >> k & 1u)) continue;
-            // list position of the segment: only learned windows and the
-            // LRC/LRCSeg predictors use it, and those lists have fixed blocks
-            const uint32_t start = (uint32_t)s[k] << L.log2_block, count = q0[k].w;
-            int64_t w0 = 0, w1 = (int64_t)count - 1;
-            if (lrn >> k & 1u) {
-                w0 = imax64(w0, (int64_t)plo[k] - start);
-                w1 = imin64(w1, (int64_t)phi[k] - start);
-            } else if (L.codec == EXCL_CODEC_SEGLRC || L.codec == EXCL_CODEC_HS_SEGLRC || L.codec == EXCL_CODEC_LRCSEG) {
-                // Regression window (SegLRC_Intersection_kernel.cu:366-371): the
-                // pivot (key - b) / a in IEEE single precision, widened by the
-                // fit's safe range. The range was measured with this same
-                // expression on every element, so a present key always lies inside.
-                float a, bb;
-                uint32_t rl, rr;
-                int64_t off;
-                if (L.codec == EXCL_CODEC_LRCSEG) {
-                    a = __uint_as_float(L.reg[0]);
-                    bb = __uint_as_float(L.reg[1]);
-                    rl = L.reg[2];
-                    rr = L.reg[3];
-                    off = start;
-                } else {
-                    a = __uint_as_float(q1[k].y);
-                    bb = __uint_as_float(q1[k].z);
-                    rl = (q1[k].w & 0xffffu) == kProbeUnbounded ? 0x7fffffffu : (q1[k].w & 0xffffu);
-                    rr = (q1[k].w >> 16) == kProbeUnbounded ? 0x7fffffffu : (q1[k].w >> 16);
-                    off = 0;
-                }
-                const float px = __fdiv_rn(__fsub_rn(__uint2float_rn(key[k]), bb), a);
-                if (isfinite(px) && fabsf(px) < 2.0e9f) {
-                    const int64_t P = (int64_t)__float2int_rz(px) - off;
-                    w0 = imax64(w0, P - (int64_t)rl);
-                    w1 = imin64(w1, P + (int64_t)rr);
-                }
-            }
-            if (w0 <= w1) {
-                t0[k] = (int)w0;
-                t1[k] = (int)w1;
-            }
-        }
-        for (;;) {
-            uint32_t more = 0;
-#pragma unroll
-            for (int k = 0; k < K; ++k)
-                if (t0[k] <= t1[k]) {
-                    const int mid = (t0[k] + t1[k]) >> 1;
-                    SegRec rec;
-                    rec.start = (uint32_t)s[k] << L.log2_block;
-                    rec.aux = q0[k].z;
-                    SegReg reg;
-                    reg.a = __uint_as_float(q1[k].y);
-                    reg.b = __uint_as_float(q1[k].z);
-                    const ResidParams rp = resid_params(L, rec, reg);
-                    const BlkHdr h = blk_hdr(q1[k].x);
-                    const uint32_t v =
-                        resid_value(rp, (uint32_t)mid, block_value_ra(lw + q0[k].y, h, q0[k].w, (uint32_t)mid));
-                    if (v == key[k]) {
-                        found |= 1u << k;
-                        t1[k] = t0[k] - 1;
-                    } else if (v < key[k]) {
-                        t0[k] = mid + 1;
-                    } else {
-                        t1[k] = mid - 1;
-                    }
-                    more |= t0[k] <= t1[k];
-                }
-            if (!more) break;
-        }
-    }
-    return found;
+    if (t0 > t1) return false;
+    return resid_find(blk, h, rp, rec.count, (int)t0, (int)t1, key);
 }
 
 // Segment of L (list-relative) whose head is the last one <= key, found with
@@ -290,7 +127,7 @@ __device__ __forceinline__ int locate_segment(const DevIndexView &ix, const List
     uint32_t lo = 0, hi = L.nseg;
     if (ALGO != EXCL_ALGO_BSEARCH) {
         const uint32_t bk = (uint32_t)((uint64_t)key >> L.dir_shift);
-        const uint32_t d0 = ix.dir[L.dir_base + bk].x, d1 = ix.dir[L.dir_base + bk + 1].x;
+        const uint32_t d0 = ldg(ix.dir + L.dir_base + bk), d1 = ldg(ix.dir + L.dir_base + bk + 1);
         lo = codec_is_hs(L.codec) ? d0 : (d0 ? d0 - 1u : 0u);
         hi = d1;
     }
@@ -304,7 +141,7 @@ __device__ __forceinline__ int locate_segment(const DevIndexView &ix, const List
 // probe choice): when the tile's surviving keys span few of the list's
 // segments (at most b.merge_segs, whose docIDs fit kMergeCap), the warp
 // decodes that span into shared memory once and every key is looked up there;
-// otherwise each key is probed on its own (probe_keys).
+// otherwise each key is probed on its own (probe_key).
 
 // MINB: resident 8-warp CTAs per SM the register budget is cut for (4: 64
 // registers; 5: 48; 6: 40), traded for more probes in flight; the launch
@@ -398,42 +235,29 @@ __global__ void __launch_bounds__(WARPS * 32, (8 / WARPS) * MINB) k_probe(DevInd
             }
             (void)mseg0;
             uint32_t nout = 0;
-            // kProbeIlp keys per lane per round: keys base + 32k + lane
-            for (uint32_t base = 0; base < alive; base += 32u * kProbeIlp) {
-                uint32_t kv[kProbeIlp], act = 0;
-#pragma unroll
-                for (int k = 0; k < kProbeIlp; ++k) {
-                    const uint32_t i = base + 32u * k + lane;
-                    kv[k] = i < alive ? keys[i] : 0u;
-                    act |= (uint32_t)(i < alive) << k;
-                }
-                uint32_t fm = 0;
+            for (uint32_t base = 0; base < alive; base += 32) {
+                const uint32_t i = base + lane;
+                const bool valid = i < alive;
+                const uint32_t key = valid ? keys[i] : 0u;
+                bool f;
                 if (span) {
-#pragma unroll
-                    for (int k = 0; k < kProbeIlp; ++k) {
-                        // first position with mbuf[pos] >= key, in shared memory
-                        uint32_t lo = 0, hi = span;
-                        while (lo < hi) {
-                            const uint32_t mid = (lo + hi) >> 1;
-                            if (mbuf[mid] < kv[k]) lo = mid + 1;
-                            else hi = mid;
-                        }
-                        fm |= (uint32_t)((act >> k & 1u) && lo < span && mbuf[lo] == kv[k]) << k;
+                    // first position with mbuf[pos] >= key, in shared memory
+                    uint32_t lo = 0, hi = span;
+                    while (lo < hi) {
+                        const uint32_t mid = (lo + hi) >> 1;
+                        if (mbuf[mid] < key) lo = mid + 1;
+                        else hi = mid;
                     }
+                    f = valid && lo < span && mbuf[lo] == key;
                 } else {
-                    fm = probe_keys<ALGO, KIND, kProbeIlp>(ix, L, kv, act, fallbacks);
+                    f = valid && probe_key<ALGO, KIND>(ix, L, key, fallbacks);
                 }
-                probes += __popc(act);
-                // every lane has read its keys before any survivor is written
-                // back; groups are compacted in order, so survivors stay sorted
+                probes += valid;
+                const uint32_t m = __ballot_sync(0xffffffffu, f);
+                const uint32_t pos = nout + __popc(m & ((1u << lane) - 1u));
                 __syncwarp();
-#pragma unroll
-                for (int k = 0; k < kProbeIlp; ++k) {
-                    const bool f = fm >> k & 1u;
-                    const uint32_t m = __ballot_sync(0xffffffffu, f);
-                    if (f) keys[nout + __popc(m & ((1u << lane) - 1u))] = kv[k];
-                    nout += __popc(m);
-                }
+                if (f) keys[pos] = key;
+                nout += __popc(m);
             }
             __syncwarp();
             alive = nout;

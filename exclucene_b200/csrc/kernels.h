@@ -31,13 +31,6 @@ struct BatchView {
 // probe kernel: shared-memory merge of a tile's keys against a decoded span
 constexpr uint32_t kMergeCap = 512;      // docIDs of the span (two 256-blocks)
 constexpr uint32_t kMergeMinKeys = 32;   // fewer keys than this: always probe
-// keys each lane probes at once (independent dependent-load chains in
-// flight). Measured on the Zipf/SegLRC batch: 2 keys ran 5% slower than 1
-// (register spills; more chains per lane did not raise the loads in flight).
-#ifndef EXCL_PROBE_ILP
-#define EXCL_PROBE_ILP 1
-#endif
-constexpr int kProbeIlp = EXCL_PROBE_ILP;
 
 // pipeline.cu
 constexpr uint32_t kPackThreads = 256;

@@ -189,8 +189,7 @@ void DeviceIndex::release() {
     seg_gword = nullptr;
     seg_probe = nullptr;
     lists = nullptr;
-    words = seg_head = nullptr;
-    dir = nullptr;
+    words = seg_head = dir = nullptr;
     seg_rec = nullptr;
     seg_reg = nullptr;
     tilemap = post_base = nullptr;
@@ -470,16 +469,6 @@ extern "C" int excl_index_upload(excl_ctx *ctx, excl_index *ix) {
             sgw[g] = ix->lists[l].word_base + ix->seg_rec[g].off;
         }
     sgw[nsegs] = ix->words.size() - kWordPad;
-    // directory entries carry the head of the segment they point to, so a
-    // probe learns from one load whether the key precedes that segment
-    std::vector<uint2> dir2(ix->dir.size());
-    for (uint32_t l = 0; l < ix->nlists; ++l) {
-        const ListDesc &L = ix->lists[l];
-        for (uint32_t b = 0; b <= L.ndir && (size_t)L.dir_base + b < dir2.size(); ++b) {
-            const uint32_t sg = ix->dir[(size_t)L.dir_base + b];
-            dir2[(size_t)L.dir_base + b] = make_uint2(sg, sg < L.nseg ? ix->seg_head[(size_t)L.seg_base + sg] : 0xffffffffu);
-        }
-    }
     std::vector<ProbeRec> prec(nsegs);
     for (size_t g = 0; g < nsegs; ++g) {
         const SegRec &r = ix->seg_rec[g];
@@ -526,7 +515,7 @@ extern "C" int excl_index_upload(excl_ctx *ctx, excl_index *ix) {
     up(d->seg_head, ix->seg_head.data(), ix->seg_head.size() * 4);
     up(d->seg_rec, ix->seg_rec.data(), ix->seg_rec.size() * sizeof(SegRec));
     up(d->seg_reg, ix->seg_reg.data(), ix->seg_reg.size() * sizeof(SegReg));
-    up(d->dir, dir2.data(), dir2.size() * sizeof(uint2));
+    up(d->dir, ix->dir.data(), ix->dir.size() * 4);
     up(d->tilemap, ix->tilemap.data(), ix->tilemap.size() * 8);
     up(d->post_base, pb.data(), pb.size() * 8);
     up(d->seg_list, slist.data(), slist.size() * 4);
@@ -538,7 +527,7 @@ extern "C" int excl_index_upload(excl_ctx *ctx, excl_index *ix) {
         return st;
     }
     d->bytes = ix->lists.size() * sizeof(ListDesc) + ix->words.size() * 4 + ix->seg_head.size() * 4 +
-               ix->seg_rec.size() * sizeof(SegRec) + ix->seg_reg.size() * sizeof(SegReg) + dir2.size() * sizeof(uint2) +
+               ix->seg_rec.size() * sizeof(SegRec) + ix->seg_reg.size() * sizeof(SegReg) + ix->dir.size() * 4 +
                ix->tilemap.size() * 8 + pb.size() * 8 + slist.size() * 4 + sgw.size() * 8 +
                prec.size() * sizeof(ProbeRec);
     d->device = ctx->device;

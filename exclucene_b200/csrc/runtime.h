@@ -17,7 +17,7 @@ struct DeviceIndex {
     uint32_t *seg_head = nullptr;
     SegRec *seg_rec = nullptr;
     SegReg *seg_reg = nullptr;
-    uint2 *dir = nullptr;  // directory entries with the head of their segment
+    uint32_t *dir = nullptr;
     uint64_t *tilemap = nullptr;
     uint64_t *post_base = nullptr;
     uint32_t *seg_list = nullptr;
