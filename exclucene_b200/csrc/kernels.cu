@@ -157,11 +157,20 @@ __global__ void __launch_bounds__(WARPS * 32, (8 / WARPS) * MINB) k_probe(DevInd
     uint32_t *keys = s_keys[w];  // the tile's keys (a sub-range of the decoded segment when tiles are cut)
     uint32_t *mbuf = s_merge[w];
     ListDesc &L = s_list[w];
-    const uint32_t T = min(b.tile_prefix[b.nq], b.max_tiles);
+    // work order: the pack kernel's tile_order (heavy tiles first); after a
+    // tile overflow (reported as kErrCapacity) tile_order may have holes, so
+    // the tiles that fit are taken in id order instead
+    const uint32_t Tall = b.tile_prefix[b.nq];
+    const uint32_t T = min(Tall, b.max_tiles);
+    const uint32_t H = min(b.tile_prefix[b.nq + 1], T);
+    const bool ordered = Tall <= b.max_tiles;
     uint32_t probes = 0, fallbacks = 0, nkeys = 0, merges = 0;
     for (;;) {
         uint32_t t = 0;
-        if (lane == 0) t = atomicAdd(b.tile_counter, 1u);
+        if (lane == 0) {
+            const uint32_t wi = atomicAdd(b.tile_counter, 1u);
+            t = wi >= T || !ordered ? wi : b.tile_order[wi < H ? wi : b.max_tiles - 1u - (wi - H)];
+        }
         t = __shfl_sync(0xffffffffu, t, 0);
         if (t >= T) break;
         const uint32_t q = b.tile_q[t];  // owner written by the pack kernel

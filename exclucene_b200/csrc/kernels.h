@@ -14,6 +14,8 @@ struct BatchView {
     const uint32_t *qnterms;     // terms per query
     const uint32_t *tile_prefix; // nq + 1, exclusive prefix of tiles per query
     uint32_t *tile_q;            // max_tiles, query owning each tile
+    uint32_t *tile_order;        // max_tiles, probe order: heavy tiles from the front, the rest from the back
+                                 // (tile_prefix[nq + 1] = heavy tiles)
     uint32_t *tile_counter;      // work-queue head (zeroed by k_pack_scan)
     const uint32_t *key_base;    // nq + 1, exclusive prefix of shortest-list lengths
     uint32_t *tile_count;        // survivors per tile
@@ -48,6 +50,7 @@ struct PackSync {
     uint32_t flag[kPackMaxCtas];
     uint32_t agg_t[kPackMaxCtas];
     uint32_t agg_k[kPackMaxCtas];
+    uint32_t agg_h[kPackMaxCtas];
 };
 
 // Everything one batch launch needs.

@@ -60,6 +60,59 @@ __device__ __forceinline__ uint64_t chunk_word(uint32_t tag, uint32_t status, ui
     return ((uint64_t)tag << 34) | ((uint64_t)status << 32) | v;
 }
 
+// Block-wide exclusive scan of three values at once; returns the block totals.
+__device__ __forceinline__ void block_scan3(const uint32_t (&v)[3], uint32_t (&e)[3], uint32_t (&t)[3],
+                                            uint32_t (*sh)[33]) {
+    const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    uint32_t in[3] = {v[0], v[1], v[2]};
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const uint32_t x = __shfl_up_sync(0xffffffffu, in[j], o);
+            if (lane >= (uint32_t)o) in[j] += x;
+        }
+    if (lane == 31)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) sh[j][w] = in[j];
+    __syncthreads();
+    if (w == 0) {
+        uint32_t a[3], c[3];
+#pragma unroll
+        for (int j = 0; j < 3; ++j) c[j] = a[j] = lane < nw ? sh[j][lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                const uint32_t x = __shfl_up_sync(0xffffffffu, c[j], o);
+                if (lane >= (uint32_t)o) c[j] += x;
+            }
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            if (lane < nw) sh[j][lane] = c[j] - a[j];
+            if (lane == 31) sh[j][32] = c[j];
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        e[j] = sh[j][w] + in[j] - v[j];
+        t[j] = sh[j][32];
+    }
+}
+
+// Tiles of a query's shortest list that hold at least half a tile of keys:
+// the first `heavy` tiles (all full tiles, and the last one when it is at
+// least half full). A tile's probe time grows with its keys, so these go to
+// the front of the probe kernel's work queue and the small tiles fill the end
+// (longest first keeps the busiest SM near the average). Variable (HS) tiles
+// all count as heavy.
+__device__ __forceinline__ uint32_t heavy_tiles(uint32_t n, uint32_t nt, uint32_t log2_block, uint32_t split) {
+    if (!log2_block || nt == 0) return nt;
+    const uint32_t S = (1u << log2_block) >> tile_split_of(log2_block, split);
+    return min(nt, n / S + (2u * (n % S) >= S ? 1u : 0u));
+}
+
 // Block-wide exclusive scan of two values at once; returns the block totals.
 __device__ __forceinline__ void block_scan2(uint32_t a, uint32_t b, uint32_t &ea, uint32_t &eb, uint32_t &ta,
                                             uint32_t &tb, uint32_t *sa, uint32_t *sb) {
@@ -112,7 +165,7 @@ __global__ void __launch_bounds__(kPackThreads) k_pack_scan(const ListDesc *__re
                                                             const uint32_t *toff,   // coherent loads only
                                                             uint32_t nq,
                                                             BatchView b, PackSync *__restrict__ sync) {
-    __shared__ uint32_t sa[33], sb[33], s_pre[2], s_et[kPackThreads], s_id, s_tag;
+    __shared__ uint32_t s_sc[3][33], s_pre[3], s_et[kPackThreads], s_eh[kPackThreads], s_h[kPackThreads], s_id, s_tag;
     if (threadIdx.x == 0) {
         s_id = atomicAdd(&sync->ticket, 1u);
         s_tag = next_tag(*(volatile uint32_t *)&sync->epoch);
@@ -120,7 +173,7 @@ __global__ void __launch_bounds__(kPackThreads) k_pack_scan(const ListDesc *__re
     __syncthreads();
     const uint32_t bid = s_id, tag = s_tag;
     const uint32_t q = bid * blockDim.x + threadIdx.x;
-    uint32_t nt = 0, nk = 0;
+    uint32_t nt = 0, nk = 0, lb0 = 0;
     if (q < nq) {
         const uint32_t t0 = toff[q], t1 = toff[q + 1];
         uint32_t k = t1 >= t0 ? t1 - t0 : 0u;
@@ -131,7 +184,7 @@ __global__ void __launch_bounds__(kPackThreads) k_pack_scan(const ListDesc *__re
         uint32_t *dst = const_cast<uint32_t *>(b.qterms) + (size_t)q * kMaxTerms;
         if (k <= kPackRegTerms) {
             // common case: all in registers, every load of the query issued at once
-            uint32_t id[kPackRegTerms], len[kPackRegTerms], ntl[kPackRegTerms];
+            uint32_t id[kPackRegTerms], len[kPackRegTerms], ntl[kPackRegTerms], lbl[kPackRegTerms];
             bool bad = false;
 #pragma unroll
             for (uint32_t j = 0; j < kPackRegTerms; ++j) id[j] = j < k ? terms[t0 + j] : 0u;
@@ -140,9 +193,8 @@ __global__ void __launch_bounds__(kPackThreads) k_pack_scan(const ListDesc *__re
                 const bool v = j < k && id[j] < nlists;
                 bad |= j < k && id[j] >= nlists;
                 len[j] = v ? __ldg(&lists[id[j]].n) : 0xffffffffu;  // absent terms sort last
-                ntl[j] = v ? split_tiles(len[j], __ldg(&lists[id[j]].ntiles), __ldg(&lists[id[j]].log2_block),
-                                         b.tile_split)
-                           : 0u;
+                lbl[j] = v ? __ldg(&lists[id[j]].log2_block) : 0u;
+                ntl[j] = v ? split_tiles(len[j], __ldg(&lists[id[j]].ntiles), lbl[j], b.tile_split) : 0u;
             }
             if (bad) {
                 atomicOr(b.err, kErrTermId);
@@ -157,12 +209,14 @@ __global__ void __launch_bounds__(kPackThreads) k_pack_scan(const ListDesc *__re
                         uint32_t x = id[j]; id[j] = id[j - 1]; id[j - 1] = x;
                         x = len[j]; len[j] = len[j - 1]; len[j - 1] = x;
                         x = ntl[j]; ntl[j] = ntl[j - 1]; ntl[j - 1] = x;
+                        x = lbl[j]; lbl[j] = lbl[j - 1]; lbl[j - 1] = x;
                     }
 #pragma unroll
             for (uint32_t j = 0; j < kPackRegTerms; ++j)
                 if (j < k) dst[j] = id[j];
             nt = k ? ntl[0] : 0u;
             nk = k ? len[0] : 0u;
+            lb0 = k ? lbl[0] : 0u;
         } else {
             uint32_t id[kMaxTerms], len[kMaxTerms];
             bool bad = false;
@@ -197,17 +251,20 @@ __global__ void __launch_bounds__(kPackThreads) k_pack_scan(const ListDesc *__re
                 len[j] = cl;
             }
             for (uint32_t i = 0; i < k; ++i) dst[i] = id[i];
-            nt = k ? split_tiles(len[0], __ldg(&lists[id[0]].ntiles), __ldg(&lists[id[0]].log2_block), b.tile_split)
-                   : 0u;
+            lb0 = k ? __ldg(&lists[id[0]].log2_block) : 0u;
+            nt = k ? split_tiles(len[0], __ldg(&lists[id[0]].ntiles), lb0, b.tile_split) : 0u;
             nk = k ? len[0] : 0u;
         }
         const_cast<uint32_t *>(b.qnterms)[q] = k;
     }
-    uint32_t et, ek, bt, bk;
-    block_scan2(nt, nk, et, ek, bt, bk, sa, sb);
+    const uint32_t nh = heavy_tiles(nk, nt, lb0, b.tile_split);
+    uint32_t ex[3], tot[3];
+    block_scan3({nt, nk, nh}, ex, tot, s_sc);
+    const uint32_t et = ex[0], ek = ex[1], bt = tot[0], bk = tot[1];
     if (threadIdx.x == 0) {
         sync->agg_t[bid] = bt;
         sync->agg_k[bid] = bk;
+        sync->agg_h[bid] = tot[2];
         st_release(&sync->flag[bid], tag);
     }
     if (threadIdx.x < 32) {
@@ -216,7 +273,7 @@ __global__ void __launch_bounds__(kPackThreads) k_pack_scan(const ListDesc *__re
         // predecessors in flight at once; one fence then orders the totals'
         // loads after the flags that published them.
         const uint32_t lane = threadIdx.x;
-        uint32_t pt = 0, pk = 0;
+        uint32_t pt = 0, pk = 0, ph = 0;
         for (uint32_t p0 = 0; p0 < bid; p0 += 128) {
             uint32_t f[4];
 #pragma unroll
@@ -244,6 +301,7 @@ __global__ void __launch_bounds__(kPackThreads) k_pack_scan(const ListDesc *__re
                 if (p < bid) {
                     pt += ld_relaxed(&sync->agg_t[p]);
                     pk += ld_relaxed(&sync->agg_k[p]);
+                    ph += ld_relaxed(&sync->agg_h[p]);
                 }
             }
         }
@@ -251,19 +309,24 @@ __global__ void __launch_bounds__(kPackThreads) k_pack_scan(const ListDesc *__re
         for (int o = 16; o > 0; o >>= 1) {
             pt += __shfl_xor_sync(0xffffffffu, pt, o);
             pk += __shfl_xor_sync(0xffffffffu, pk, o);
+            ph += __shfl_xor_sync(0xffffffffu, ph, o);
         }
         if (lane == 0) {
             s_pre[0] = pt;
             s_pre[1] = pk;
+            s_pre[2] = ph;
         }
     }
     s_et[threadIdx.x] = et;
+    s_eh[threadIdx.x] = ex[2];
+    s_h[threadIdx.x] = nh;
     __syncthreads();
     const uint32_t pt = s_pre[0];
     if (threadIdx.x == 0) {
         const uint32_t pk = s_pre[1];
         if (bid == gridDim.x - 1) {
             const_cast<uint32_t *>(b.tile_prefix)[nq] = pt + bt;
+            const_cast<uint32_t *>(b.tile_prefix)[nq + 1] = s_pre[2] + tot[2];  // heavy tiles in the batch
             const_cast<uint32_t *>(b.key_base)[nq] = pk + bk;
             if ((uint64_t)pt + bt > b.max_tiles || (uint64_t)pk + bk > b.max_keys) atomicOr(b.err, kErrCapacity);
         }
@@ -285,7 +348,10 @@ __global__ void __launch_bounds__(kPackThreads) k_pack_scan(const ListDesc *__re
         const_cast<uint32_t *>(b.key_base)[q] = s_pre[1] + ek;
     }
     // owner of each of this CTA's tiles: the last query whose first tile is
-    // at or before it (queries with no tiles share their successor's start)
+    // at or before it (queries with no tiles share their successor's start);
+    // and the tile's place in the probe order: heavy tiles from the front in
+    // query order, the others from the back of tile_order
+    const uint32_t ph = s_pre[2];
     for (uint32_t tl = threadIdx.x; tl < bt && pt + tl < b.max_tiles; tl += blockDim.x) {
         uint32_t lo = 0, hi = blockDim.x - 1;
         while (lo < hi) {
@@ -293,7 +359,10 @@ __global__ void __launch_bounds__(kPackThreads) k_pack_scan(const ListDesc *__re
             if (s_et[mid] <= tl) lo = mid;
             else hi = mid - 1;
         }
-        b.tile_q[pt + tl] = bid * blockDim.x + lo;
+        const uint32_t t = pt + tl, i = tl - s_et[lo], hb = ph + s_eh[lo];
+        b.tile_q[t] = bid * blockDim.x + lo;
+        if (i < s_h[lo]) b.tile_order[hb + i] = t;
+        else b.tile_order[b.max_tiles - 1u - (t - hb - s_h[lo])] = t;
     }
 }
 

@@ -229,6 +229,7 @@ int ctx_alloc_batch(excl_ctx *ctx) {
     st |= dalloc(ctx, &ctx->d_tile_q, (size_t)ctx->max_tiles + 1, "alloc tile owner");
     st |= dalloc(ctx, &ctx->d_tile_count, (size_t)ctx->max_tiles + 1, "alloc tile count");
     st |= dalloc(ctx, &ctx->d_tile_slot, (size_t)ctx->max_tiles + 1, "alloc tile slot");
+    st |= dalloc(ctx, &ctx->d_tile_order, (size_t)ctx->max_tiles + 1, "alloc tile order");
     st |= dalloc(ctx, &ctx->d_scratch, (size_t)c.max_keys, "alloc scratch");
     st |= dalloc(ctx, &ctx->d_misc, 16, "alloc misc");
     st |= dalloc(ctx, &ctx->d_stats, 4, "alloc stats");
@@ -278,6 +279,7 @@ int run_pipeline(excl_ctx *ctx, excl_index *ix, const uint32_t *d_terms, const u
     b.key_base = ctx->d_key_base;
     b.tile_count = ctx->d_tile_count;
     b.tile_slot = ctx->d_tile_slot;
+    b.tile_order = ctx->d_tile_order;
     b.scratch = ctx->d_scratch;
     b.max_tiles = ctx->max_tiles;
     b.merge_segs = ctx->merge_segs;
@@ -421,7 +423,7 @@ extern "C" int excl_ctx_destroy(excl_ctx *ctx) {
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     uint32_t *bufs[] = {ctx->d_terms,   ctx->d_toff, ctx->d_qterms,   ctx->d_qnterms,   ctx->d_tile_prefix,
                         ctx->d_tile_q,  ctx->d_tile_count, ctx->d_scratch, ctx->d_misc, ctx->d_key_base,
-                        ctx->d_tile_slot, ctx->d_offsets, ctx->d_docids};
+                        ctx->d_tile_slot, ctx->d_tile_order, ctx->d_offsets, ctx->d_docids};
     for (uint32_t *p : bufs) cudaFree(p);
     if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
     cudaFree(ctx->d_stats);

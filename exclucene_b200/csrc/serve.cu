@@ -49,7 +49,7 @@ constexpr uint64_t up256(uint64_t b) { return (b + 255) & ~255ull; }
 // Byte layout of one batch's block of the pool (the queries themselves stay
 // in the slot's mapped host arrays).
 struct WsLayout {
-    uint64_t qterms, qnterms, tile_prefix, key_base, tile_q, tile_count, tile_slot, scratch, total;
+    uint64_t qterms, qnterms, tile_prefix, key_base, tile_q, tile_count, tile_slot, tile_order, scratch, total;
 };
 
 WsLayout ws_layout(uint64_t nq, uint64_t /*nterms*/, uint64_t tiles, uint64_t keys) {
@@ -67,6 +67,7 @@ WsLayout ws_layout(uint64_t nq, uint64_t /*nterms*/, uint64_t tiles, uint64_t ke
     L.tile_q = take(tiles + 1);
     L.tile_count = take(tiles + 1);
     L.tile_slot = take(tiles + 1);
+    L.tile_order = take(tiles + 1);
     L.scratch = take(keys);
     L.total = o;
     return L;
@@ -246,6 +247,7 @@ int launch_on_slot(excl_server *s, Slot *sl, uint64_t nterms, uint64_t tiles, ui
     b.key_base = at(L.key_base);
     b.tile_count = at(L.tile_count);
     b.tile_slot = at(L.tile_slot);
+    b.tile_order = at(L.tile_order);
     b.scratch = at(L.scratch);
     b.max_tiles = (uint32_t)tiles;
     b.merge_segs = 2;
