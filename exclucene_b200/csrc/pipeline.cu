@@ -351,13 +351,19 @@ __global__ void __launch_bounds__(kPackThreads) k_pack_scan(const ListDesc *__re
     // at or before it (queries with no tiles share their successor's start);
     // and the tile's place in the probe order: heavy tiles from the front in
     // query order, the others from the back of tile_order
+    // (a thread's tiles ascend, so its owners do too: the search resumes from
+    // the last owner, and a run of one query's tiles costs one check each)
     const uint32_t ph = s_pre[2];
+    uint32_t lo = 0;
     for (uint32_t tl = threadIdx.x; tl < bt && pt + tl < b.max_tiles; tl += blockDim.x) {
-        uint32_t lo = 0, hi = blockDim.x - 1;
-        while (lo < hi) {
-            const uint32_t mid = (lo + hi + 1) >> 1;
-            if (s_et[mid] <= tl) lo = mid;
-            else hi = mid - 1;
+        if (lo + 1 < blockDim.x && s_et[lo + 1] <= tl) {
+            uint32_t hi = blockDim.x - 1;
+            ++lo;
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi + 1) >> 1;
+                if (s_et[mid] <= tl) lo = mid;
+                else hi = mid - 1;
+            }
         }
         const uint32_t t = pt + tl, i = tl - s_et[lo], hb = ph + s_eh[lo];
         b.tile_q[t] = bid * blockDim.x + lo;
@@ -400,7 +406,8 @@ __device__ __forceinline__ void warp_lower_bound2(const uint32_t *a, uint32_t n,
 // of the queries starting in it; then the chunk's inclusive prefix is
 // published. Phase B (every warp of the grid, once all chunk tickets are
 // taken, so every chunk is owned by a running CTA): survivors copied tile by
-// tile, each tile after its chunk's prefix is out.
+// tile, each tile after its chunk's prefix is out; a warp gathers the
+// bookkeeping of 32 of its tiles at once.
 // The batch's error bits to the host word the batch names (the device word is
 // cleared for the next batch); nothing when it names none.
 __device__ __forceinline__ void hand_over_flags(const BatchView &b) {
@@ -503,15 +510,21 @@ __global__ void __launch_bounds__(kSSThreads) k_scatter(BatchView b, PackSync *_
             st_release64(&chunk_state[c], chunk_word(tag, kPrefix, base + tot));
         }
     }
-    // phase B: warp per tile over the whole grid; eight independent loads per lane in flight
+    // phase B: warp w takes tiles w, w + nw, w + 2nw, ... (neighbouring tiles
+    // go to different warps, so a query with many survivors spreads over the
+    // grid). Lane j handles the warp's j-th tile of a round of 32: its survivor
+    // count, its chunk's prefix (bounded wait), its output position and slot,
+    // all lanes at once; then the warp copies the non-empty tiles one after
+    // another, eight independent loads per lane.
     const uint32_t gw = blockIdx.x * (kSSThreads / 32) + w, nw = gridDim.x * (kSSThreads / 32);
     const uint32_t *__restrict__ scr = b.scratch;
-    uint32_t ready = 0xffffffffu;  // chunk whose prefix this warp has seen
-    for (uint32_t t = gw; t < T; t += nw) {
-        const uint32_t n = b.tile_count[t];
-        if (n == 0) continue;
-        const uint32_t c = t / kSSChunk;
-        if (c != ready) {
+    for (uint64_t j0 = 0; gw + j0 * nw < T; j0 += 32) {
+        const uint64_t tt = gw + (j0 + lane) * nw;
+        const uint32_t t = tt < T ? (uint32_t)tt : T;
+        const uint32_t n = t < T ? b.tile_count[t] : 0u;
+        uint32_t o = 0, slot = 0;
+        if (n) {
+            const uint32_t c = t / kSSChunk;
             uint64_t s = ld_acquire64(&chunk_state[c]);
             uint32_t spins = 0;
             while ((uint32_t)(s >> 34) != tag || ((uint32_t)(s >> 32) & 3u) != kPrefix) {
@@ -522,20 +535,27 @@ __global__ void __launch_bounds__(kSSThreads) k_scatter(BatchView b, PackSync *_
                 __nanosleep(64);
                 s = ld_acquire64(&chunk_state[c]);
             }
-            ready = c;
+            o = ld_acquire(&tile_out[t]);
+            slot = b.tile_slot[t];
         }
-        const uint64_t o = ld_acquire(&tile_out[t]);
-        const uint32_t *src = scr + b.tile_slot[t];
-        uint32_t v[kTileKeys / 32];
+        uint32_t m = __ballot_sync(0xffffffffu, n != 0u);
+        while (m) {
+            const uint32_t l = (uint32_t)(__ffs(m) - 1);
+            m &= m - 1u;
+            const uint32_t nl = __shfl_sync(0xffffffffu, n, l), ol = __shfl_sync(0xffffffffu, o, l),
+                           sl = __shfl_sync(0xffffffffu, slot, l);
+            const uint32_t *src = scr + sl;
+            uint32_t v[kTileKeys / 32];
 #pragma unroll
-        for (uint32_t i = 0; i < kTileKeys / 32; ++i) {
-            const uint32_t k = lane + 32u * i;
-            if (k < n) v[i] = src[k];
-        }
+            for (uint32_t i = 0; i < kTileKeys / 32; ++i) {
+                const uint32_t k = lane + 32u * i;
+                if (k < nl) v[i] = src[k];
+            }
 #pragma unroll
-        for (uint32_t i = 0; i < kTileKeys / 32; ++i) {
-            const uint32_t k = lane + 32u * i;
-            if (k < n && o + k < cap) docids[o + k] = v[i];
+            for (uint32_t i = 0; i < kTileKeys / 32; ++i) {
+                const uint32_t k = lane + 32u * i;
+                if (k < nl && (uint64_t)ol + k < cap) docids[(uint64_t)ol + k] = v[i];
+            }
         }
     }
     // the last CTA out resets the chunk ticket and hands the batch's error
