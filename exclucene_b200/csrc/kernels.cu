@@ -174,11 +174,15 @@ __global__ void __launch_bounds__(WARPS * 32, (8 / WARPS) * MINB) k_probe(DevInd
         t = __shfl_sync(0xffffffffu, t, 0);
         if (t >= T) break;
         const uint32_t q = b.tile_q[t];  // owner written by the pack kernel
+        // the query's sorted terms (lane j holds term j), first tile, term
+        // count and key base: one round of independent loads
+        const uint32_t tq = b.qterms[(size_t)q * kMaxTerms + lane];
         const uint32_t ti = t - b.tile_prefix[q];
         const uint32_t k = b.qnterms[q];
-        const uint32_t *qt = b.qterms + (size_t)q * kMaxTerms;
+        const uint32_t kbase = b.key_base[q];
+        const uint32_t list0 = __shfl_sync(0xffffffffu, tq, 0);
         __syncwarp();
-        if (lane < 5) reinterpret_cast<uint4 *>(&L)[lane] = reinterpret_cast<const uint4 *>(ix.lists + qt[0])[lane];
+        if (lane < 5) reinterpret_cast<uint4 *>(&L)[lane] = reinterpret_cast<const uint4 *>(ix.lists + list0)[lane];
         __syncwarp();
         // decode the tile's keys: one fixed segment, or 1..255 consecutive
         // variable segments / one 256-slice of a large segment
@@ -209,8 +213,9 @@ __global__ void __launch_bounds__(WARPS * 32, (8 / WARPS) * MINB) k_probe(DevInd
         nkeys += kc;
         uint32_t alive = kc;
         for (uint32_t j = 1; j < k && alive; ++j) {
+            const uint32_t lj = __shfl_sync(0xffffffffu, tq, j);
             __syncwarp();
-            if (lane < 5) reinterpret_cast<uint4 *>(&L)[lane] = reinterpret_cast<const uint4 *>(ix.lists + qt[j])[lane];
+            if (lane < 5) reinterpret_cast<uint4 *>(&L)[lane] = reinterpret_cast<const uint4 *>(ix.lists + lj)[lane];
             __syncwarp();
             // merge when the keys' range covers few segments: estimated from
             // the list's density first (no loads), then measured
@@ -273,7 +278,7 @@ __global__ void __launch_bounds__(WARPS * 32, (8 / WARPS) * MINB) k_probe(DevInd
         }
         // survivors go to the tile's key-indexed slot (its keys' positions in
         // the batch's concatenated shortest lists)
-        const uint64_t slot = (uint64_t)b.key_base[q] + first_elem;
+        const uint64_t slot = (uint64_t)kbase + first_elem;
         if (slot + kc > b.max_keys) {
             if (lane == 0) atomicOr(b.err, kErrCapacity);
             alive = 0;
