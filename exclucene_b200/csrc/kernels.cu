@@ -153,6 +153,9 @@ __global__ void __launch_bounds__(WARPS * 32, (8 / WARPS) * MINB) k_probe(DevInd
     __shared__ uint32_t s_keys[WARPS][kTileKeys];
     __shared__ uint32_t s_merge[WARPS][kMergeCap];
     __shared__ ListDesc s_list[WARPS];
+    // the scatter kernel may launch now; the pack kernel's output is read below
+    pdl_launch_dependents();
+    pdl_wait();
     const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
     uint32_t *keys = s_keys[w];  // the tile's keys (a sub-range of the decoded segment when tiles are cut)
     uint32_t *mbuf = s_merge[w];
@@ -324,7 +327,7 @@ static void launch_probe_t(const DevIndexView &ix, const BatchView &b, int nsm, 
         if (dev >= 0 && dev < 64) occ[dev] = per_sm;
     }
     const uint32_t grid = (uint32_t)std::max(1, std::min(per_sm, (8 / WARPS) * MINB) * nsm);
-    k_probe<ALGO, WARPS, MINB, KIND><<<grid, WARPS * 32, 0, st>>>(ix, b);
+    launch_pdl(k_probe<ALGO, WARPS, MINB, KIND>, dim3(grid), dim3(WARPS * 32), st, ix, b);
 }
 
 template <int ALGO, int WARPS, int MINB>

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <utility>
 
 #include "excl_device.cuh"
 
@@ -29,6 +30,32 @@ struct BatchView {
     uint32_t *err_out;           // or null: device-mapped host word that receives this batch's error bits at its end (the device word is cleared)
     uint64_t *stats;             // [probes, fallbacks] or null
 };
+
+// Programmatic dependent launch: the batch's kernels are launched with
+// programmatic stream serialization, so a kernel's CTAs may become resident
+// while the previous kernel of the stream still runs. Each kernel lets its
+// successor launch at once (pdl_launch_dependents) and waits, before its
+// first read of the previous kernel's output, until that kernel has finished
+// and its writes are visible (pdl_wait; a no-op when launched without the
+// attribute). This hides the launch and ramp-up gaps between the three
+// launches of a batch.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t st, Args &&...args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
 
 // probe kernel: shared-memory merge of a tile's keys against a decoded span
 constexpr uint32_t kMergeCap = 512;      // docIDs of the span (two 256-blocks)

@@ -166,6 +166,11 @@ __global__ void __launch_bounds__(kPackThreads) k_pack_scan(const ListDesc *__re
                                                             uint32_t nq,
                                                             BatchView b, PackSync *__restrict__ sync) {
     __shared__ uint32_t s_sc[3][33], s_pre[3], s_et[kPackThreads], s_eh[kPackThreads], s_h[kPackThreads], s_id, s_tag;
+    // the probe kernel may launch now (it waits for this grid's results);
+    // this grid reads the batch's queries only, and (when launched after
+    // another batch on this stream) the shared scan state once that batch ends
+    pdl_launch_dependents();
+    pdl_wait();
     if (threadIdx.x == 0) {
         s_id = atomicAdd(&sync->ticket, 1u);
         s_tag = next_tag(*(volatile uint32_t *)&sync->epoch);
@@ -425,6 +430,8 @@ __global__ void __launch_bounds__(kSSThreads) k_scatter(BatchView b, PackSync *_
     __shared__ uint32_t s_c, s_base, s_qlo, s_qhi;
     constexpr uint32_t kPer = kSSChunk / kSSThreads;
     static_assert(kPer == 2, "two tiles per thread");
+    pdl_launch_dependents();
+    pdl_wait();  // the probe kernel's counts and slots, the pack kernel's prefixes
     const uint32_t tag = *(volatile uint32_t *)&sync->epoch;  // set by this batch's k_pack_scan
     const uint32_t nq = b.nq;
     const uint32_t T = min(b.tile_prefix[nq], b.max_tiles);
@@ -582,8 +589,8 @@ int launch_batch(const BatchLaunch &L, cudaStream_t st) {
     if (L.ev) cudaEventRecord(L.ev[1], st);
     e |= launch_probe(L.ixv, L.b, L.algo, L.warps, L.ctas_per_sm, L.nsm, st);
     if (L.ev) cudaEventRecord(L.ev[2], st);
-    k_scatter<<<std::max(1, 2 * L.nsm), kSSThreads, 0, st>>>(L.b, L.sync, L.chunk_state, L.offsets, L.docids, L.cap);
-    e |= (int)cudaGetLastError();
+    e |= (int)launch_pdl(k_scatter, dim3(std::max(1, 2 * L.nsm)), dim3(kSSThreads), st, L.b, L.sync, L.chunk_state,
+                         L.offsets, L.docids, L.cap);
     if (L.ev) cudaEventRecord(L.ev[3], st);
     return e;
 }
