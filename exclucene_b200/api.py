@@ -582,7 +582,7 @@ def library_path() -> str:
 # Allocation-free form of Context.intersect_device, for callers that cannot
 # allocate device memory when they query (their budget is fixed at start-up,
 # or they run without a Context, whose creation allocates the batch buffers).
-# Its scratch is a fixed 5.1 MiB device array inside the library, shared by
+# Its scratch is a fixed 5.6 MiB device array inside the library, shared by
 # all calls: calls that overlap on the GPU race. The first call on a device
 # looks the array up; make it before any stream capture.
 

@@ -160,30 +160,26 @@ __global__ void __launch_bounds__(WARPS * 32, (8 / WARPS) * MINB) k_probe(DevInd
     uint32_t *keys = s_keys[w];  // the tile's keys (a sub-range of the decoded segment when tiles are cut)
     uint32_t *mbuf = s_merge[w];
     ListDesc &L = s_list[w];
-    // work order: the pack kernel's tile_order (heavy tiles first); after a
-    // tile overflow (reported as kErrCapacity) tile_order may have holes, so
-    // the tiles that fit are taken in id order instead
-    const uint32_t Tall = b.tile_prefix[b.nq];
-    const uint32_t T = min(Tall, b.max_tiles);
+    // work order: the pack kernel writes one record {tile, query, tile within
+    // the query, shortest list} per tile into tile_order, heavy tiles from the
+    // front, the others from the back. The records fill the first H and the
+    // last T - H slots exactly, also after a tile overflow (reported as
+    // kErrCapacity), where T is capped at max_tiles and the slots fill up.
+    const uint32_t T = min(b.tile_prefix[b.nq], b.max_tiles);
     const uint32_t H = min(b.tile_prefix[b.nq + 1], T);
-    const bool ordered = Tall <= b.max_tiles;
     uint32_t probes = 0, fallbacks = 0, nkeys = 0, merges = 0;
     for (;;) {
-        uint32_t t = 0;
-        if (lane == 0) {
-            const uint32_t wi = atomicAdd(b.tile_counter, 1u);
-            t = wi >= T || !ordered ? wi : b.tile_order[wi < H ? wi : b.max_tiles - 1u - (wi - H)];
-        }
-        t = __shfl_sync(0xffffffffu, t, 0);
-        if (t >= T) break;
-        const uint32_t q = b.tile_q[t];  // owner written by the pack kernel
-        // the query's sorted terms (lane j holds term j), first tile, term
-        // count and key base: one round of independent loads
+        uint32_t wi = 0;
+        if (lane == 0) wi = atomicAdd(b.tile_counter, 1u);
+        wi = __shfl_sync(0xffffffffu, wi, 0);
+        if (wi >= T) break;
+        const uint4 wr = b.tile_order[wi < H ? wi : b.max_tiles - 1u - (wi - H)];
+        const uint32_t t = wr.x, q = wr.y, ti = wr.z, list0 = wr.w;
+        // the query's sorted terms (lane j holds term j), term count, key base
+        // and the shortest list's descriptor: one round of independent loads
         const uint32_t tq = b.qterms[(size_t)q * kMaxTerms + lane];
-        const uint32_t ti = t - b.tile_prefix[q];
         const uint32_t k = b.qnterms[q];
         const uint32_t kbase = b.key_base[q];
-        const uint32_t list0 = __shfl_sync(0xffffffffu, tq, 0);
         __syncwarp();
         if (lane < 5) reinterpret_cast<uint4 *>(&L)[lane] = reinterpret_cast<const uint4 *>(ix.lists + list0)[lane];
         __syncwarp();
@@ -196,7 +192,8 @@ __global__ void __launch_bounds__(WARPS * 32, (8 / WARPS) * MINB) k_probe(DevInd
             // decoded (d-gaps need its prefix) and the part's keys probed
             const uint32_t sp = tile_split_of(L.log2_block, b.tile_split);
             const uint32_t sg = L.seg_base + (ti >> sp);
-            const uint32_t cnt = ix.seg_rec[sg].count;
+            // fixed blocks: every segment but the last holds 2^log2_block postings
+            const uint32_t cnt = min(1u << L.log2_block, L.n - ((ti >> sp) << L.log2_block));
             const uint32_t sub = (1u << L.log2_block) >> sp, e0 = (ti & ((1u << sp) - 1u)) * sub;
             first_elem = ((ti >> sp) << L.log2_block) + e0;
             warp_decode<KIND>(ix, L, sg, 0, cnt, keys, lane);

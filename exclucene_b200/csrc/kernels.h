@@ -14,9 +14,9 @@ struct BatchView {
     const uint32_t *qterms;      // nq * kMaxTerms list ids, ascending length
     const uint32_t *qnterms;     // terms per query
     const uint32_t *tile_prefix; // nq + 1, exclusive prefix of tiles per query
-    uint32_t *tile_q;            // max_tiles, query owning each tile
-    uint32_t *tile_order;        // max_tiles, probe order: heavy tiles from the front, the rest from the back
-                                 // (tile_prefix[nq + 1] = heavy tiles)
+    uint32_t *tile_q;            // max_tiles, scratch of k_scatter (each tile's output position)
+    uint4 *tile_order;           // max_tiles work records {tile, query, tile within the query, shortest list}:
+                                 // heavy tiles from the front, the rest from the back (tile_prefix[nq + 1] = heavy tiles)
     uint32_t *tile_counter;      // work-queue head (zeroed by k_pack_scan)
     const uint32_t *key_base;    // nq + 1, exclusive prefix of shortest-list lengths
     uint32_t *tile_count;        // survivors per tile

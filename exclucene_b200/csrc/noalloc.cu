@@ -12,7 +12,7 @@
 //
 // Limits: at most EXCL_NOALLOC_MAX_QUERIES queries per call and at most
 // EXCL_NOALLOC_MAX_KEYS docIDs summed over the queries' shortest lists. The
-// array takes 5,392,896 bytes (5.1 MiB) on every GPU that loads the library,
+// array takes 5,835,264 bytes (5.6 MiB) on every GPU that loads the library,
 // until the process exits.
 //
 // Sharing: every call uses the same array and it keeps the last call's
@@ -47,13 +47,13 @@ constexpr uint64_t kOffTileQ = kOffKeyBase + up64(kNAQueries + 2);
 constexpr uint64_t kOffTileCount = kOffTileQ + up64(kNATiles + 1);
 constexpr uint64_t kOffTileSlot = kOffTileCount + up64(kNATiles + 1);
 constexpr uint64_t kOffTileOrder = kOffTileSlot + up64(kNATiles + 1);
-constexpr uint64_t kOffSurvivors = kOffTileOrder + up64(kNATiles + 1);
+constexpr uint64_t kOffSurvivors = kOffTileOrder + up64(4 * ((uint64_t)kNATiles + 1));  // 16-byte work records
 constexpr uint64_t kOffMisc = kOffSurvivors + up64(kNAKeys);
 constexpr uint64_t kOffStats = kOffMisc + 64;           // 3 x u64 counters
 constexpr uint64_t kWords = kOffStats + 64;
 static_assert(sizeof(PackSync) <= 4 * (kOffChunkState - kOffSync), "pack state region");
 static_assert(2 * (kNATiles / kSSChunk + 2) <= kOffTilePrefix - kOffChunkState, "chunk state region");
-static_assert(kWords * 4 == 5392896, "scratch size stated in the comments and excl_gpu.h");
+static_assert(kWords * 4 == 5835264, "scratch size stated in the comments and excl_gpu.h");
 
 static __device__ __align__(256) uint32_t g_noalloc_scratch[kWords];
 
@@ -115,7 +115,7 @@ extern "C" int excl_intersect_device_noalloc(excl_index *ix, const uint32_t *d_t
     b.key_base = base + kOffKeyBase;
     b.tile_count = base + kOffTileCount;
     b.tile_slot = base + kOffTileSlot;
-    b.tile_order = base + kOffTileOrder;
+    b.tile_order = reinterpret_cast<uint4 *>(base + kOffTileOrder);
     b.scratch = base + kOffSurvivors;
     b.max_tiles = kNATiles;
     b.merge_segs = 2;

@@ -165,7 +165,8 @@ __global__ void __launch_bounds__(kPackThreads) k_pack_scan(const ListDesc *__re
                                                             const uint32_t *toff,   // coherent loads only
                                                             uint32_t nq,
                                                             BatchView b, PackSync *__restrict__ sync) {
-    __shared__ uint32_t s_sc[3][33], s_pre[3], s_et[kPackThreads], s_eh[kPackThreads], s_h[kPackThreads], s_id, s_tag;
+    __shared__ uint32_t s_sc[3][33], s_pre[3], s_et[kPackThreads], s_eh[kPackThreads], s_h[kPackThreads],
+        s_l0[kPackThreads], s_id, s_tag;
     // the probe kernel may launch now (it waits for this grid's results);
     // this grid reads the batch's queries only, and (when launched after
     // another batch on this stream) the shared scan state once that batch ends
@@ -178,7 +179,7 @@ __global__ void __launch_bounds__(kPackThreads) k_pack_scan(const ListDesc *__re
     __syncthreads();
     const uint32_t bid = s_id, tag = s_tag;
     const uint32_t q = bid * blockDim.x + threadIdx.x;
-    uint32_t nt = 0, nk = 0, lb0 = 0;
+    uint32_t nt = 0, nk = 0, lb0 = 0, l0 = 0;
     if (q < nq) {
         const uint32_t t0 = toff[q], t1 = toff[q + 1];
         uint32_t k = t1 >= t0 ? t1 - t0 : 0u;
@@ -222,6 +223,7 @@ __global__ void __launch_bounds__(kPackThreads) k_pack_scan(const ListDesc *__re
             nt = k ? ntl[0] : 0u;
             nk = k ? len[0] : 0u;
             lb0 = k ? lbl[0] : 0u;
+            l0 = k ? id[0] : 0u;
         } else {
             uint32_t id[kMaxTerms], len[kMaxTerms];
             bool bad = false;
@@ -259,6 +261,7 @@ __global__ void __launch_bounds__(kPackThreads) k_pack_scan(const ListDesc *__re
             lb0 = k ? __ldg(&lists[id[0]].log2_block) : 0u;
             nt = k ? split_tiles(len[0], __ldg(&lists[id[0]].ntiles), lb0, b.tile_split) : 0u;
             nk = k ? len[0] : 0u;
+            l0 = k ? id[0] : 0u;
         }
         const_cast<uint32_t *>(b.qnterms)[q] = k;
     }
@@ -325,6 +328,7 @@ __global__ void __launch_bounds__(kPackThreads) k_pack_scan(const ListDesc *__re
     s_et[threadIdx.x] = et;
     s_eh[threadIdx.x] = ex[2];
     s_h[threadIdx.x] = nh;
+    s_l0[threadIdx.x] = l0;
     __syncthreads();
     const uint32_t pt = s_pre[0];
     if (threadIdx.x == 0) {
@@ -354,8 +358,8 @@ __global__ void __launch_bounds__(kPackThreads) k_pack_scan(const ListDesc *__re
     }
     // owner of each of this CTA's tiles: the last query whose first tile is
     // at or before it (queries with no tiles share their successor's start);
-    // and the tile's place in the probe order: heavy tiles from the front in
-    // query order, the others from the back of tile_order
+    // its work record goes to its place in the probe order: heavy tiles from
+    // the front in query order, the others from the back of tile_order
     // (a thread's tiles ascend, so its owners do too: the search resumes from
     // the last owner, and a run of one query's tiles costs one check each)
     const uint32_t ph = s_pre[2];
@@ -371,9 +375,9 @@ __global__ void __launch_bounds__(kPackThreads) k_pack_scan(const ListDesc *__re
             }
         }
         const uint32_t t = pt + tl, i = tl - s_et[lo], hb = ph + s_eh[lo];
-        b.tile_q[t] = bid * blockDim.x + lo;
-        if (i < s_h[lo]) b.tile_order[hb + i] = t;
-        else b.tile_order[b.max_tiles - 1u - (t - hb - s_h[lo])] = t;
+        const uint4 wr = make_uint4(t, bid * blockDim.x + lo, i, s_l0[lo]);
+        if (i < s_h[lo]) b.tile_order[hb + i] = wr;
+        else b.tile_order[b.max_tiles - 1u - (t - hb - s_h[lo])] = wr;
     }
 }
 

@@ -423,7 +423,8 @@ extern "C" int excl_ctx_destroy(excl_ctx *ctx) {
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     uint32_t *bufs[] = {ctx->d_terms,   ctx->d_toff, ctx->d_qterms,   ctx->d_qnterms,   ctx->d_tile_prefix,
                         ctx->d_tile_q,  ctx->d_tile_count, ctx->d_scratch, ctx->d_misc, ctx->d_key_base,
-                        ctx->d_tile_slot, ctx->d_tile_order, ctx->d_offsets, ctx->d_docids};
+                        ctx->d_tile_slot, reinterpret_cast<uint32_t *>(ctx->d_tile_order), ctx->d_offsets,
+                        ctx->d_docids};
     for (uint32_t *p : bufs) cudaFree(p);
     if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
     cudaFree(ctx->d_stats);

@@ -61,7 +61,8 @@ struct excl_ctx {
     uint32_t *d_terms = nullptr, *d_toff = nullptr;
     uint32_t *d_qterms = nullptr, *d_qnterms = nullptr, *d_tile_prefix = nullptr, *d_tile_q = nullptr;
     uint32_t *d_tile_count = nullptr, *d_scratch = nullptr, *d_misc = nullptr;
-    uint32_t *d_key_base = nullptr, *d_tile_slot = nullptr, *d_tile_order = nullptr;
+    uint32_t *d_key_base = nullptr, *d_tile_slot = nullptr;
+    uint4 *d_tile_order = nullptr;
     excl::PackSync *d_sync = nullptr;
     uint64_t *d_stats = nullptr, *d_chunk_state = nullptr;
     uint32_t *d_offsets = nullptr, *d_docids = nullptr;

@@ -67,7 +67,7 @@ WsLayout ws_layout(uint64_t nq, uint64_t /*nterms*/, uint64_t tiles, uint64_t ke
     L.tile_q = take(tiles + 1);
     L.tile_count = take(tiles + 1);
     L.tile_slot = take(tiles + 1);
-    L.tile_order = take(tiles + 1);
+    L.tile_order = take(4 * (tiles + 1));
     L.scratch = take(keys);
     L.total = o;
     return L;
@@ -247,7 +247,7 @@ int launch_on_slot(excl_server *s, Slot *sl, uint64_t nterms, uint64_t tiles, ui
     b.key_base = at(L.key_base);
     b.tile_count = at(L.tile_count);
     b.tile_slot = at(L.tile_slot);
-    b.tile_order = at(L.tile_order);
+    b.tile_order = reinterpret_cast<uint4 *>(at(L.tile_order));
     b.scratch = at(L.scratch);
     b.max_tiles = (uint32_t)tiles;
     b.merge_segs = 2;

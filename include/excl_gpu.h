@@ -266,7 +266,7 @@ int excl_ctx_check(excl_ctx *ctx);
  * reference. For callers that cannot call cudaMalloc when they query (a host
  * that fixes its device memory budget at start-up, or an embedding without an
  * excl_ctx, whose creation allocates the batch buffers): the per-batch scratch
- * lives in one fixed device array inside the library (5.1 MiB on every GPU that
+ * lives in one fixed device array inside the library (5.6 MiB on every GPU that
  * loads it, held until the process exits), so the call allocates nothing.
  * The index must already be uploaded, on the current device. The caller passes
  * the inputs and outputs as device pointers and the cudaStream_t to run on;
