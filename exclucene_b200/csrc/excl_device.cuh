@@ -281,9 +281,18 @@ __device__ __forceinline__ void warp_decode(const DevIndexView &ix, const ListDe
                                             uint32_t kc, uint32_t *buf, uint32_t lane) {
     const bool dgap = KIND == kKindDgap || (KIND == kKindAny && codec_is_dgap(L.codec));
     const bool newpfd = KIND == kKindAny && codec_is_newpfd(L.codec);
-    const SegRec rec = ix.seg_rec[sg];
+    // the segment's 64-byte probe record: head, block offset, aux, count,
+    // descriptor, regression and list position, all in one round trip (no
+    // dependent load of the block's descriptor word before its bits)
+    const uint4 *prv = reinterpret_cast<const uint4 *>(ix.seg_probe + sg);
+    const uint4 p0 = __ldg(prv), p1 = __ldg(prv + 1), p2 = __ldg(prv + 2);
+    SegRec rec;
+    rec.off = p0.y;
+    rec.aux = p0.z;
+    rec.count = p0.w;
+    rec.start = p2.x;
     const uint32_t *blk = ix.words + L.word_base + rec.off;
-    const BlkHdr h = blk_hdr(ldg(blk));
+    const BlkHdr h = blk_hdr(p1.x);
     const uint32_t vpl = (kc + 31u) >> 5;
     const uint32_t el = lane * vpl;
     uint32_t v[8];
@@ -314,7 +323,7 @@ __device__ __forceinline__ void warp_decode(const DevIndexView &ix, const ListDe
         __syncwarp();
     }
     if (dgap) {
-        if (lane == 0 && e0 == 0) v[0] = ix.seg_head[sg];
+        if (lane == 0 && e0 == 0) v[0] = p0.x;
         uint32_t run = 0;
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
@@ -331,7 +340,10 @@ __device__ __forceinline__ void warp_decode(const DevIndexView &ix, const ListDe
 #pragma unroll
         for (int j = 0; j < 8; ++j) v[j] += excl;
     } else {
-        const ResidParams rp = resid_params(L, rec, ix.seg_reg[sg]);
+        SegReg reg;
+        reg.a = __uint_as_float(p1.y);
+        reg.b = __uint_as_float(p1.z);
+        const ResidParams rp = resid_params(L, rec, reg);
 #pragma unroll
         for (int j = 0; j < 8; ++j) v[j] = resid_value(rp, e0 + el + j, v[j]);
     }
