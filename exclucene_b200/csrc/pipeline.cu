@@ -383,37 +383,10 @@ __global__ void __launch_bounds__(kPackThreads) k_pack_scan(const ListDesc *__re
 
 // ---------------------------------------------------------------------------
 
-// One warp finds two lower bounds in a[0, n) (first i with a[i] >= x, n if
-// none): lanes 0-15 search x1, lanes 16-31 x2, each a 16-way split per round.
-__device__ __forceinline__ void warp_lower_bound2(const uint32_t *a, uint32_t n, uint32_t x1, uint32_t x2,
-                                                  uint32_t &r1, uint32_t &r2) {
-    const uint32_t lane = threadIdx.x & 31u, sub = lane & 15u;
-    const uint32_t half = lane >> 4 ? 0xffff0000u : 0x0000ffffu;
-    const uint32_t x = lane >> 4 ? x2 : x1;
-    uint32_t lo = 0, hi = n;
-    while (__any_sync(0xffffffffu, lo < hi)) {
-        const uint32_t len = hi - lo;
-        const uint32_t step = (len + 15u) >> 4;
-        const uint32_t m = step ? (len + step - 1u) / step : 0u;  // probes inside [lo, hi)
-        const uint32_t pos = lo + sub * step;
-        const bool pred = sub < m && a[pos] < x;
-        const uint32_t k = __popc(__ballot_sync(0xffffffffu, pred) & half);
-        if (lo < hi) {
-            const uint32_t nlo = k ? lo + (k - 1u) * step + 1u : lo;
-            const uint32_t nhi = k < m ? lo + k * step : hi;
-            lo = nlo;
-            hi = nhi;
-        }
-    }
-    r1 = __shfl_sync(0xffffffffu, lo, 0);
-    r2 = __shfl_sync(0xffffffffu, lo, 16);
-}
-
 // Phase A (CTAs holding a chunk ticket): survivor total of the chunk,
 // decoupled look-back for its base, the absolute output position of each of
-// its tiles (into tile_q, free once the probe kernel is done) and the offsets
-// of the queries starting in it; then the chunk's inclusive prefix is
-// published. Phase B (every warp of the grid, once all chunk tickets are
+// its tiles (into tile_q, free once the probe kernel is done); then the
+// chunk's inclusive prefix is published. Phase B (every warp of the grid, once all chunk tickets are
 // taken, so every chunk is owned by a running CTA): survivors copied tile by
 // tile, each tile after its chunk's prefix is out; a warp gathers the
 // bookkeeping of 32 of its tiles at once.
@@ -429,9 +402,8 @@ __global__ void __launch_bounds__(kSSThreads) k_scatter(BatchView b, PackSync *_
                                                         uint64_t *__restrict__ chunk_state,
                                                         uint32_t *__restrict__ offsets,
                                                         uint32_t *__restrict__ docids, uint64_t cap) {
-    __shared__ uint32_t s_out[kSSChunk + 1];  // output position of each tile of the chunk, within the chunk
     __shared__ uint32_t sa[33], sb[33];
-    __shared__ uint32_t s_c, s_base, s_qlo, s_qhi;
+    __shared__ uint32_t s_c, s_base;
     constexpr uint32_t kPer = kSSChunk / kSSThreads;
     static_assert(kPer == 2, "two tiles per thread");
     pdl_launch_dependents();
@@ -492,28 +464,11 @@ __global__ void __launch_bounds__(kSSThreads) k_scatter(BatchView b, PackSync *_
                 p -= 32;
             }
             if (lane == 0) s_base = excl;
-        } else if (w == 1) {
-            // meanwhile: the queries whose first tile lies in this chunk (the
-            // last chunk also takes the end offset and queries starting at T)
-            uint32_t qlo, qhi;
-            warp_lower_bound2(b.tile_prefix, nq + 1, t0, t0 + kSSChunk, qlo, qhi);
-            if (lane == 0) {
-                s_qlo = qlo;
-                s_qhi = c == nch - 1 ? nq + 1 : qhi;
-            }
         }
-        s_out[threadIdx.x * kPer] = ex;
-        s_out[threadIdx.x * kPer + 1] = ex + c0;
-        if (threadIdx.x == 0) s_out[kSSChunk] = tot;
         __syncthreads();
         const uint32_t base = s_base;
         if (ta < T) tile_out[ta] = base + ex;
         if (ta + 1 < T) tile_out[ta + 1] = base + ex + c0;
-        const uint32_t qlo = s_qlo, qhi = s_qhi;
-        for (uint32_t qq = qlo + threadIdx.x; qq < qhi; qq += blockDim.x) {
-            const uint32_t lt = min(b.tile_prefix[qq], T) - t0;
-            offsets[qq] = base + s_out[min(lt, kSSChunk)];
-        }
         if (c == nch - 1 && threadIdx.x == 0 && (uint64_t)base + tot > cap) atomicOr(b.err, kErrCapacity);
         __syncthreads();  // tile positions written before the prefix goes out
         if (threadIdx.x == 0) {
@@ -527,6 +482,24 @@ __global__ void __launch_bounds__(kSSThreads) k_scatter(BatchView b, PackSync *_
     // count, its chunk's prefix (bounded wait), its output position and slot,
     // all lanes at once; then the warp copies the non-empty tiles one after
     // another, eight independent loads per lane.
+    // the query offsets: the output position of each query's first tile, or
+    // for a query with no tile after it, the batch's total (the last chunk's
+    // inclusive prefix); each once its chunk's prefix is out
+    for (uint32_t qq = blockIdx.x * blockDim.x + threadIdx.x; qq <= nq; qq += gridDim.x * blockDim.x) {
+        const uint32_t tp = min(b.tile_prefix[qq], T);
+        const uint32_t c = tp < T ? tp / kSSChunk : nch - 1u;
+        uint64_t s = ld_acquire64(&chunk_state[c]);
+        uint32_t spins = 0;
+        while ((uint32_t)(s >> 34) != tag || ((uint32_t)(s >> 32) & 3u) != kPrefix) {
+            if (++spins > kSpin) {
+                atomicOr(b.err, kErrScanSpin);
+                break;
+            }
+            __nanosleep(64);
+            s = ld_acquire64(&chunk_state[c]);
+        }
+        offsets[qq] = tp < T ? ld_acquire(&tile_out[tp]) : (uint32_t)s;
+    }
     const uint32_t gw = blockIdx.x * (kSSThreads / 32) + w, nw = gridDim.x * (kSSThreads / 32);
     const uint32_t *__restrict__ scr = b.scratch;
     for (uint64_t j0 = 0; gw + j0 * nw < T; j0 += 32) {
