@@ -34,7 +34,7 @@ FALLBACK_HBM_GBS = 6650.0
 
 # dram__bytes_read.sum + dram__bytes_write.sum of one k_probe launch (hash-directory search) on
 # the full-size workload, from one ncu --set full capture of this same bench command
-NCU_PROBE_TRAFFIC = {"zipf": 44.78e6}
+NCU_PROBE_TRAFFIC = {"zipf": 45.18e6}
 
 
 def parse():
