@@ -101,6 +101,32 @@ def test_invalid_batches_raise(gpu_ctx, corpus):
     ix.close()
 
 
+def test_tile_overflow_reports_capacity(corpus):
+    """A batch with more tiles (and shortest-list docIDs) than a small context
+    holds fails with EXCL_E_CAPACITY: the pack kernel's work order then covers
+    only the tiles that fit, and nothing runs past the buffers. The context
+    answers the next batch exactly."""
+    ix = _index(corpus, "seglrc")
+    ctx = ex.Context(0, max_queries=8, max_keys=2048)  # room for 2048/32 + 8 + 1 = 73 tiles
+    try:
+        ctx.upload(ix)
+        lens = np.diff(corpus.list_offsets).astype(np.int64)
+        order = np.argsort(lens, kind="stable")
+        longest = order[::-1][:4].astype(np.uint32)  # two pairs of the longest lists: hundreds of tiles each
+        assert lens[longest].min() > 256 * 80
+        with pytest.raises(ex.ExclError) as e:
+            ctx.intersect(ix, longest, np.array([0, 2, 4], np.uint32))
+        assert e.value.status == ex.api.E_CAPACITY
+        short = order[(lens[order] > 0) & (lens[order] <= 400)][:4].astype(np.uint32)
+        toff = np.array([0, 2, 4], np.uint32)
+        offs, docs = ctx.intersect(ix, short, toff)
+        eo, ed = oracle.answer(corpus.docs, corpus.list_offsets, short, toff)
+        assert np.array_equal(offs.astype(np.uint64), eo) and np.array_equal(docs, ed)
+    finally:
+        ctx.close()
+        ix.close()
+
+
 def test_batching_does_not_change_results(gpu_ctx, corpus, expected):
     ix = _index(corpus, "seglrc")
     gpu_ctx.upload(ix)
