@@ -2,7 +2,7 @@
 // and HS_ParaPFD formats: hash partition, regression fits, residuals and
 // minima, d-gaps and medians, and the ParaPFD blocks, with the same bytes as
 // the host build (codec.cpp), which restates the reference encoders
-// (ParaPFor.cpp:31-113, ParaPFD_Compression/main.cpp:163-189,
+// (ParaPFor.cpp:31-94, ParaPFD_Compression/main.cpp:163-189,
 // SegLRC_Generator.cu:190-331, LRC_Generator.cu:155-287,
 // LRCSeg_Generator.cu:160-215, HS_SegLRC_Generator.cu:180-594).
 //
@@ -359,7 +359,7 @@ __global__ void __launch_bounds__(kBuildWarps * 32) k_block_plan(const uint32_t 
         if (en) {
             p.eb = nbits_d(last);
             p.hb = nbits_d(orh);
-            // not representable in the descriptor (ParaPFor.cpp:79-88)
+            // not representable in the descriptor (ParaPFor.cpp:79-88: eb from the last position, hb from the highs, 5-bit fields)
             if (p.eb >= 32 || p.hb >= 32 || en > 0xffffu) {
                 if (lane == 0) atomicOr(err, kErrBuildFormat);
                 p.en = p.eb = p.hb = 0;

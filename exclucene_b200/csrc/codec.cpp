@@ -3,7 +3,7 @@
 // as the device-resident image (words + per-list + per-segment arrays).
 //
 // Bit-exactness notes
-//  * Block bytes follow ParaPFor.cpp:75-145 (descriptor lb<<26|eb<<21|hb<<16|en,
+//  * Block bytes follow ParaPFor.cpp:56-126 (descriptor lb<<26|eb<<21|hb<<16|en,
 //    LSB-first packing of lows, exception positions, exception high bits).
 //  * The regression fits follow the reference's double-precision host code
 //    (SegLRC_Generator.cu:264-331, LRC_Generator.cu:221-287). This file is
@@ -69,7 +69,7 @@ static void unpack_bits(const uint32_t *in, uint32_t n, uint32_t bits, uint32_t 
 }
 
 // Smallest b with #(v >= 2^b) satisfying (float)nEx <= frac * n in single
-// precision (ParaPFor.cpp:50-72), computed from a histogram of bit lengths.
+// precision (ParaPFor.cpp:31-53), computed from a histogram of bit lengths.
 static uint32_t best_b(const uint32_t *in, uint32_t n, float frac) {
     uint32_t hist[33] = {0};
     for (uint32_t i = 0; i < n; ++i) ++hist[nbits(in[i])];

@@ -208,7 +208,7 @@ constexpr uint32_t kLgRuntime = 8;
 // lanes storing runs of 2, 4 or 8 consecutive values hit distinct banks.
 __device__ __forceinline__ uint32_t sw(uint32_t i) { return i + (i >> 5); }
 
-// Exceptions of a staged block (ParaPFor.cpp:116-125): the G = 2^lg lanes of
+// Exceptions of a staged block (ParaPFor.cpp:112-123): the G = 2^lg lanes of
 // a group patch the high bits of the listed positions into the group's
 // values, element i at vals[sw(base + i)]. Positions are distinct, so the
 // lanes never write the same word.

@@ -115,7 +115,7 @@ struct BlkHdr {
     uint32_t lb, eb, hb, en;
 };
 
-// ParaPFor.cpp:121-125 descriptor fields.
+// ParaPFor.cpp:102-106 descriptor fields.
 __device__ __forceinline__ BlkHdr blk_hdr(uint32_t d) {
     BlkHdr h;
     h.lb = (d >> 26) & 31u;

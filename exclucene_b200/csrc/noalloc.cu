@@ -49,7 +49,7 @@ constexpr uint64_t kOffTileSlot = kOffTileCount + up64(kNATiles + 1);
 constexpr uint64_t kOffTileOrder = kOffTileSlot + up64(kNATiles + 1);
 constexpr uint64_t kOffSurvivors = kOffTileOrder + up64(4 * ((uint64_t)kNATiles + 1));  // 16-byte work records
 constexpr uint64_t kOffMisc = kOffSurvivors + up64(kNAKeys);
-constexpr uint64_t kOffStats = kOffMisc + 64;           // 3 x u64 counters
+constexpr uint64_t kOffStats = kOffMisc + 64;           // 4 x u64 counters (probes, fallbacks, keys, merges)
 constexpr uint64_t kWords = kOffStats + 64;
 static_assert(sizeof(PackSync) <= 4 * (kOffChunkState - kOffSync), "pack state region");
 static_assert(2 * (kNATiles / kSSChunk + 2) <= kOffTilePrefix - kOffChunkState, "chunk state region");
@@ -65,14 +65,17 @@ int g_nsm[kMaxDevices];
 // First call on a device (with that device current): look up the device
 // address of the array. The host-side name g_noalloc_scratch is only a
 // stand-in, never a device address, so kernels get this pointer instead.
-int setup_device(int dev, uint32_t **base, int *nsm) {
+// The batch pipeline's cross-CTA state must start zeroed (its tags start at
+// 1). A file-scope device array is zero when the module loads; the state is
+// cleared once more here, on the caller's stream so the clear is ordered
+// before this first batch, in case the array was used before the lookup.
+int setup_device(int dev, cudaStream_t st, uint32_t **base, int *nsm) {
     std::lock_guard<std::mutex> g(g_mu);
     if (!g_base[dev]) {
         void *p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess || !p) return EXCL_E_CUDA;
-        // the batch pipeline's cross-CTA state starts zeroed (its tags start at 1)
-        e = cudaMemset(static_cast<uint32_t *>(p) + kOffSync, 0, 4 * (kOffTilePrefix - kOffSync));
+        e = cudaMemsetAsync(static_cast<uint32_t *>(p) + kOffSync, 0, 4 * (kOffTilePrefix - kOffSync), st);
         if (e != cudaSuccess) return EXCL_E_CUDA;
         int n = 0;
         e = cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
@@ -99,11 +102,11 @@ extern "C" int excl_intersect_device_noalloc(excl_index *ix, const uint32_t *d_t
     int dev = -1;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return EXCL_E_CUDA;
     if (dev != ix->dev->device) return EXCL_E_INVALID;  // the index lives on another device
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
     uint32_t *base = nullptr;
     int nsm = 0;
-    int s = setup_device(dev, &base, &nsm);
+    int s = setup_device(dev, st, &base, &nsm);
     if (s) return s;
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
 
     BatchView b{};
     b.nq = nq;

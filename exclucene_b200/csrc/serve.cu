@@ -317,7 +317,8 @@ void dispatch_loop(excl_server *s) {
         if (sl->batch.empty()) continue;
         const uint64_t ws = ws_layout(sl->batch.size(), nterms, tiles, keys).total;
         if (!s->pool.alloc(ws, &sl->pool_off)) {  // cannot happen: ws <= largest free block
-            for (auto &r : sl->batch) s->queue.push_front(r);
+            // back to the queue head in their original (FIFO) order
+            for (auto it = sl->batch.rbegin(); it != sl->batch.rend(); ++it) s->queue.push_front(*it);
             sl->batch.clear();
             continue;
         }

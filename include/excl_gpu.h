@@ -33,7 +33,7 @@ typedef enum {
 } excl_status;
 
 /* List formats (one codec per list). Block bytes are the reference ParaPFD
- * layout (ParaPFor.cpp:75-113); see excl_build_params for the segmentation. */
+ * layout (ParaPFor.cpp:56-94); see excl_build_params for the segmentation. */
 typedef enum {
     EXCL_CODEC_PARAPFD = 0,   /* d-gaps, ParaPFD blocks (ParaPFD_Compression/main.cpp:163-189) */
     EXCL_CODEC_LRC = 1,       /* list regression, int intercept (LRC_Generator.cu:155-287) */
@@ -56,7 +56,7 @@ typedef enum {
 /* ---------------------------------------------------------------------------
  * Codec calls — replace `uint32_t encodeArray(const uint32_t*, uint32_t*, uint32_t)`
  * and `decodeArray` (Compressed/include/ParaPFor.h:15-16). Reentrant; FRAC is an
- * argument instead of the global `float FRAC` (ParaPFor.cpp:38). Byte-identical
+ * argument instead of the global `float FRAC` (ParaPFor.cpp:19). Byte-identical
  * blocks. `cap` is the capacity of `out` in words. */
 int excl_parapfd_encode(const uint32_t *in, uint32_t n, float frac, uint32_t *out, size_t cap, size_t *words);
 int excl_parapfd_decode(const uint32_t *in, size_t nwords, uint32_t n, uint32_t *out, size_t *consumed);
@@ -103,7 +103,7 @@ int excl_index_free(excl_index *ix);
  * the ParaPFD blocks are computed by kernels on the context's device
  * (HS_SegLRC_Generator.cu:503-594, SegLRC_Generator.cu:94-436,
  * LRC_Generator.cu:96-287, LRCSeg_Generator.cu:98-215, ParaPFD_Compression/
- * main.cpp:163-189, ParaPFor.cpp:31-113; the reference runs the fits and the
+ * main.cpp:163-189, ParaPFor.cpp:31-94; the reference runs the fits and the
  * encoder on the host). Fits of lists longer than 65,536 postings run on host
  * threads, overlapped. d_docs is the CSR docID array in device memory; list l
  * is d_docs[list_offsets[l] .. list_offsets[l+1]) (list_offsets on the host,
@@ -276,7 +276,10 @@ int excl_ctx_check(excl_ctx *ctx);
  * lists (else EXCL_E_CAPACITY after the batch).
  * The first call on a device looks up the array's device address; make that
  * first call before any stream capture. All calls share the array: calls whose
- * work overlaps on the GPU race and must be serialised by the caller. */
+ * work overlaps on the GPU race and must be serialised by the caller.
+ * The call takes no context lock: the index must not be re-uploaded
+ * (excl_index_upload) or closed (excl_index_close) while a call that uses it
+ * is running, on any thread. */
 #define EXCL_NOALLOC_MAX_QUERIES 4096u
 #define EXCL_NOALLOC_MAX_KEYS (1u << 20)
 int excl_intersect_device_noalloc(excl_index *ix, const uint32_t *d_terms, const uint32_t *d_term_offsets,

@@ -18,8 +18,8 @@
  *                      term scorer lands on it exactly, and score() is
  *                      ConjunctionScorer::score() (sum times coord)
  *
- * Header only, no CUDA types; a CLucene subclass of Scorer that forwards to
- * GpuConjunction is shown in INTEGRATION.md. docIDs above INT32_MAX are not
+ * Header only, no CUDA types; a CLucene Scorer subclass binds it by
+ * forwarding next/skipTo/doc/score to a GpuConjunction. docIDs above INT32_MAX are not
  * representable in CLucene's int32_t doc(); doc() returns them cast, and
  * skipTo compares as unsigned.
  */

@@ -20,15 +20,22 @@ LIB = os.path.join(HERE, "liboracle.so")
 REF_CODEC = os.path.join(HERE, "_ref", "libparapfor_ref.so")
 REF_NEWPFD = os.path.join(HERE, "_ref", "libnewpfor_ref.so")
 REF_FIT = os.path.join(HERE, "_ref", "libfit_ref.so")
+# Root of the reference source tree used by the pinning builds and tests; the
+# EXCL_REFERENCE environment variable overrides the default location.
+REFERENCE = os.environ.get("EXCL_REFERENCE", "/root/reference")
+
+
+def have_reference_tree() -> bool:
+    return os.path.isdir(os.path.join(REFERENCE, "src", "gpu"))
 
 
 def build(ref: bool | None = None) -> None:
     """make -C oracle (and the reference builds when the reference tree exists)."""
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
     if ref is None:
-        ref = os.path.isdir("/root/reference/src/gpu")
+        ref = have_reference_tree()
     if ref:
-        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={REFERENCE}"], check=True)
 
 
 if not os.path.exists(LIB):

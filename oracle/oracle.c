@@ -60,7 +60,7 @@ static void or_unpack(const uint32_t *in, uint32_t *out, uint32_t bit, uint32_t 
     }
 }
 
-/* ParaPFor.cpp:50-72 (tryB / findBestB): smallest b in [0,32) whose exception
+/* ParaPFor.cpp:31-53 (tryB / findBestB): smallest b in [0,32) whose exception
  * count satisfies (float)nEx <= FRAC * n, evaluated in single precision. */
 static uint32_t or_find_best_b(const uint32_t *in, uint32_t n, float frac) {
     for (uint32_t b = 0; b < 32; ++b) {
@@ -72,7 +72,7 @@ static uint32_t or_find_best_b(const uint32_t *in, uint32_t n, float frac) {
     return 32;
 }
 
-/* ParaPFor.cpp:75-113 (encodeBlock). Returns words written, or 0 with *err set
+/* ParaPFor.cpp:56-94 (encodeBlock). Returns words written, or 0 with *err set
  * when the block is not representable by the descriptor (lb or hb = 32, or
  * more than 65535 exceptions). */
 uint32_t or_parapfd_encode_block(const uint32_t *in, uint32_t n, float frac, uint32_t *out, int *err) {
@@ -115,7 +115,7 @@ uint32_t or_parapfd_encode_block(const uint32_t *in, uint32_t n, float frac, uin
     return w;
 }
 
-/* ParaPFor.cpp:120-145 (decodeBlock). Returns words consumed. */
+/* ParaPFor.cpp:101-126 (decodeBlock). Returns words consumed. */
 uint32_t or_parapfd_decode_block(const uint32_t *in, uint32_t n, uint32_t *out) {
     uint32_t d = in[0];
     uint32_t lb = (d >> 26) % 32u, eb = (d >> 21) & 31u, hb = (d >> 16) & 31u, en = d & 65535u;

@@ -4,7 +4,7 @@
 
 #include "ParaPFor.h"
 
-extern float FRAC;  // ParaPFor.cpp:38
+extern float FRAC;  // ParaPFor.cpp:19
 
 extern "C" {
 void ref_set_frac(float f) { FRAC = f; }

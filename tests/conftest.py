@@ -7,8 +7,6 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
-REFERENCE = "/root/reference"
-
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")
@@ -21,14 +19,16 @@ def _ensure_built():
     b.build()
     import oracle
 
-    oracle.build(ref=os.path.isdir(os.path.join(REFERENCE, "src", "gpu")))
+    oracle.build(ref=oracle.have_reference_tree())
 
 
 _ensure_built()
 
 
 def have_reference() -> bool:
-    return os.path.isdir(os.path.join(REFERENCE, "src", "gpu"))
+    import oracle
+
+    return oracle.have_reference_tree()
 
 
 @pytest.fixture(scope="session")

@@ -1,7 +1,8 @@
 """Writes tests/golden/*.npz from the reference's own code compiled from its
 sources (oracle/_ref: ParaPFor.cpp and the generators' getRegressionInfo).
 
-Run in a tree that has the reference sources at /root/reference:
+Run in a tree that has the reference sources (at EXCL_REFERENCE, default
+/root/reference):
     make -C oracle all ref && python tests/golden/make_golden.py
 The fixtures hold seeded synthetic inputs and the reference's outputs, so the
 checks that use them run anywhere (no reference tree needed).
@@ -18,7 +19,7 @@ import oracle  # noqa: E402
 
 OUT = os.path.dirname(os.path.abspath(__file__))
 FRACS = [0.0, 0.04, 0.08, np.float32(np.float32(0.04) + np.float32(0.04)) + np.float32(0.04), 0.1, 0.2, 0.64]
-INVERTED_LIST = "/root/reference/src/gpu/Preprocess/ExtractList/data/InvertedList"
+INVERTED_LIST = os.path.join(oracle.REFERENCE, "src/gpu/Preprocess/ExtractList/data/InvertedList")
 
 
 def codec_vectors():

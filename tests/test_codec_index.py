@@ -109,7 +109,7 @@ def test_index_build_uniform_wide_universe(cname, codec):
 
 def test_index_rejects_unrepresentable_gap():
     """A d-gap >= 2^31 needs b = 32, which the descriptor's 5-bit lb field cannot
-    hold (ParaPFor.cpp:107 stores lb << 26 and :122 reads it back modulo 32)."""
+    hold (ParaPFor.cpp:88 stores lb << 26 and :103 reads it back modulo 32)."""
     with pytest.raises(ex.ExclError) as e:
         ex.Index(np.array([0, 2 ** 32 - 8], np.uint32), np.array([0, 2], np.uint64), codec="parapfd")
     assert e.value.status == api.E_FORMAT

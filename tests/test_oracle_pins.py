@@ -74,7 +74,7 @@ def test_inverted_list_fixture_digest():
     """The reference's shipped list encodes to the digests recorded from the reference codec."""
     import hashlib
 
-    path = "/root/reference/src/gpu/Preprocess/ExtractList/data/InvertedList"
+    path = os.path.join(oracle.REFERENCE, "src/gpu/Preprocess/ExtractList/data/InvertedList")
     docs = np.fromfile(path, dtype=np.uint32)
     lines = [ln.split() for ln in open(os.path.join(GOLD, "inverted_list_digest.txt")) if ln.startswith("frac")]
     for _, frac, _, nw, _, h in lines:

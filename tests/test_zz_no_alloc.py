@@ -6,12 +6,14 @@ whose creation allocates). This file is collected last so that a run stopping
 at the first failure has already run every other test; it also passes alone.
 The entry point's results must equal excl_intersect_device's on the same
 batch, bit for bit (integer docIDs), on two calls in a row — the second call
-finds the first call's data in the shared scratch array.
+finds the first call's data in the shared scratch array — and both must equal
+the CPU oracle's exact AND of the batch.
 """
 import numpy as np
 import pytest
 
 import exclucene_b200 as ex
+import oracle
 from exclucene_b200 import api, synth
 
 pytestmark = pytest.mark.gpu
@@ -48,6 +50,9 @@ def _run_both(torch, w, ctx, ix, algo):
     ctx.check()
     ro = ref_offs.cpu().numpy()
     rd = ref_docs.cpu().numpy()[: int(ro[-1])]
+    # the allocating path against the CPU oracle's exact AND on the same batch
+    eo, ed = oracle.answer(w.docs, w.list_offsets, w.terms, w.term_offsets)
+    assert np.array_equal(ro.astype(np.uint64), eo) and np.array_equal(rd.view(np.uint32), ed)
     stream = torch.cuda.current_stream(dev)
     for call in range(2):
         offs = torch.full((w.nq + 1,), -1, dtype=torch.int32, device=dev)
@@ -58,6 +63,10 @@ def _run_both(torch, w, ctx, ix, algo):
         o = offs.cpu().numpy()
         assert np.array_equal(o, ro), f"offsets differ on call {call}"
         assert np.array_equal(docs.cpu().numpy()[: int(o[-1])], rd), f"docIDs differ on call {call}"
+        # and the no-alloc result itself against the oracle
+        assert np.array_equal(o.astype(np.uint64), eo), f"offsets differ from the oracle on call {call}"
+        assert np.array_equal(docs.cpu().numpy()[: int(o[-1])].view(np.uint32), ed), \
+            f"docIDs differ from the oracle on call {call}"
 
 
 @pytest.mark.parametrize("codec,algo", [("seglrc", "auto"), ("parapfd", "bsearch"), ("hs_parapfd", "hashseg")])
