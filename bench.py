@@ -1,17 +1,29 @@
 """Benchmark of the batched decode + AND-intersection path on B200.
 
-python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload zipf|pairs|skewed]
+python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                [--workload zipf|pairs|skewed|learned|serving] [--scale S]
 
 One step = one batch of the workload's queries through the device pipeline
 (pack -> scan -> persistent probe -> scan -> scatter), with the compressed
 index resident in HBM. Prints ONE JSON line on rank 0.
 
 Workloads (seeded synthetic stand-ins for the reference's Baidu/GOV2 data):
-  zipf    10M docs, 100k terms, df_r = min(5M, 5M/r) (~60.4M postings), SegLRC
-          (256-entry segments, FRAC 0), 10,000 queries of 2-5 terms ~ df^0.5
-  pairs   1,000 pairs of 4,096 / 1,048,576 uniform docIDs over 2^23, ParaPFD
-          blocks of 128, FRAC 0.10
-  skewed  2^26 universe, clustered-run lists, HS-bucketed ParaPFD, 5,000 queries
+  zipf     10M docs, 100k terms, df_r = min(5M, 5M/r) (~60.4M postings), SegLRC
+           (256-entry segments, FRAC 0), 10,000 queries of 2-5 terms ~ df^0.5
+  pairs    1,000 pairs of 4,096 / 1,048,576 uniform docIDs over 2^23, ParaPFD
+           blocks of 128, FRAC 0.10
+  skewed   2^26 universe, clustered-run lists, HS-bucketed ParaPFD, 5,000 queries
+  learned  64 clustered + 64 Zipf-gap long lists, 20,000 probe-key lists
+  serving  1e9 postings over 2M terms, ParaPFD / SegLRC by length, 100,000 queries
+
+Parity: the CPU oracle (oracle/, test infrastructure) is the checker. Before
+any timing it computes the exact AND of the batch; after each timed region the
+last result of that configuration is compared with it query by query, and the
+line's "parity" object reports the mismatches (the run exits 1 on any). The
+oracle also supplies the CPU baseline legs; it is never inside a timed GPU
+region. --impl reference runs only the oracle's CPU path, on inputs made by
+the oracle's own restatement of the workload generators and encoders, so that
+arm loads no library of the package.
 """
 from __future__ import annotations
 
@@ -59,16 +71,25 @@ def parse():
 # ---------------------------------------------------------------------------
 # workloads
 
-def make_workload(name: str, scale: float):
-    from exclucene_b200 import synth
-
+def make_workload(name: str, scale: float, gen=None, nq_factor: int = 1):
+    """The named workload at `scale`. `gen` supplies the generators: the
+    package's (GPU arm) or the oracle's restatement of the same seeded
+    generators (CPU reference arm, which loads no product code); both give the
+    same lists and queries bit for bit. `nq_factor` > 1 draws that many times
+    the queries from the same stream for the query-stream workloads (zipf,
+    serving: one batch per rank under --gpus N, the first being the
+    single-GPU batch); the list-per-query workloads ignore it (every rank runs
+    the same batch, so no rank holds other ranks' lists)."""
+    if gen is None:
+        from exclucene_b200 import synth as gen
+    synth = gen
     if name == "zipf":
         nt = max(1000, int(100_000 * scale))
         w = synth.zipf_corpus(ndocs=int(10_000_000 * max(scale, 0.01)), nterms=nt, cap=int(5_000_000 * scale),
-                              nq=max(100, int(10_000 * scale)), qmin=2, qmax=5)
+                              nq=max(100, int(10_000 * scale)) * nq_factor, qmin=2, qmax=5)
         return w, dict(codec="seglrc", block=256, frac=0.0), (
             f"zipf corpus: {int(10_000_000 * max(scale, 0.01))} docs, {nt} terms, df_r=min(cap,cap/r), "
-            f"{w.nq} queries of 2-5 terms ~ df^0.5; SegLRC 256-entry segments, FRAC 0")
+            f"{w.nq // nq_factor} queries of 2-5 terms ~ df^0.5; SegLRC 256-entry segments, FRAC 0")
     if name == "pairs":
         npairs = max(10, int(1000 * scale))
         w = synth.pairs(npairs=npairs)
@@ -91,7 +112,7 @@ def make_workload(name: str, scale: float):
     if name == "serving":
         total, nterms = int(1_000_000_000 * scale), max(1000, int(2_000_000 * scale))
         nq = max(1000, int(100_000 * min(scale * 10, 1.0)))
-        w = synth.serving(total=total, nterms=nterms, nq=nq)
+        w = synth.serving(total=total, nterms=nterms, nq=nq * nq_factor)
         return w, dict(codec="seglrc", block=256, frac=0.0, codecs=w.codecs), (
             f"serving corpus: {total:.2e} postings over {nterms} terms (Zipf(1) dfs, 2^28 universe), ParaPFD "
             f"below 1e4 postings else SegLRC; {nq} queries of 2-8 terms ~ df^0.5")
@@ -234,12 +255,30 @@ def cpu_run(w, img, seconds: float, threads: int):
     return t, n, postings * reps, reps
 
 
+def bench_config(w, params, desc) -> dict:
+    """The `config` object of both arms' JSON lines (identical for the same
+    workload): what one step processes, nothing about how."""
+    lens = np.diff(w.list_offsets).astype(np.int64)
+    return {"workload": desc, "codec": params["codec"] if "codecs" not in params else "parapfd+seglrc",
+            "block": params["block"], "frac": params["frac"], "queries_per_step": int(w.nq),
+            "postings_per_step": int(lens[w.terms.astype(np.int64)].sum()),
+            "l2": "GPU arm: flushed (512 MB read) before each timed step; CPU arm: n/a"}
+
+
 def reference_arm(args, w, desc, params):
-    import exclucene_b200 as ex
+    """The reference's CPU path (oracle port: ParaPFD/regression block decode +
+    exact AND) on the box's host cores. Its inputs come from the oracle's
+    restatement of the workload generators and its compressed index from the
+    oracle's block encoders (byte-pinned to the reference codec), so this arm
+    loads no library of the package under test."""
     import oracle
 
     threads = os.cpu_count() or 1
-    img = oracle.CompressedImage(ex.Index(w.docs, w.list_offsets, **params).export())
+    codecs = params.get("codecs")
+    img = oracle.encode_corpus(w.docs, w.list_offsets,
+                               codecs if codecs is not None else oracle.CODECS[params["codec"]],
+                               block=params["block"], frac=params["frac"], bucket=params.get("hs_bucket", 256),
+                               kbits=params.get("hs_kbits", 0), ubits=params.get("hs_ubits", 32))
     vals = []
     n = p = reps = 0
     for i in range(args.warmup + args.steps):
@@ -248,11 +287,12 @@ def reference_arm(args, w, desc, params):
             vals.append(p / t)
     v = float(np.median(vals))
     sample = (f"per step {reps} x the first {n} of {w.nq} queries; ParaPFD/regression decode + exact AND on "
-              f"the same compressed index (oracle port of the reference CPU path), {threads} threads")
+              f"the compressed index built by the oracle's encoders (oracle port of the reference CPU path), "
+              f"{threads} threads")
     line = {"metric": "postings/s", "value": v, "unit": "postings/s", "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-            "config": {"workload": desc},
+            "config": bench_config(w, params, desc),
             "cpu_baseline": {"value": v, "unit": "postings/s", "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": "postings/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -345,20 +385,38 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    w, params, desc = make_workload(args.workload, args.scale)
-    if args.codec:
-        params["codec"] = args.codec
-
     if args.impl == "reference":
+        # rank 0 alone, on the single-GPU batch; no product code is loaded
         if rank == 0:
+            import oracle
+
+            gen = type("OracleGen", (), {k[3:]: staticmethod(getattr(oracle, k)) for k in dir(oracle)
+                                         if k.startswith("wl_")})
+            w, params, desc = make_workload(args.workload, args.scale, gen)
+            if args.codec:
+                params["codec"] = args.codec
             reference_arm(args, w, desc, params)
         return
+
+    # under --gpus N the query-stream workloads draw N batches from one stream
+    # and rank r takes batch r (replicas.shard_queries); the others run the
+    # same batch on every rank. Either way each rank's batch is a full step.
+    import copy
 
     import torch
     import torch.distributed as dist
 
     import exclucene_b200 as ex
     from exclucene_b200 import replicas
+
+    stream_wl = args.workload in ("zipf", "serving")
+    wall, params, desc = make_workload(args.workload, args.scale, nq_factor=world if stream_wl else 1)
+    if args.codec:
+        params["codec"] = args.codec
+    w = wall
+    if world > 1 and stream_wl:
+        w = copy.copy(wall)
+        w.terms, w.term_offsets, _, _ = replicas.shard_queries(wall.terms, wall.term_offsets, rank, world)
 
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
@@ -438,7 +496,40 @@ def main():
         c.check()
         if world > 1:
             dist.barrier()
+        # outside the timed region: the last timed step's result against the oracle
+        offs_h = d_offs.cpu().numpy().astype(np.uint32)
+        parity[algo if c is ctx else algo + "/graph"] = mismatched_queries(
+            offs_h, d_docs[: int(offs_h[-1])].cpu().numpy().astype(np.uint32))
         return float(np.mean(tot)), float(np.mean(probe)), st
+
+    # The checker: the exact AND of this rank's batch by the CPU oracle,
+    # computed once before any timing; every timed configuration's last
+    # result is compared with it query by query after its timed region.
+    import oracle
+
+    ora_offs, ora_docs = oracle.answer_batch(w.docs, w.list_offsets, w.terms, w.term_offsets)
+    ora_cs = oracle.checksum(ora_offs, ora_docs)
+    parity = {}
+
+    def mismatched_queries(offs_h, docs_h) -> int:
+        o = offs_h.astype(np.uint64)
+        if len(o) != len(ora_offs):
+            return w.nq
+        if np.array_equal(o, ora_offs):
+            if len(ora_docs) == 0:
+                return 0
+            diff = (docs_h != ora_docs).astype(np.int64)
+            starts = ora_offs[:-1].astype(np.int64)
+            nonempty = np.diff(ora_offs) > 0
+            per_q = np.zeros(w.nq, dtype=np.int64)
+            per_q[nonempty] = np.add.reduceat(diff, starts[nonempty])
+            return int((per_q > 0).sum())
+        bad = 0
+        for q in range(w.nq):
+            a = docs_h[int(o[q]):int(o[q + 1])] if o[q + 1] >= o[q] else None
+            if a is None or not np.array_equal(a, ora_docs[int(ora_offs[q]):int(ora_offs[q + 1])]):
+                bad += 1
+        return bad
 
     postings = query_postings(w)
     algos = [args.algo] if args.algo else ["bsearch", "hashseg"] + ([] if args.no_learn else ["learned"])
@@ -462,15 +553,14 @@ def main():
         ms, launch_mode = per_algo_graph[best][0], "cuda graph"
     main_ctx = gctx if launch_mode == "cuda graph" else ctx
     best_algo = "auto" if best == "tuned" else best  # the tuned setting runs as algo=auto
-    # replicas: every rank ran the whole batch; the job time is the slowest rank's
+    # every rank ran a full batch; the job time is the slowest rank's and the
+    # job's work is the sum of the ranks' batches
     ms = replicas.max_over_ranks(ms, device=dev)
     pms = replicas.max_over_ranks(pms, device=dev)
-    value = world * postings / (ms / 1e3)
-
-    # checksum of the last device result (traceability)
-    offs_h = d_offs.cpu().numpy().astype(np.uint32)
-    docs_h = d_docs[: int(offs_h[-1])].cpu().numpy().astype(np.uint32)
-    cs = ex.checksum(offs_h, docs_h)
+    job_postings = replicas.sum_over_ranks(postings, device=dev)
+    job_queries = replicas.sum_over_ranks(w.nq, device=dev)
+    value = job_postings / (ms / 1e3)
+    cs = ora_cs
 
     # end to end through the public host API, inputs and results in host memory:
     # excl_submit_into (H2D of the queries from pinned memory; the last kernel
@@ -506,7 +596,9 @@ def main():
             tot = fn()
             e2e_t.append(time.perf_counter() - t0)
         e2e_ms[name] = replicas.max_over_ranks(float(np.mean(e2e_t)), device=dev) * 1e3
-    assert ex.checksum(p_off, p_docs[:tot]) == cs and ex.checksum(h_off, h_docs[:tot]) == cs
+    parity["e2e submit_into"] = mismatched_queries(np.asarray(p_off, dtype=np.uint32),
+                                                   np.asarray(p_docs[:tot], dtype=np.uint32))
+    parity["e2e submit_wait"] = mismatched_queries(h_off, h_docs[:tot])
     e2e_s = e2e_ms["submit_into"] / 1e3
     h2d = w.terms.nbytes + w.term_offsets.nbytes
     d2h = h_off.nbytes + 4 * tot
@@ -520,14 +612,21 @@ def main():
     serving = None
     if not args.no_serve:
         serving = serving_measure(ix, w, ["hashseg"] + ([] if args.no_learn else ["learned"]), local, cs)
+    if serving:
+        for a, res in serving["by_algo"].items():
+            parity[f"serving {a}"] = sum(0 if r["checksum_ok"] else 1 for r in res.values())
+    mism = int(replicas.sum_over_ranks(sum(parity.values()), device=dev))
+    parity_line = {"checked_queries": int(job_queries), "mismatches": mism,
+                   "per_run": parity, "oracle_checksum": list(ora_cs),
+                   "checker": "CPU oracle exact AND (oracle.answer_batch) of the same batch, per query; "
+                              "serving runs by result checksum"}
     line = {
         "metric": "postings/s", "value": value, "unit": "postings/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "config": {"workload": desc, "codec": params["codec"], "algo": best, "queries_per_step": w.nq,
-                   "postings_per_step": postings, "index_device_bytes": int(sizes.device_bytes),
-                   "index_postings": int(sizes.postings), "l2": "flushed (512 MB read) before each timed step"},
-        "queries_per_s": world * w.nq / (ms / 1e3),
+        "config": bench_config(w, params, desc),
+        "algo": best, "index_device_bytes": int(sizes.device_bytes), "index_postings": int(sizes.postings),
+        "queries_per_s": job_queries / (ms / 1e3),
         "launch": launch_mode,
         "per_algo_ms": {a: round(per_algo[a][0], 4) for a in per_algo},
         "per_algo_graph_ms": {a: round(per_algo_graph[a][0], 4) for a in per_algo_graph},
@@ -542,18 +641,19 @@ def main():
         "learned_models": learn,
         "index_build": index_build,
         "autotune": tune,
-        "per_algo_postings_per_s": {a: world * postings / (min(per_algo[a][0], per_algo_graph[a][0]) / 1e3)
+        "per_algo_postings_per_s": {a: job_postings / (min(per_algo[a][0], per_algo_graph[a][0]) / 1e3)
                                     for a in per_algo},
         "stats": {"tiles": int(st.tiles), "keys": int(st.keys), "probes": int(st.probes),
                   "fallbacks": int(st.fallbacks), "probe_ms": pms, "pack_ms": st.pack_ms,
                   "compact_ms": st.compact_ms},
         "checksum": list(cs),
+        "parity": parity_line,
         "roofline": {"bound": "hbm", "kernel": "k_probe", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak,
                      "traffic": NCU_PROBE_TRAFFIC.get(args.workload) if args.scale == 1.0 else None,
                      "traffic_note": "ncu dram read+write per k_probe launch, hash-directory search",
                      "algorithmic_bytes": algo_bytes, "peak_kind": peak_kind},
-        "e2e": {"value": world * postings / e2e_s, "unit": "postings/s", "h2d_bytes_per_step": int(h2d),
+        "e2e": {"value": job_postings / e2e_s, "unit": "postings/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_s * 1e3, "api": "excl_submit_into + excl_wait",
                 "ms_per_step_submit_wait": e2e_ms["submit_wait"],
                 "l2": "flushed before each step (outside the wall-clock region)"},
@@ -564,19 +664,26 @@ def main():
         "serving": serving,
     }
     if rank == 0 and world == 1 and not args.no_cpu:
-        import oracle
-
         threads = os.cpu_count() or 1
-        t, n, p, reps = cpu_run(w, oracle.CompressedImage(arrays), args.cpu_sample_s, threads)
+        img = oracle.encode_corpus(w.docs, w.list_offsets,
+                                   params["codecs"] if params.get("codecs") is not None
+                                   else oracle.CODECS[params["codec"]], block=params["block"], frac=params["frac"],
+                                   bucket=params.get("hs_bucket", 256), kbits=params.get("hs_kbits", 0),
+                                   ubits=params.get("hs_ubits", 32))
+        t, n, p, reps = cpu_run(w, img, args.cpu_sample_s, threads)
         line["cpu_baseline"] = {"value": p / t, "unit": "postings/s", "cores": threads, "kind": "port",
                                 "sample": f"{reps} x the first {n} of {w.nq} queries ({t:.1f} s); ParaPFD/regression "
-                                          "decode + exact AND on the same compressed index (oracle port)"}
+                                          "decode + exact AND on the index built by the oracle's encoders "
+                                          "(oracle port)"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     gctx.close()
     ctx.close()
     if world > 1:
         dist.destroy_process_group()
+    if mism:
+        sys.stderr.write(f"parity: {mism} queries differ from the oracle\n")
+        sys.exit(1)
 
 
 if __name__ == "__main__":

@@ -6,7 +6,8 @@ data-path collective. The process group is used only to line the ranks up
 around the timed region and to combine results for checking:
 
 - `shard_queries` gives a rank its contiguous block of a query stream;
-- `max_over_ranks` is the job time (the slowest rank);
+- `max_over_ranks` is the job time (the slowest rank), `sum_over_ranks`
+  the job's total work;
 - `combine_checksums` merges per-rank checksum triples into the triple of
   the whole stream (counts add, the docID fingerprint XORs), so a sharded
   run can be checked against a single-GPU run of the same queries.
@@ -37,6 +38,18 @@ def max_over_ranks(value: float, group=None, device=None) -> float:
         return float(value)
     t = torch.tensor([float(value)], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX, group=group)
+    return float(t[0])
+
+
+def sum_over_ranks(value: float, group=None, device=None) -> float:
+    """The sum of `value` over the ranks of the default (or given) group."""
+    import torch
+    import torch.distributed as dist
+
+    if not dist.is_initialized() or dist.get_world_size(group) == 1:
+        return float(value)
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
     return float(t[0])
 
 

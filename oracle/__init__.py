@@ -248,9 +248,12 @@ _runqc = _f(_lib, "or_run_queries_compressed", C.c_double, u32p, u32p, u32p, u32
 
 
 class CompressedImage:
-    """The arrays of an exported index, laid out for the compressed CPU path."""
+    """The arrays of a compressed index, laid out for the compressed CPU path:
+    from an exported index (`arrays`), or from encode_corpus (oracle encoder)."""
 
-    def __init__(self, arrays):
+    def __init__(self, arrays=None):
+        if arrays is None:
+            return
         L = arrays.lists
         self.words = np.ascontiguousarray(arrays.words, dtype=np.uint32)
         self.lcodec = np.ascontiguousarray(L["codec"], dtype=np.uint32)
@@ -451,3 +454,183 @@ def ref_fit_lrc_raw(y) -> np.ndarray:
     out = np.zeros(3, dtype=np.uint32)
     _rf().ref_fit_lrc(_p(y), len(y), _p(out))
     return out
+
+
+# ---------------------------------------------------------------------------
+# The benchmark's seeded workloads, restated here (workloads.c) so the CPU
+# reference arm needs no product code; whole-corpus encoding with this
+# oracle's encoders; exact answers of whole batches on host threads.
+
+_wl_new = {
+    "pairs": _f(_lib, "or_wl_pairs", C.c_void_p, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                C.c_uint32),
+    "zipf": _f(_lib, "or_wl_zipf_corpus", C.c_void_p, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+               C.c_uint32, C.c_uint32, C.c_uint32),
+    "skewed": _f(_lib, "or_wl_skewed", C.c_void_p, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                 C.c_uint32, C.c_uint32, C.c_uint32, C.c_double, C.c_double, C.c_uint32),
+    "learned": _f(_lib, "or_wl_learned", C.c_void_p, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                  C.c_uint32, C.c_double, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32),
+    "serving": _f(_lib, "or_wl_serving", C.c_void_p, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32,
+                  C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32),
+}
+_wl_free = _f(_lib, "or_wl_free", None, C.c_void_p)
+_wl_get = {n: _f(_lib, "or_wl_" + n, r, C.c_void_p) for n, r in (
+    ("ndocs", C.c_uint64), ("nlists", C.c_uint32), ("nqueries", C.c_uint32), ("nterms", C.c_uint64),
+    ("ninfo", C.c_uint32), ("docs", C.c_void_p), ("loff", C.c_void_p), ("terms", C.c_void_p), ("toff", C.c_void_p),
+    ("codecs", C.c_void_p), ("info", C.c_void_p))}
+
+
+class Workload:
+    """Concatenated sorted docID lists (list_offsets), queries (term_offsets)."""
+
+    def __init__(self, docs, list_offsets, terms, term_offsets, codecs, info):
+        self.docs, self.list_offsets, self.terms, self.term_offsets = docs, list_offsets, terms, term_offsets
+        self.codecs, self.info = codecs, info
+
+    @property
+    def nlists(self) -> int:
+        return len(self.list_offsets) - 1
+
+    @property
+    def nq(self) -> int:
+        return len(self.term_offsets) - 1
+
+    def list(self, i: int) -> np.ndarray:
+        return self.docs[self.list_offsets[i]:self.list_offsets[i + 1]]
+
+
+def _wl_arr(ptr, n, ct, dtype):
+    if n == 0 or not ptr:
+        return np.zeros(0, dtype=dtype)
+    return np.ctypeslib.as_array(C.cast(ptr, C.POINTER(ct)), shape=(n,)).copy()
+
+
+def _wl_take(h) -> Workload:
+    g = _wl_get
+    try:
+        nd, nl, nq, nt, ni = g["ndocs"](h), g["nlists"](h), g["nqueries"](h), g["nterms"](h), g["ninfo"](h)
+        cod = g["codecs"](h)
+        return Workload(_wl_arr(g["docs"](h), nd, C.c_uint32, np.uint32),
+                        _wl_arr(g["loff"](h), nl + 1, C.c_uint64, np.uint64),
+                        _wl_arr(g["terms"](h), nt, C.c_uint32, np.uint32),
+                        _wl_arr(g["toff"](h), nq + 1, C.c_uint32, np.uint32),
+                        _wl_arr(cod, nl, C.c_uint8, np.uint8) if cod else None,
+                        _wl_arr(g["info"](h), ni, C.c_double, np.float64))
+    finally:
+        _wl_free(h)
+
+
+def _threads(t: int) -> int:
+    return t if t > 0 else (os.cpu_count() or 1)
+
+
+def wl_pairs(seed=0xEC1E0001, npairs=1000, short_len=4096, long_len=1 << 20, ubits=23, threads=0) -> Workload:
+    return _wl_take(_wl_new["pairs"](seed, npairs, short_len, long_len, ubits, _threads(threads)))
+
+
+def wl_zipf_corpus(seed=0xEC1E0002, ndocs=10_000_000, nterms=100_000, cap=5_000_000, nq=10_000, qmin=2, qmax=5,
+                   threads=0) -> Workload:
+    return _wl_take(_wl_new["zipf"](seed, ndocs, nterms, cap, nq, qmin, qmax, _threads(threads)))
+
+
+def wl_skewed(seed=0xEC1E0003, ubits=26, npool=32, long_min=1_000_000, long_max=20_000_000, nq=5000,
+              short_min=1000, short_max=10_000, run_mean=64.0, gap_mean=4096.0, threads=0) -> Workload:
+    return _wl_take(_wl_new["skewed"](seed, ubits, npool, long_min, long_max, nq, short_min, short_max, run_mean,
+                                      gap_mean, _threads(threads)))
+
+
+def wl_learned(seed=0xEC1E0004, ubits=31, nclust=64, nzipf=64, lmin=10_000_000, lmax=100_000_000, zipf_s=1.2,
+               zipf_cap=1 << 20, nq=20_000, kmin=1000, kmax=100_000, threads=0) -> Workload:
+    return _wl_take(_wl_new["learned"](seed, ubits, nclust, nzipf, lmin, lmax, zipf_s, zipf_cap, nq, kmin, kmax,
+                                       _threads(threads)))
+
+
+def wl_serving(seed=0xEC1E0005, ubits=28, nterms=2_000_000, total=1_000_000_000, nq=100_000, qmin=2, qmax=8,
+               pfd_below=10_000, threads=0) -> Workload:
+    return _wl_take(_wl_new["serving"](seed, ubits, nterms, total, nq, qmin, qmax, pfd_below, _threads(threads)))
+
+
+_corpus_plan = _f(_lib, "or_corpus_plan", None, u32p, u64p, C.c_uint32, C.POINTER(C.c_uint8), C.c_uint32,
+                  C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, u32p)
+_corpus_enc = _f(_lib, "or_corpus_encode", C.c_int, u32p, u64p, C.c_uint32, C.POINTER(C.c_uint8), C.c_uint32,
+                 C.c_float, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, u32p, u64p, u64p, u32p, u32p, u32p, u32p,
+                 u32p, u32p)
+
+
+def encode_corpus(docs, list_offsets, codecs, block: int = 256, frac: float = 0.0, bucket: int = 256,
+                  kbits: int = 0, ubits: int = 32, threads: int = 0) -> CompressedImage:
+    """Every list encoded by this oracle's block encoders (per-list codec ids
+    as in CODECS, or one id for all), as the compressed CPU path's image."""
+    d = _u32(docs)
+    lo = np.ascontiguousarray(list_offsets, dtype=np.uint64)
+    nl = len(lo) - 1
+    cod = (np.full(nl, int(codecs), dtype=np.uint8) if np.isscalar(codecs)
+           else np.ascontiguousarray(codecs, dtype=np.uint8))
+    cp = cod.ctypes.data_as(C.POINTER(C.c_uint8))
+    th = _threads(threads)
+    nseg = np.zeros(max(nl, 1), dtype=np.uint32)
+    _corpus_plan(_p(d), _p(lo, u64p), nl, cp, block, bucket, kbits, ubits, th, _p(nseg))
+    nseg = nseg[:nl]
+    seg_base = np.zeros(nl + 1, dtype=np.uint64)
+    np.cumsum(nseg, out=seg_base[1:])
+    lens = np.diff(lo)
+    slot = 3 * lens + 8 * nseg.astype(np.uint64) + 8
+    word_cap = np.zeros(nl + 1, dtype=np.uint64)
+    np.cumsum(slot, out=word_cap[1:])
+    ns = int(seg_base[-1])
+    words = np.zeros(int(word_cap[-1]) + 8, dtype=np.uint32)
+    nwords = np.zeros(max(nl, 1), dtype=np.uint32)
+    head = np.zeros(max(ns, 1), dtype=np.uint32)
+    rec = np.zeros(4 * max(ns, 1), dtype=np.uint32)
+    sreg = np.zeros(4 * max(ns, 1), dtype=np.uint32)
+    lreg = np.zeros(4 * max(nl, 1), dtype=np.uint32)
+    r = _corpus_enc(_p(d), _p(lo, u64p), nl, cp, block, frac, bucket, kbits, ubits, th, _p(nseg),
+                    _p(seg_base, u64p), _p(word_cap, u64p), _p(words), _p(nwords), _p(head), _p(rec), _p(sreg),
+                    _p(lreg))
+    if r != 0:
+        raise ValueError("a list is not representable in its format")
+    # pack the per-list word slots back to back
+    nw = nwords[:nl].astype(np.int64)
+    base = np.zeros(nl + 1, dtype=np.uint64)
+    np.cumsum(nw, out=base[1:])
+    packed = np.zeros(int(base[-1]) + 8, dtype=np.uint32)
+    idx = (np.repeat(word_cap[:-1].astype(np.int64), nw) + np.arange(int(base[-1]), dtype=np.int64) -
+           np.repeat(base[:-1].astype(np.int64), nw))
+    packed[: int(base[-1])] = words[idx]
+    img = CompressedImage()
+    img.words = packed
+    img.lcodec = cod.astype(np.uint32)
+    img.ln = lens.astype(np.uint32)
+    img.lseg = seg_base[:-1].astype(np.uint32)
+    img.lnseg = nseg.astype(np.uint32)
+    img.lword = np.ascontiguousarray(base[:-1])
+    img.lreg = lreg
+    img.head = head
+    img.rec = rec
+    img.sreg = sreg
+    img.max_list = int(lens.max()) if nl else 1
+    img.max_seg = int(rec[3::4].max()) if ns else 1
+    img.nsegs = ns
+    return img
+
+
+_ans_pass = _f(_lib, "or_answer_pass", None, u32p, u64p, u32p, u64p, C.c_uint32, C.c_uint32, C.c_uint64, u64p, u64p,
+               u32p)
+
+
+def answer_batch(docs, list_offsets, terms, term_offsets, threads: int = 0) -> tuple[np.ndarray, np.ndarray]:
+    """answer() on host threads: exact (offsets[nq+1], docids) of a batch."""
+    d = _u32(docs)
+    lo = np.ascontiguousarray(list_offsets, dtype=np.uint64)
+    t = _u32(terms) if len(terms) else np.zeros(1, np.uint32)
+    to = np.ascontiguousarray(term_offsets, dtype=np.uint64)
+    nq = len(to) - 1
+    th = _threads(threads)
+    counts = np.zeros(max(nq, 1), dtype=np.uint64)
+    maxl = int(np.diff(lo).max()) if len(lo) > 1 else 1
+    _ans_pass(_p(d), _p(lo, u64p), _p(t), _p(to, u64p), nq, th, maxl, _p(counts, u64p), None, None)
+    offs = np.zeros(nq + 1, dtype=np.uint64)
+    np.cumsum(counts[:nq], out=offs[1:])
+    out = np.zeros(max(int(offs[-1]), 1), dtype=np.uint32)
+    _ans_pass(_p(d), _p(lo, u64p), _p(t), _p(to, u64p), nq, th, maxl, None, _p(offs, u64p), _p(out))
+    return offs, out[: int(offs[-1])]
