@@ -4,8 +4,8 @@ python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                 [--workload zipf|pairs|skewed|learned|serving] [--scale S]
 
 One step = one batch of the workload's queries through the device pipeline
-(pack -> scan -> persistent probe -> scan -> scatter), with the compressed
-index resident in HBM. Prints ONE JSON line on rank 0.
+(one persistent kernel: pack -> probe -> scatter), with the compressed index
+resident in HBM. Prints ONE JSON line on rank 0.
 
 Workloads (seeded synthetic stand-ins for the reference's Baidu/GOV2 data):
   zipf     10M docs, 100k terms, df_r = min(5M, 5M/r) (~60.4M postings), SegLRC
@@ -44,9 +44,9 @@ sys.path.insert(0, ROOT)
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 
-# dram__bytes_read.sum + dram__bytes_write.sum of one k_probe launch (hash-directory search) on
-# the full-size workload, from one ncu --set full capture of this same bench command
-NCU_PROBE_TRAFFIC = {"zipf": 45.18e6}
+# dram__bytes_read.sum + dram__bytes_write.sum of one k_batch launch on the full-size workload,
+# from one ncu capture of this bench command (profiles/); None until captured for this build
+NCU_BATCH_TRAFFIC: dict = {}
 
 
 def parse():
@@ -122,6 +122,21 @@ def make_workload(name: str, scale: float, gen=None, nq_factor: int = 1):
 def query_postings(w) -> int:
     lens = np.diff(w.list_offsets).astype(np.int64)
     return int(lens[w.terms.astype(np.int64)].sum())
+
+
+def batch_bytes(w, tiles: int, results: int) -> int:
+    """Bookkeeping bytes of one batch beside the probe's (algorithmic_bytes):
+    the pack phase reads the query offsets and terms and three fields of each
+    term's list descriptor and writes the sorted terms, per-query counts and
+    prefixes and a 16-byte work record per tile; the probe phase reads each
+    tile's record, query row and prefixes and writes its count and slot and
+    the survivors; the scatter phase reads tile counts and slots, writes and
+    reads tile positions, moves the survivors and writes the offsets."""
+    nq, nterms = w.nq, len(w.terms)
+    pack = 4 * (nq + 1) + 4 * nterms + 12 * nterms + 4 * nterms + 4 * nq + 8 * (nq + 2) + 16 * tiles
+    probe = tiles * (16 + 4 + 4 + 8) + 4 * nterms + 4 * results
+    scatter = tiles * (8 + 4 + 4) + 4 * results + 4 * (nq + 1)
+    return pack + probe + scatter
 
 
 def algorithmic_bytes(w, arrays) -> int:
@@ -532,7 +547,7 @@ def main():
         return bad
 
     postings = query_postings(w)
-    algos = [args.algo] if args.algo else ["bsearch", "hashseg"] + ([] if args.no_learn else ["learned"])
+    algos = [args.algo] if args.algo else ["bsearch", "hashseg", "segreg"] + ([] if args.no_learn else ["learned"])
     per_algo, per_algo_graph = {}, {}
     tune = None
     with ClockSampler(local) as clk:
@@ -604,14 +619,18 @@ def main():
     d2h = h_off.nbytes + 4 * tot
 
     peak, peak_kind = peak_hbm()
-    algo_bytes = algorithmic_bytes(w, arrays)
-    achieved = algo_bytes / (pms / 1e3) / 1e9
+    probe_bytes = algorithmic_bytes(w, arrays)
+    algo_bytes = probe_bytes + batch_bytes(w, int(st.tiles), int(ora_offs[-1]))
+    # the dominant kernel is the batch kernel itself (one launch per step):
+    # its duration is the stream-launched step's CUDA-event time
+    kms = replicas.max_over_ranks(per_algo[best][0], device=dev)
+    achieved = algo_bytes / (kms / 1e3) / 1e9
 
     # whole-index decode (K1/K2): compressed words + per-segment metadata read, 4 B per posting written
     dec = decode_measure(ctx, ix, w, sizes, arrays, stream, flush, args)
     serving = None
     if not args.no_serve:
-        serving = serving_measure(ix, w, ["hashseg"] + ([] if args.no_learn else ["learned"]), local, cs)
+        serving = serving_measure(ix, w, ["segreg"] + ([] if args.no_learn else ["learned"]), local, cs)
     if serving:
         for a, res in serving["by_algo"].items():
             parity[f"serving {a}"] = sum(0 if r["checksum_ok"] else 1 for r in res.values())
@@ -638,6 +657,10 @@ def main():
         "learned_over_bsearch": (min(per_algo["bsearch"][0], per_algo_graph["bsearch"][0]) /
                                  min(per_algo["learned"][0], per_algo_graph["learned"][0]))
         if "learned" in per_algo and "bsearch" in per_algo else None,
+        # against the codec's own linear model (SegLRC segment regression windows)
+        "learned_over_segreg": (min(per_algo["segreg"][0], per_algo_graph["segreg"][0]) /
+                                min(per_algo["learned"][0], per_algo_graph["learned"][0]))
+        if "learned" in per_algo and "segreg" in per_algo else None,
         "learned_models": learn,
         "index_build": index_build,
         "autotune": tune,
@@ -648,17 +671,19 @@ def main():
                   "compact_ms": st.compact_ms},
         "checksum": list(cs),
         "parity": parity_line,
-        "roofline": {"bound": "hbm", "kernel": "k_probe", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak,
-                     "traffic": NCU_PROBE_TRAFFIC.get(args.workload) if args.scale == 1.0 else None,
-                     "traffic_note": "ncu dram read+write per k_probe launch, hash-directory search",
-                     "algorithmic_bytes": algo_bytes, "peak_kind": peak_kind},
+        "roofline": {"bound": "hbm", "kernel": "k_batch", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "kernel_ms": kms,
+                     "traffic": NCU_BATCH_TRAFFIC.get(args.workload) if args.scale == 1.0 else None,
+                     "traffic_note": "ncu dram read+write per k_batch launch",
+                     "algorithmic_bytes": algo_bytes, "probe_bytes": probe_bytes,
+                     "probe_phase_gbs": probe_bytes / (pms / 1e3) / 1e9 if pms > 0 else None,
+                     "peak_kind": peak_kind},
         "e2e": {"value": job_postings / e2e_s, "unit": "postings/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_s * 1e3, "api": "excl_submit_into + excl_wait",
                 "ms_per_step_submit_wait": e2e_ms["submit_wait"],
                 "l2": "flushed before each step (outside the wall-clock region)"},
-        # pack, probe, scatter per batch: the per-algo runs, the tuned run, the two e2e arms
-        "gpu_launches": 3 * (2 * len(algos) + (2 if tune else 0) + 2) * args.steps,
+        # one batch kernel per step: the per-algo runs (stream and graph), the tuned runs, the two e2e arms
+        "gpu_launches": (2 * len(algos) + (2 if tune else 0) + 2) * args.steps,
         "clocks": clocks,
         "decode": dec,
         "serving": serving,

@@ -14,15 +14,18 @@ _LIB = _os.path.join(_os.path.dirname(_os.path.abspath(__file__)), "libexcl_gpu.
 __all__ = ["Context", "Index", "Batch", "Server", "query_parse", "query_encode", "ExclError", "checksum", "parapfd_encode", "parapfd_decode",
            "encode_array_compat", "library_path", "CODEC_PARAPFD", "CODEC_LRC", "CODEC_LRCSEG", "CODEC_SEGLRC",
            "CODEC_HS_SEGLRC", "CODEC_HS_PARAPFD", "CODEC_NEWPFD", "newpfd_encode", "newpfd_decode", "ALGO_AUTO", "ALGO_BSEARCH", "ALGO_HASHSEG", "ALGO_LEARNED",
-           "pinned_empty"]
+           "ALGO_SEGREG", "pinned_empty"]
 
-if _os.path.exists(_LIB):
-    from .api import (ALGO_AUTO, ALGO_BSEARCH, ALGO_HASHSEG, ALGO_LEARNED, CODEC_HS_PARAPFD, CODEC_HS_SEGLRC, CODEC_LRC,
-                      CODEC_LRCSEG, CODEC_NEWPFD, CODEC_PARAPFD, CODEC_SEGLRC, Batch, Context, ExclError, Index, checksum,
-                      Server, encode_array_compat, library_path, newpfd_decode, newpfd_encode, parapfd_decode,
-                      parapfd_encode, pinned_empty, query_encode, query_parse)
-else:
-    def __getattr__(name):
-        if name in __all__:
+_API_NAMES = set(__all__)
+
+
+def __getattr__(name):
+    # the binding is loaded on first use, so the build module imports (and can
+    # rebuild) even when the library is missing or older than the binding
+    if name in _API_NAMES:
+        if not _os.path.exists(_LIB):
             raise ImportError(f"{_LIB} is not built; run `python -m exclucene_b200.build`")
-        raise AttributeError(name)
+        from . import api
+
+        return getattr(api, name)
+    raise AttributeError(name)

@@ -31,8 +31,8 @@ STATUS_NAMES = ["OK", "INVALID", "CUDA", "CAPACITY", "FORMAT", "TIMEOUT", "DEVIC
 
 CODEC_PARAPFD, CODEC_LRC, CODEC_LRCSEG, CODEC_SEGLRC, CODEC_HS_SEGLRC, CODEC_HS_PARAPFD, CODEC_NEWPFD = range(7)
 CODEC_NAMES = {"parapfd": 0, "lrc": 1, "lrcseg": 2, "seglrc": 3, "hs_seglrc": 4, "hs_parapfd": 5, "newpfd": 6}
-ALGO_AUTO, ALGO_BSEARCH, ALGO_HASHSEG, ALGO_LEARNED = range(4)
-ALGO_NAMES = {"auto": 0, "bsearch": 1, "hashseg": 2, "learned": 3}
+ALGO_AUTO, ALGO_BSEARCH, ALGO_HASHSEG, ALGO_LEARNED, ALGO_SEGREG = range(5)
+ALGO_NAMES = {"auto": 0, "bsearch": 1, "hashseg": 2, "learned": 3, "segreg": 4}
 
 
 class ExclError(RuntimeError):
@@ -148,6 +148,7 @@ _qencode = _sig("excl_query_encode", C.c_int, u32p, u32p, C.c_uint32, C.c_void_p
                 C.POINTER(C.c_size_t))
 _autotune = _sig("excl_autotune", C.c_int, C.c_void_p, C.c_void_p, u32p, u32p, C.c_uint32, C.POINTER(TuneReport))
 _set_tuning = _sig("excl_ctx_set_tuning", C.c_int, C.c_void_p, C.POINTER(TuneReport))
+_set_wait_check = _sig("excl_ctx_set_wait_check", C.c_int, C.c_void_p, C.c_uint32)
 _learn = _sig("excl_learn_models", C.c_int, C.c_void_p, C.c_void_p, C.POINTER(LearnParams), C.POINTER(LearnReport))
 _mexport = _sig("excl_model_export", C.c_int, C.c_void_p, C.c_uint32, C.POINTER(C.c_float), C.POINTER(C.c_float),
                 C.POINTER(C.c_int32), C.POINTER(C.c_uint32))
@@ -161,7 +162,7 @@ EXPORTED = ["excl_learn_models", "excl_model_export", "excl_model_grad", "excl_m
             "excl_ctx_destroy", "excl_last_error", "excl_ctx_stream", "excl_index_upload",
             "excl_decode_lists_device", "excl_decode_lists", "excl_submit", "excl_wait", "excl_batch_free",
             "excl_intersect_device", "excl_ctx_check", "excl_last_stats", "excl_checksum", "excl_submit_into",
-            "excl_host_alloc", "excl_host_free", "excl_ctx_set_tuning"]
+            "excl_host_alloc", "excl_host_free", "excl_ctx_set_tuning", "excl_ctx_set_wait_check"]
 
 
 def _p32(a: np.ndarray):
@@ -475,6 +476,11 @@ class Context:
         _check_status(_build_dev(self._h, C.c_void_p(d_docs), loff.ctypes.data_as(u64p), len(loff) - 1, C.byref(p),
                                  C.byref(h)), self, "excl_index_build_device")
         return Index.from_handle(h, len(loff) - 1, np.diff(loff))
+
+    def set_wait_check(self, polls: int) -> None:
+        """excl_ctx_set_wait_check: polls > 0 makes every later batch run one
+        bounded device wait that gives up (the device failure path); 0 stops it."""
+        _check_status(_set_wait_check(self._h, int(polls)), self, "excl_ctx_set_wait_check")
 
     def set_tuning(self, algo="auto", warps_per_cta: int = 8, ctas_per_sm: int = 5, merge_segs: int = 2,
                    tile_split: int = 0, **_ignored) -> None:

@@ -25,9 +25,9 @@ NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", *ARCH, "-Xcompiler", "-fPIC,-ffp
               "--expt-relaxed-constexpr", f"-I{INCLUDE}"]
 CXX_FLAGS = ["-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-pthread", f"-I{INCLUDE}"]
 
-GPU_SOURCES = ["codec.cpp", "kernels.cu", "pipeline.cu", "decode.cu", "runtime.cu", "learned_train.cu", "noalloc.cu",
+GPU_SOURCES = ["codec.cpp", "kernels.cu", "decode.cu", "runtime.cu", "learned_train.cu", "noalloc.cu",
                "serve.cu", "refformat.cpp", "build_gpu.cu"]
-GPU_HEADERS = ["excl_internal.h", "excl_device.cuh", "kernels.h", "runtime.h"]
+GPU_HEADERS = ["excl_internal.h", "excl_device.cuh", "kernels.h", "runtime.h", "batch_phases.cuh"]
 SYNTH_SOURCES = ["synth.cpp"]
 
 LIB_GPU = os.path.join(PKG, "libexcl_gpu.so")

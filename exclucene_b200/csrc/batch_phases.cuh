@@ -1,27 +1,29 @@
-// The batch pipeline: three launches per batch, no memsets, no host sync.
+// Pack and scatter phases of the one-launch batch kernel (k_batch in
+// kernels.cu). A batch is one persistent grid that runs three phases:
 //
-//   k_pack_scan  per query: sort the terms by list length (stable insertion
-//                sort, ParaPFD_Intersection.cu:155-173), count the shortest
-//                list's tiles and docIDs; then the exclusive prefixes of both
-//                over the batch and the owner query of every tile. CTAs take
-//                their place in the scan from a ticket, so a CTA only waits
-//                on CTAs that are already running (decoupled look-back).
-//   k_probe      kernels.cu.
-//   k_scatter    single-pass decoupled look-back over chunks of 512 tiles:
-//                chunk survivor totals, their prefixes, each tile's output
-//                position and the per-query offsets (replaces cudppScan and
-//                ucntResult, ParaPFD_Intersection.cu:262,301); then every
-//                warp of the grid copies survivors to the result array
-//                (replaces saCompact, :279).
+//   pack     CTAs take chunks of 256 queries by ticket. Per query: sort the
+//            terms by list length (stable insertion sort,
+//            ParaPFD_Intersection.cu:155-173), count the shortest list's
+//            tiles, docIDs and heavy tiles; a block scan plus a decoupled
+//            look-back over the chunks give the batch's prefixes; each tile's
+//            16-byte work record goes to its place in the probe order (heavy
+//            tiles from the front, the others from the back). The chunk that
+//            finishes last publishes the batch's "packed" tag.
+//   probe    kernels.cu: warps take work records from a counter.
+//   scatter  once every taken tile is probed (a count the probe warps add to
+//            once each as they leave the probe loop), CTAs take chunks of 512
+//            tiles: survivor totals, a decoupled look-back for their base,
+//            each tile's output position (replaces cudppScan and ucntResult,
+//            ParaPFD_Intersection.cu:262,301); then every warp copies
+//            survivors to the result array (replaces saCompact, :279) and
+//            every thread writes query offsets.
 //
-// Cross-CTA state (PackSync, chunk states) carries the batch's tag, so it
-// needs no clearing between batches; every wait is bounded and raises
-// kErrScanSpin when it gives up. Nothing here needs all CTAs to be resident,
-// so batches may run concurrently on several streams.
-#include <cuda_runtime.h>
-
-#include <algorithm>
-
+// Every wait is on work that a running CTA already holds (a ticket it took,
+// tiles it took), so the grid needs no co-residency and batches on other
+// streams may share the GPU. Cross-CTA state carries the batch's tag and is
+// never cleared between batches; the counters are reset by the last CTA to
+// leave. Every wait is bounded and raises kErrScanSpin when it gives up.
+#pragma once
 #include "kernels.h"
 
 namespace excl {
@@ -47,18 +49,47 @@ __device__ __forceinline__ uint64_t ld_acquire64(const uint64_t *p) {
     asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
     return v;
 }
+__device__ __forceinline__ void red_release_add(uint32_t *p, uint32_t v) {
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
 
 constexpr uint32_t kPackRegTerms = 8;  // queries with up to this many terms are sorted in registers
-constexpr uint32_t kSpin = 1u << 22;  // x >= 32 ns: a wait gives up after > 0.1 s
 
 // Batch tags cycle through 1 .. 2^30 - 1 (0 is the state of fresh memory).
 __device__ __forceinline__ uint32_t next_tag(uint32_t e) { return e >= (1u << 30) - 1u ? 1u : e + 1u; }
 
-// Chunk state of k_scatter: tag (30 bits) | status (2 bits) | value (32 bits).
+// Chunk state of the scatter look-back: tag (30 bits) | status (2 bits) | value (32 bits).
 constexpr uint32_t kAggregate = 1u, kPrefix = 2u;
 __device__ __forceinline__ uint64_t chunk_word(uint32_t tag, uint32_t status, uint32_t v) {
     return ((uint64_t)tag << 34) | ((uint64_t)status << 32) | v;
 }
+
+// Bounded wait until *p == tag (acquire); false (and kErrScanSpin) if it gave up.
+__device__ __forceinline__ bool wait_tag(const uint32_t *p, uint32_t tag, uint32_t *err, uint32_t spin) {
+    uint32_t spins = 0;
+    while (ld_acquire(p) != tag) {
+        if (++spins > spin) {
+            atomicOr(err, kErrScanSpin);
+            return false;
+        }
+        __nanosleep(64);
+    }
+    return true;
+}
+
+// Shared memory of the pack and scatter phases (a union with the probe's).
+struct PackShared {
+    uint32_t sc[3][33], pre[3], et[kPackThreads], eh[kPackThreads], h[kPackThreads], l0[kPackThreads];
+};
+struct ScatterShared {
+    uint32_t sa[33], sb[33];
+    uint32_t c, base;
+};
 
 // Block-wide exclusive scan of three values at once; returns the block totals.
 __device__ __forceinline__ void block_scan3(const uint32_t (&v)[3], uint32_t (&e)[3], uint32_t (&t)[3],
@@ -101,84 +132,56 @@ __device__ __forceinline__ void block_scan3(const uint32_t (&v)[3], uint32_t (&e
     }
 }
 
+// Block-wide exclusive scan of one value; returns the block total.
+__device__ __forceinline__ uint32_t block_scan1(uint32_t a, uint32_t &total, uint32_t *sa) {
+    const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    uint32_t ia = a;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t xa = __shfl_up_sync(0xffffffffu, ia, o);
+        if (lane >= (uint32_t)o) ia += xa;
+    }
+    if (lane == 31) sa[w] = ia;
+    __syncthreads();
+    if (w == 0) {
+        const uint32_t va = lane < nw ? sa[lane] : 0u;
+        uint32_t ja = va;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t xa = __shfl_up_sync(0xffffffffu, ja, o);
+            if (lane >= (uint32_t)o) ja += xa;
+        }
+        if (lane < nw) sa[lane] = ja - va;
+        if (lane == 31) sa[32] = ja;
+    }
+    __syncthreads();
+    const uint32_t ex = sa[w] + ia - a;
+    total = sa[32];
+    __syncthreads();  // sa is reused by the caller's next scan
+    return ex;
+}
+
 // Tiles of a query's shortest list that hold at least half a tile of keys:
 // the first `heavy` tiles (all full tiles, and the last one when it is at
 // least half full). A tile's probe time grows with its keys, so these go to
-// the front of the probe kernel's work queue and the small tiles fill the end
-// (longest first keeps the busiest SM near the average). Variable (HS) tiles
-// all count as heavy.
+// the front of the probe order and the small tiles fill the end (longest
+// first keeps the busiest SM near the average). Variable (HS) tiles all count
+// as heavy.
 __device__ __forceinline__ uint32_t heavy_tiles(uint32_t n, uint32_t nt, uint32_t log2_block, uint32_t split) {
     if (!log2_block || nt == 0) return nt;
     const uint32_t S = (1u << log2_block) >> tile_split_of(log2_block, split);
     return min(nt, n / S + (2u * (n % S) >= S ? 1u : 0u));
 }
 
-// Block-wide exclusive scan of two values at once; returns the block totals.
-__device__ __forceinline__ void block_scan2(uint32_t a, uint32_t b, uint32_t &ea, uint32_t &eb, uint32_t &ta,
-                                            uint32_t &tb, uint32_t *sa, uint32_t *sb) {
-    const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    uint32_t ia = a, ib = b;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t xa = __shfl_up_sync(0xffffffffu, ia, o), xb = __shfl_up_sync(0xffffffffu, ib, o);
-        if (lane >= (uint32_t)o) {
-            ia += xa;
-            ib += xb;
-        }
-    }
-    if (lane == 31) {
-        sa[w] = ia;
-        sb[w] = ib;
-    }
-    __syncthreads();
-    if (w == 0) {
-        uint32_t va = lane < nw ? sa[lane] : 0u, vb = lane < nw ? sb[lane] : 0u;
-        uint32_t ja = va, jb = vb;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t xa = __shfl_up_sync(0xffffffffu, ja, o), xb = __shfl_up_sync(0xffffffffu, jb, o);
-            if (lane >= (uint32_t)o) {
-                ja += xa;
-                jb += xb;
-            }
-        }
-        if (lane < nw) {
-            sa[lane] = ja - va;
-            sb[lane] = jb - vb;
-        }
-        if (lane == 31) {
-            sa[32] = ja;
-            sb[32] = jb;
-        }
-    }
-    __syncthreads();
-    ea = sa[w] + ia - a;
-    eb = sb[w] + ib - b;
-    ta = sa[32];
-    tb = sb[32];
-}
-
-// ---------------------------------------------------------------------------
-
-__global__ void __launch_bounds__(kPackThreads) k_pack_scan(const ListDesc *__restrict__ lists, uint32_t nlists,
-                                                            const uint32_t *terms,  // device or host-mapped:
-                                                            const uint32_t *toff,   // coherent loads only
-                                                            uint32_t nq,
-                                                            BatchView b, PackSync *__restrict__ sync) {
-    __shared__ uint32_t s_sc[3][33], s_pre[3], s_et[kPackThreads], s_eh[kPackThreads], s_h[kPackThreads],
-        s_l0[kPackThreads], s_id, s_tag;
-    // the probe kernel may launch now (it waits for this grid's results);
-    // this grid reads the batch's queries only, and (when launched after
-    // another batch on this stream) the shared scan state once that batch ends
-    pdl_launch_dependents();
-    pdl_wait();
-    if (threadIdx.x == 0) {
-        s_id = atomicAdd(&sync->ticket, 1u);
-        s_tag = next_tag(*(volatile uint32_t *)&sync->epoch);
-    }
-    __syncthreads();
-    const uint32_t bid = s_id, tag = s_tag;
-    const uint32_t q = bid * blockDim.x + threadIdx.x;
+// Pack chunk `bid` of `npack` (queries bid*256 .. +255) with the CTA's 256
+// threads. The chunk that completes last finishes the phase: batch totals are
+// out (the last chunk wrote them), the probe counter and statistics are
+// cleared, and sync->packed = tag releases the probe phase.
+__device__ __noinline__ void pack_chunk(uint32_t bid, uint32_t npack, uint32_t tag, const ListDesc *__restrict__ lists,
+                                           uint32_t nlists, const uint32_t *terms, const uint32_t *toff, uint32_t nq,
+                                           const BatchView &b, PackSync *__restrict__ sync, PackShared &sm,
+                                           uint32_t spin) {
+    const uint32_t q = bid * kPackThreads + threadIdx.x;
     uint32_t nt = 0, nk = 0, lb0 = 0, l0 = 0;
     if (q < nq) {
         const uint32_t t0 = toff[q], t1 = toff[q + 1];
@@ -267,7 +270,7 @@ __global__ void __launch_bounds__(kPackThreads) k_pack_scan(const ListDesc *__re
     }
     const uint32_t nh = heavy_tiles(nk, nt, lb0, b.tile_split);
     uint32_t ex[3], tot[3];
-    block_scan3({nt, nk, nh}, ex, tot, s_sc);
+    block_scan3({nt, nk, nh}, ex, tot, sm.sc);
     const uint32_t et = ex[0], ek = ex[1], bt = tot[0], bk = tot[1];
     if (threadIdx.x == 0) {
         sync->agg_t[bid] = bt;
@@ -294,7 +297,7 @@ __global__ void __launch_bounds__(kPackThreads) k_pack_scan(const ListDesc *__re
                 const uint32_t p = p0 + lane + 32u * j;
                 uint32_t spins = 0;
                 while (f[j] != tag) {
-                    if (++spins > kSpin) {
+                    if (++spins > spin) {
                         atomicOr(b.err, kErrScanSpin);
                         break;
                     }
@@ -320,41 +323,27 @@ __global__ void __launch_bounds__(kPackThreads) k_pack_scan(const ListDesc *__re
             ph += __shfl_xor_sync(0xffffffffu, ph, o);
         }
         if (lane == 0) {
-            s_pre[0] = pt;
-            s_pre[1] = pk;
-            s_pre[2] = ph;
+            sm.pre[0] = pt;
+            sm.pre[1] = pk;
+            sm.pre[2] = ph;
         }
     }
-    s_et[threadIdx.x] = et;
-    s_eh[threadIdx.x] = ex[2];
-    s_h[threadIdx.x] = nh;
-    s_l0[threadIdx.x] = l0;
+    sm.et[threadIdx.x] = et;
+    sm.eh[threadIdx.x] = ex[2];
+    sm.h[threadIdx.x] = nh;
+    sm.l0[threadIdx.x] = l0;
     __syncthreads();
-    const uint32_t pt = s_pre[0];
-    if (threadIdx.x == 0) {
-        const uint32_t pk = s_pre[1];
-        if (bid == gridDim.x - 1) {
-            const_cast<uint32_t *>(b.tile_prefix)[nq] = pt + bt;
-            const_cast<uint32_t *>(b.tile_prefix)[nq + 1] = s_pre[2] + tot[2];  // heavy tiles in the batch
-            const_cast<uint32_t *>(b.key_base)[nq] = pk + bk;
-            if ((uint64_t)pt + bt > b.max_tiles || (uint64_t)pk + bk > b.max_keys) atomicOr(b.err, kErrCapacity);
-        }
-        if (bid == 0) {
-            *b.tile_counter = 0u;
-            if (b.stats) b.stats[0] = b.stats[1] = b.stats[2] = b.stats[3] = 0ull;
-        }
-        // the last CTA out hands the state to the next batch
-        __threadfence();
-        if (atomicAdd(&sync->done, 1u) == gridDim.x - 1) {
-            sync->ticket = 0u;
-            sync->done = 0u;
-            sync->epoch = tag;
-            __threadfence();
-        }
+    const uint32_t pt = sm.pre[0];
+    if (threadIdx.x == 0 && bid == npack - 1) {
+        const uint32_t pk = sm.pre[1];
+        const_cast<uint32_t *>(b.tile_prefix)[nq] = pt + bt;
+        const_cast<uint32_t *>(b.tile_prefix)[nq + 1] = sm.pre[2] + tot[2];  // heavy tiles in the batch
+        const_cast<uint32_t *>(b.key_base)[nq] = pk + bk;
+        if ((uint64_t)pt + bt > b.max_tiles || (uint64_t)pk + bk > b.max_keys) atomicOr(b.err, kErrCapacity);
     }
     if (q < nq) {
         const_cast<uint32_t *>(b.tile_prefix)[q] = pt + et;
-        const_cast<uint32_t *>(b.key_base)[q] = s_pre[1] + ek;
+        const_cast<uint32_t *>(b.key_base)[q] = sm.pre[1] + ek;
     }
     // owner of each of this CTA's tiles: the last query whose first tile is
     // at or before it (queries with no tiles share their successor's start);
@@ -362,34 +351,40 @@ __global__ void __launch_bounds__(kPackThreads) k_pack_scan(const ListDesc *__re
     // the front in query order, the others from the back of tile_order
     // (a thread's tiles ascend, so its owners do too: the search resumes from
     // the last owner, and a run of one query's tiles costs one check each)
-    const uint32_t ph = s_pre[2];
+    const uint32_t ph = sm.pre[2];
     uint32_t lo = 0;
     for (uint32_t tl = threadIdx.x; tl < bt && pt + tl < b.max_tiles; tl += blockDim.x) {
-        if (lo + 1 < blockDim.x && s_et[lo + 1] <= tl) {
+        if (lo + 1 < blockDim.x && sm.et[lo + 1] <= tl) {
             uint32_t hi = blockDim.x - 1;
             ++lo;
             while (lo < hi) {
                 const uint32_t mid = (lo + hi + 1) >> 1;
-                if (s_et[mid] <= tl) lo = mid;
+                if (sm.et[mid] <= tl) lo = mid;
                 else hi = mid - 1;
             }
         }
-        const uint32_t t = pt + tl, i = tl - s_et[lo], hb = ph + s_eh[lo];
-        const uint4 wr = make_uint4(t, bid * blockDim.x + lo, i, s_l0[lo]);
-        if (i < s_h[lo]) b.tile_order[hb + i] = wr;
-        else b.tile_order[b.max_tiles - 1u - (t - hb - s_h[lo])] = wr;
+        const uint32_t t = pt + tl, i = tl - sm.et[lo], hb = ph + sm.eh[lo];
+        const uint4 wr = make_uint4(t, bid * blockDim.x + lo, i, sm.l0[lo]);
+        if (i < sm.h[lo]) b.tile_order[hb + i] = wr;
+        else b.tile_order[b.max_tiles - 1u - (t - hb - sm.h[lo])] = wr;
     }
+    // this chunk is done once every thread's writes are visible; the chunk
+    // that completes last releases the probe phase
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0 && atomicAdd(&sync->done, 1u) == npack - 1) {
+        __threadfence();  // the other chunks' writes (ordered by their fence before counting) and the totals
+        *b.tile_counter = 0u;
+        *b.probe_done = 0u;
+        if (b.stats) {
+            b.stats[0] = b.stats[1] = b.stats[2] = b.stats[3] = b.stats[6] = 0ull;
+            b.stats[5] = global_ns();
+        }
+        st_release(&sync->packed, tag);
+    }
+    __syncthreads();  // sm is reused by the next chunk
 }
 
-// ---------------------------------------------------------------------------
-
-// Phase A (CTAs holding a chunk ticket): survivor total of the chunk,
-// decoupled look-back for its base, the absolute output position of each of
-// its tiles (into tile_q, free once the probe kernel is done); then the
-// chunk's inclusive prefix is published. Phase B (every warp of the grid, once all chunk tickets are
-// taken, so every chunk is owned by a running CTA): survivors copied tile by
-// tile, each tile after its chunk's prefix is out; a warp gathers the
-// bookkeeping of 32 of its tiles at once.
 // The batch's error bits to the host word the batch names (the device word is
 // cleared for the next batch); nothing when it names none.
 __device__ __forceinline__ void hand_over_flags(const BatchView &b) {
@@ -398,38 +393,52 @@ __device__ __forceinline__ void hand_over_flags(const BatchView &b) {
     __threadfence_system();
 }
 
-__global__ void __launch_bounds__(kSSThreads) k_scatter(BatchView b, PackSync *__restrict__ sync,
-                                                        uint64_t *__restrict__ chunk_state,
-                                                        uint32_t *__restrict__ offsets,
-                                                        uint32_t *__restrict__ docids, uint64_t cap) {
-    __shared__ uint32_t sa[33], sb[33];
-    __shared__ uint32_t s_c, s_base;
+// Scatter phase, run by every CTA once its warps have left the probe loop.
+// Phase A (CTAs holding a chunk ticket): survivor total of the chunk,
+// decoupled look-back for its base, the absolute output position of each of
+// its tiles (into tile_q), then the chunk's inclusive prefix. Phase B (every
+// warp, once all chunk tickets are taken, so every chunk is owned by a running
+// CTA): query offsets, and survivors copied tile by tile, each tile after its
+// chunk's prefix is out.
+__device__ __noinline__ void scatter_phase(const BatchView &b, PackSync *__restrict__ sync,
+                                              uint64_t *__restrict__ chunk_state, uint32_t *__restrict__ offsets,
+                                              uint32_t *__restrict__ docids, uint64_t cap, uint32_t tag,
+                                              ScatterShared &sm, uint32_t spin) {
     constexpr uint32_t kPer = kSSChunk / kSSThreads;
     static_assert(kPer == 2, "two tiles per thread");
-    pdl_launch_dependents();
-    pdl_wait();  // the probe kernel's counts and slots, the pack kernel's prefixes
-    const uint32_t tag = *(volatile uint32_t *)&sync->epoch;  // set by this batch's k_pack_scan
     const uint32_t nq = b.nq;
     const uint32_t T = min(b.tile_prefix[nq], b.max_tiles);
     const uint32_t nch = (T + kSSChunk - 1) / kSSChunk;
     const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
     uint32_t *tile_out = b.tile_q;
-    if (nch == 0) {  // no tiles in the batch: every offset is 0, no ticket taken
+    if (nch == 0) {  // no tiles in the batch: every offset is 0
         for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q <= nq; q += gridDim.x * blockDim.x) offsets[q] = 0u;
-        if (blockIdx.x == 0 && threadIdx.x == 0) hand_over_flags(b);  // the earlier kernels' bits
         return;
     }
     for (;;) {
-        if (threadIdx.x == 0) s_c = atomicAdd(&sync->sticket, 1u);
+        if (threadIdx.x == 0) {
+            sm.c = atomicAdd(&sync->sticket, 1u);
+            // the chunk owners start once every tile of the batch is probed
+            if (sm.c < nch) {
+                uint32_t spins = 0;
+                while (ld_acquire(b.probe_done) != T) {
+                    if (++spins > spin) {
+                        atomicOr(b.err, kErrScanSpin);
+                        break;
+                    }
+                    __nanosleep(64);
+                }
+            }
+        }
         __syncthreads();
-        const uint32_t c = s_c;
+        const uint32_t c = sm.c;
         if (c >= nch) break;
         const uint32_t t0 = c * kSSChunk;
         const uint32_t ta = t0 + threadIdx.x * kPer;
         const uint32_t c0 = ta < T ? b.tile_count[ta] : 0u;
         const uint32_t c1 = ta + 1 < T ? b.tile_count[ta + 1] : 0u;
-        uint32_t ex, e2, tot, t2;
-        block_scan2(c0 + c1, 0u, ex, e2, tot, t2, sa, sb);
+        uint32_t tot;
+        const uint32_t ex = block_scan1(c0 + c1, tot, sm.sa);
         if (threadIdx.x == 0) st_release64(&chunk_state[c], chunk_word(tag, kAggregate, tot));
         if (w == 0) {
             // look-back: sum the aggregates of the preceding chunks up to the
@@ -443,7 +452,7 @@ __global__ void __launch_bounds__(kSSThreads) k_scatter(BatchView b, PackSync *_
                     uint64_t s = ld_acquire64(&chunk_state[idx]);
                     uint32_t spins = 0;
                     while ((uint32_t)(s >> 34) != tag) {
-                        if (++spins > kSpin) {
+                        if (++spins > spin) {
                             atomicOr(b.err, kErrScanSpin);
                             s = chunk_word(tag, kPrefix, 0u);
                             break;
@@ -463,10 +472,10 @@ __global__ void __launch_bounds__(kSSThreads) k_scatter(BatchView b, PackSync *_
                 if (m) break;
                 p -= 32;
             }
-            if (lane == 0) s_base = excl;
+            if (lane == 0) sm.base = excl;
         }
         __syncthreads();
-        const uint32_t base = s_base;
+        const uint32_t base = sm.base;
         if (ta < T) tile_out[ta] = base + ex;
         if (ta + 1 < T) tile_out[ta + 1] = base + ex + c0;
         if (c == nch - 1 && threadIdx.x == 0 && (uint64_t)base + tot > cap) atomicOr(b.err, kErrCapacity);
@@ -476,12 +485,6 @@ __global__ void __launch_bounds__(kSSThreads) k_scatter(BatchView b, PackSync *_
             st_release64(&chunk_state[c], chunk_word(tag, kPrefix, base + tot));
         }
     }
-    // phase B: warp w takes tiles w, w + nw, w + 2nw, ... (neighbouring tiles
-    // go to different warps, so a query with many survivors spreads over the
-    // grid). Lane j handles the warp's j-th tile of a round of 32: its survivor
-    // count, its chunk's prefix (bounded wait), its output position and slot,
-    // all lanes at once; then the warp copies the non-empty tiles one after
-    // another, eight independent loads per lane.
     // the query offsets: the output position of each query's first tile, or
     // for a query with no tile after it, the batch's total (the last chunk's
     // inclusive prefix); each once its chunk's prefix is out
@@ -491,7 +494,7 @@ __global__ void __launch_bounds__(kSSThreads) k_scatter(BatchView b, PackSync *_
         uint64_t s = ld_acquire64(&chunk_state[c]);
         uint32_t spins = 0;
         while ((uint32_t)(s >> 34) != tag || ((uint32_t)(s >> 32) & 3u) != kPrefix) {
-            if (++spins > kSpin) {
+            if (++spins > spin) {
                 atomicOr(b.err, kErrScanSpin);
                 break;
             }
@@ -500,7 +503,13 @@ __global__ void __launch_bounds__(kSSThreads) k_scatter(BatchView b, PackSync *_
         }
         offsets[qq] = tp < T ? ld_acquire(&tile_out[tp]) : (uint32_t)s;
     }
-    const uint32_t gw = blockIdx.x * (kSSThreads / 32) + w, nw = gridDim.x * (kSSThreads / 32);
+    // survivors: warp w takes tiles w, w + nw, w + 2nw, ... (neighbouring
+    // tiles go to different warps, so a query with many survivors spreads over
+    // the grid). Lane j handles the warp's j-th tile of a round of 32: its
+    // survivor count, its chunk's prefix (bounded wait), its output position
+    // and slot, all lanes at once; then the warp copies the non-empty tiles
+    // one after another, eight independent loads per lane.
+    const uint32_t gw = blockIdx.x * (blockDim.x / 32) + w, nw = gridDim.x * (blockDim.x / 32);
     const uint32_t *__restrict__ scr = b.scratch;
     for (uint64_t j0 = 0; gw + j0 * nw < T; j0 += 32) {
         const uint64_t tt = gw + (j0 + lane) * nw;
@@ -512,7 +521,7 @@ __global__ void __launch_bounds__(kSSThreads) k_scatter(BatchView b, PackSync *_
             uint64_t s = ld_acquire64(&chunk_state[c]);
             uint32_t spins = 0;
             while ((uint32_t)(s >> 34) != tag || ((uint32_t)(s >> 32) & 3u) != kPrefix) {
-                if (++spins > kSpin) {
+                if (++spins > spin) {
                     atomicOr(b.err, kErrScanSpin);
                     break;
                 }
@@ -542,34 +551,6 @@ __global__ void __launch_bounds__(kSSThreads) k_scatter(BatchView b, PackSync *_
             }
         }
     }
-    // the last CTA out resets the chunk ticket and hands the batch's error
-    // bits (set by this and the earlier kernels of the batch) to the host;
-    // every thread's writes are fenced before its CTA counts itself done
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0 && atomicAdd(&sync->sdone, 1u) == gridDim.x - 1) {
-        sync->sticket = 0u;
-        sync->sdone = 0u;
-        hand_over_flags(b);
-        __threadfence();
-    }
-}
-
-// ---------------------------------------------------------------------------
-
-int launch_batch(const BatchLaunch &L, cudaStream_t st) {
-    if (L.b.nq > kPackMaxQueries) return (int)cudaErrorInvalidValue;
-    if (L.ev) cudaEventRecord(L.ev[0], st);
-    const uint32_t pack_blocks = std::max(1u, (L.b.nq + kPackThreads - 1) / kPackThreads);
-    k_pack_scan<<<pack_blocks, kPackThreads, 0, st>>>(L.lists, L.nlists, L.terms, L.toff, L.b.nq, L.b, L.sync);
-    int e = (int)cudaGetLastError();
-    if (L.ev) cudaEventRecord(L.ev[1], st);
-    e |= launch_probe(L.ixv, L.b, L.algo, L.warps, L.ctas_per_sm, L.nsm, st);
-    if (L.ev) cudaEventRecord(L.ev[2], st);
-    e |= (int)launch_pdl(k_scatter, dim3(std::max(1, 2 * L.nsm)), dim3(kSSThreads), st, L.b, L.sync, L.chunk_state,
-                         L.offsets, L.docids, L.cap);
-    if (L.ev) cudaEventRecord(L.ev[3], st);
-    return e;
 }
 
 }  // namespace excl

@@ -1,15 +1,17 @@
-// sm_100a kernels of the batched AND-intersection path: the probe kernel
-// and the per-key search it runs against each longer list. The batch's
-// bookkeeping kernels (query pack + prefixes, survivor scatter) are in
-// pipeline.cu; whole-list decode is in decode.cu.
+// sm_100a kernel of the batched AND-intersection path: one persistent launch
+// per batch (k_batch) that packs the queries, probes, and scatters the
+// results; this file holds its probe phase and the per-key search it runs
+// against each longer list, batch_phases.cuh the pack and scatter phases.
+// Whole-list decode is in decode.cu.
 //
-//   k_probe<ALGO>    persistent kernel: each warp takes (query, tile) work
-//                    items from an atomic queue, decodes the tile of the
-//                    shortest list into smem, probes every longer list and
-//                    compacts survivors with ballot/popc (replaces the search
-//                    kernels, e.g. ParaPFD_Intersection_kernel.cu:145-458).
+//   probe phase   each warp takes (query, tile) work items from an atomic
+//                 queue, decodes the tile of the shortest list into smem,
+//                 probes every longer list and compacts survivors with
+//                 ballot/popc (replaces the search kernels, e.g.
+//                 ParaPFD_Intersection_kernel.cu:145-458).
 #include <cstdio>
 
+#include "batch_phases.cuh"
 #include "excl_device.cuh"
 #include "kernels.h"
 
@@ -43,24 +45,28 @@ __device__ __forceinline__ bool probe_key(const DevIndexView &ix, const ListDesc
             ++fallback;
         }
     }
+    // the segment: fixed blocks hold 2^log2_block postings, so a learned rank
+    // window names its segments directly; a window inside one segment needs
+    // no head search at all (a present key's rank lies in the window)
+    const ProbeRec *pr = ix.seg_probe + L.seg_base;
+    int s;
     if (learned) {
         lo = (uint32_t)(plo >> L.log2_block);
         hi = (uint32_t)(phi >> L.log2_block) + 1u;
+        s = hi - lo == 1u ? (int)lo : last_head_le_rec(pr, lo, hi, key);
     } else if (ALGO == EXCL_ALGO_BSEARCH) {
         lo = 0;
-        hi = L.nseg;
+        s = last_head_le(ix.seg_head + L.seg_base, 0, L.nseg, key);
     } else {
         const uint32_t b = (uint32_t)((uint64_t)key >> L.dir_shift);
         const uint32_t d0 = ldg(ix.dir + L.dir_base + b), d1 = ldg(ix.dir + L.dir_base + b + 1);
         lo = codec_is_hs(L.codec) ? d0 : (d0 ? d0 - 1u : 0u);
         hi = d1;
+        s = last_head_le_rec(pr, lo, hi, key);
     }
-    // segment search and record: the record holds the head, block offset,
-    // count, base/median, block descriptor and segment regression
-    const ProbeRec *pr = ix.seg_probe + L.seg_base;
-    const int s = (ALGO == EXCL_ALGO_BSEARCH && !learned) ? last_head_le(ix.seg_head + L.seg_base, lo, hi, key)
-                                                          : last_head_le_rec(pr, lo, hi, key);
     if (s < (int)lo) return false;
+    // the segment's record: head, block offset, count, base/median, block
+    // descriptor and segment regression
     const uint4 q0 = __ldg(reinterpret_cast<const uint4 *>(pr + s));
     const uint4 q1 = __ldg(reinterpret_cast<const uint4 *>(pr + s) + 1);
     SegRec rec;
@@ -85,7 +91,8 @@ __device__ __forceinline__ bool probe_key(const DevIndexView &ix, const ListDesc
     if (learned) {
         t0 = imax64(t0, plo - rec.start);
         t1 = imin64(t1, phi - rec.start);
-    } else if (L.codec == EXCL_CODEC_SEGLRC || L.codec == EXCL_CODEC_HS_SEGLRC || L.codec == EXCL_CODEC_LRCSEG) {
+    } else if ((ALGO == EXCL_ALGO_SEGREG || ALGO == EXCL_ALGO_AUTO) &&
+               (L.codec == EXCL_CODEC_SEGLRC || L.codec == EXCL_CODEC_HS_SEGLRC || L.codec == EXCL_CODEC_LRCSEG)) {
         // Regression window (SegLRC_Intersection_kernel.cu:366-371): the pivot
         // (key - b) / a in IEEE single precision, widened by the fit's safe
         // range. The range was measured with this same expression on every
@@ -135,183 +142,252 @@ __device__ __forceinline__ int locate_segment(const DevIndexView &ix, const List
 }
 
 // ---------------------------------------------------------------------------
-// Persistent probe kernel.
+// The batch kernel: one persistent launch per batch (pack, probe, scatter;
+// the pack and scatter phases are in batch_phases.cuh).
 //
-// For each longer list a tile chooses between two methods (the merge-path /
-// probe choice): when the tile's surviving keys span few of the list's
-// segments (at most b.merge_segs, whose docIDs fit kMergeCap), the warp
+// Probe phase: for each longer list a tile chooses between two methods (the
+// merge-path / probe choice): when the tile's surviving keys span few of the
+// list's segments (at most b.merge_segs, whose docIDs fit kMergeCap), the warp
 // decodes that span into shared memory once and every key is looked up there;
 // otherwise each key is probed on its own (probe_key).
+
+constexpr int kBatchWarps = 8;
+static_assert(kBatchWarps * 32 == kPackThreads && kBatchWarps * 32 == kSSThreads, "one CTA shape for every phase");
+
+struct ProbeShared {
+    uint32_t keys[kBatchWarps][kTileKeys];
+    uint32_t merge[kBatchWarps][kMergeCap];
+    ListDesc list[kBatchWarps];
+};
+
+// Spin limit of every cross-CTA wait (x >= 64 ns of sleep per poll: > 0.25 s).
+constexpr uint32_t kSpin = 1u << 22;
 
 // MINB: resident 8-warp CTAs per SM the register budget is cut for (4: 64
 // registers; 5: 48; 6: 40), traded for more probes in flight; the launch
 // shape is an autotuner choice. KIND: the codec family the instance handles
-// (kKindAny for mixed indexes); a one-family instance needs fewer registers
-// (residual codecs: no spills at 64, the 64-register spills at 48).
-template <int ALGO, int WARPS, int MINB, int KIND>
-__global__ void __launch_bounds__(WARPS * 32, (8 / WARPS) * MINB) k_probe(DevIndexView ix, BatchView b) {
-    __shared__ uint32_t s_keys[WARPS][kTileKeys];
-    __shared__ uint32_t s_merge[WARPS][kMergeCap];
-    __shared__ ListDesc s_list[WARPS];
-    // the scatter kernel may launch now; the pack kernel's output is read below
-    pdl_launch_dependents();
-    pdl_wait();
+// (kKindAny for mixed indexes); a one-family instance needs fewer registers.
+template <int ALGO, int MINB, int KIND>
+__global__ void __launch_bounds__(kBatchWarps * 32, MINB) k_batch(DevIndexView ix, BatchView b, PackSync *sync,
+                                                                  uint64_t *chunk_state, const ListDesc *lists,
+                                                                  uint32_t nlists, const uint32_t *terms,
+                                                                  const uint32_t *toff, uint32_t *offsets,
+                                                                  uint32_t *docids, uint64_t cap, uint32_t spin) {
+    __shared__ union {
+        ProbeShared probe;
+        PackShared pack;
+        ScatterShared scatter;
+    } sm;
+    __shared__ uint32_t s_tag, s_ticket;
     const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
-    uint32_t *keys = s_keys[w];  // the tile's keys (a sub-range of the decoded segment when tiles are cut)
-    uint32_t *mbuf = s_merge[w];
-    ListDesc &L = s_list[w];
-    // work order: the pack kernel writes one record {tile, query, tile within
-    // the query, shortest list} per tile into tile_order, heavy tiles from the
-    // front, the others from the back. The records fill the first H and the
-    // last T - H slots exactly, also after a tile overflow (reported as
-    // kErrCapacity), where T is capped at max_tiles and the slots fill up.
-    const uint32_t T = min(b.tile_prefix[b.nq], b.max_tiles);
-    const uint32_t H = min(b.tile_prefix[b.nq + 1], T);
-    uint32_t probes = 0, fallbacks = 0, nkeys = 0, merges = 0;
+    // every CTA reads the same epoch: it changes only when the last CTA of
+    // this grid leaves, and that CTA has counted every other one out
+    if (threadIdx.x == 0) s_tag = next_tag(*(volatile uint32_t *)&sync->epoch);
+    __syncthreads();
+    const uint32_t tag = s_tag;
+    // failure-path self-test: a bounded wait on a flag that nothing sets gives
+    // up and raises the expired-wait bit; the batch itself is unaffected
+    if (b.check_polls && blockIdx.x == 0 && threadIdx.x == 0) wait_tag(b.check_flag, tag, b.err, b.check_polls);
+
+    // ---- pack: chunks of 256 queries by ticket
+    const uint32_t npack = max(1u, (b.nq + kPackThreads - 1) / kPackThreads);
     for (;;) {
-        uint32_t wi = 0;
-        if (lane == 0) wi = atomicAdd(b.tile_counter, 1u);
-        wi = __shfl_sync(0xffffffffu, wi, 0);
-        if (wi >= T) break;
-        const uint4 wr = b.tile_order[wi < H ? wi : b.max_tiles - 1u - (wi - H)];
-        const uint32_t t = wr.x, q = wr.y, ti = wr.z, list0 = wr.w;
-        // the query's sorted terms (lane j holds term j), term count, key base
-        // and the shortest list's descriptor: one round of independent loads
-        const uint32_t tq = b.qterms[(size_t)q * kMaxTerms + lane];
-        const uint32_t k = b.qnterms[q];
-        const uint32_t kbase = b.key_base[q];
-        __syncwarp();
-        if (lane < 5) reinterpret_cast<uint4 *>(&L)[lane] = reinterpret_cast<const uint4 *>(ix.lists + list0)[lane];
-        __syncwarp();
-        // decode the tile's keys: one fixed segment, or 1..255 consecutive
-        // variable segments / one 256-slice of a large segment
-        uint32_t kc = 0, first_elem;
-        keys = s_keys[w];
-        if (L.log2_block) {
-            // tile ti: part (ti mod 2^s) of segment ti >> s; the whole segment is
-            // decoded (d-gaps need its prefix) and the part's keys probed
-            const uint32_t sp = tile_split_of(L.log2_block, b.tile_split);
-            const uint32_t sg = L.seg_base + (ti >> sp);
-            // fixed blocks: every segment but the last holds 2^log2_block postings
-            const uint32_t cnt = min(1u << L.log2_block, L.n - ((ti >> sp) << L.log2_block));
-            const uint32_t sub = (1u << L.log2_block) >> sp, e0 = (ti & ((1u << sp) - 1u)) * sub;
-            first_elem = ((ti >> sp) << L.log2_block) + e0;
-            warp_decode<KIND>(ix, L, sg, 0, cnt, keys, lane);
-            kc = e0 < cnt ? min(sub, cnt - e0) : 0u;
-            keys += e0;
-        } else {
-            const uint64_t tm = ix.tilemap[L.tile_base + ti];
-            const uint32_t sg0 = L.seg_base + (uint32_t)(tm >> 32);
-            const uint32_t e0 = (uint32_t)(tm >> 8) & kTileMaxE0, ns = (uint32_t)tm & 0xffu;
-            first_elem = ix.seg_rec[sg0].start + e0;
-            for (uint32_t g = 0; g < ns; ++g) {
-                const uint32_t c = min(kTileKeys - kc, ix.seg_rec[sg0 + g].count - (g ? 0u : e0));
-                warp_decode<KIND>(ix, L, sg0 + g, g ? 0u : e0, c, keys + kc, lane);
-                kc += c;
-            }
-        }
-        nkeys += kc;
-        uint32_t alive = kc;
-        for (uint32_t j = 1; j < k && alive; ++j) {
-            const uint32_t lj = __shfl_sync(0xffffffffu, tq, j);
-            __syncwarp();
-            if (lane < 5) reinterpret_cast<uint4 *>(&L)[lane] = reinterpret_cast<const uint4 *>(ix.lists + lj)[lane];
-            __syncwarp();
-            // merge when the keys' range covers few segments: estimated from
-            // the list's density first (no loads), then measured
-            uint32_t span = 0, mseg0 = 0;
-            if (b.merge_segs && alive >= kMergeMinKeys) {
-                const uint32_t klo = keys[0], khi = keys[alive - 1];
-                const double dens = (double)L.n / ((double)(L.last_doc - L.first_doc) + 1.0);
-                if ((double)(khi - klo) * dens < 0.75 * kMergeCap) {
-                    int sl = 0;
-                    if (lane < 2) sl = locate_segment<ALGO>(ix, L, lane ? khi : klo);
-                    const int s0 = max(__shfl_sync(0xffffffffu, sl, 0), 0), s1 = __shfl_sync(0xffffffffu, sl, 1);
-                    if (s1 >= s0 && (uint32_t)(s1 - s0) < b.merge_segs) {
-                        const uint32_t a0 = ix.seg_rec[L.seg_base + s0].start;
-                        const SegRec r1 = ix.seg_rec[L.seg_base + s1];
-                        if (r1.start + r1.count - a0 <= kMergeCap) {
-                            span = r1.start + r1.count - a0;
-                            mseg0 = (uint32_t)s0;
-                            ++merges;
-                            for (uint32_t sg = L.seg_base + s0; sg <= L.seg_base + (uint32_t)s1; ++sg) {
-                                const SegRec r = ix.seg_rec[sg];
-                                for (uint32_t e0 = 0; e0 < r.count; e0 += kTileKeys)
-                                    warp_decode<KIND>(ix, L, sg, e0, min(kTileKeys, r.count - e0), mbuf + (r.start - a0) + e0,
-                                                lane);
-                            }
-                        }
-                    } else if (s1 < 0) {
-                        alive = 0;  // every key precedes the list: nothing survives
-                        continue;
-                    }
-                }
-            }
-            (void)mseg0;
-            uint32_t nout = 0;
-            for (uint32_t base = 0; base < alive; base += 32) {
-                const uint32_t i = base + lane;
-                const bool valid = i < alive;
-                const uint32_t key = valid ? keys[i] : 0u;
-                bool f;
-                if (span) {
-                    // first position with mbuf[pos] >= key, in shared memory
-                    uint32_t lo = 0, hi = span;
-                    while (lo < hi) {
-                        const uint32_t mid = (lo + hi) >> 1;
-                        if (mbuf[mid] < key) lo = mid + 1;
-                        else hi = mid;
-                    }
-                    f = valid && lo < span && mbuf[lo] == key;
-                } else {
-                    f = valid && probe_key<ALGO, KIND>(ix, L, key, fallbacks);
-                }
-                probes += valid;
-                const uint32_t m = __ballot_sync(0xffffffffu, f);
-                const uint32_t pos = nout + __popc(m & ((1u << lane) - 1u));
-                __syncwarp();
-                if (f) keys[pos] = key;
-                nout += __popc(m);
-            }
-            __syncwarp();
-            alive = nout;
-        }
-        // survivors go to the tile's key-indexed slot (its keys' positions in
-        // the batch's concatenated shortest lists)
-        const uint64_t slot = (uint64_t)kbase + first_elem;
-        if (slot + kc > b.max_keys) {
-            if (lane == 0) atomicOr(b.err, kErrCapacity);
-            alive = 0;
-        }
-        uint32_t *dst = b.scratch + slot;
-        for (uint32_t i = lane; i < alive; i += 32) dst[i] = keys[i];
-        if (lane == 0) {
-            b.tile_count[t] = alive;
-            b.tile_slot[t] = (uint32_t)slot;
-        }
-        __syncwarp();
+        if (threadIdx.x == 0) s_ticket = atomicAdd(&sync->ticket, 1u);
+        __syncthreads();
+        const uint32_t bid = s_ticket;
+        __syncthreads();
+        if (bid >= npack) break;
+        if (bid == 0 && threadIdx.x == 0 && b.stats) b.stats[4] = global_ns();
+        pack_chunk(bid, npack, tag, lists, nlists, terms, toff, b.nq, b, sync, sm.pack, spin);
     }
-    if (b.stats) {
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            probes += __shfl_xor_sync(0xffffffffu, probes, o);
-            fallbacks += __shfl_xor_sync(0xffffffffu, fallbacks, o);
+    if (threadIdx.x == 0) wait_tag(&sync->packed, tag, b.err, spin);
+    __syncthreads();
+
+    // ---- probe. Work order: one record {tile, query, tile within the query,
+    // shortest list} per tile in tile_order, heavy tiles from the front, the
+    // others from the back. The records fill the first H and the last T - H
+    // slots exactly, also after a tile overflow (reported as kErrCapacity),
+    // where T is capped at max_tiles and the slots fill up.
+    {
+        uint32_t *keys = sm.probe.keys[w];  // the tile's keys (a sub-range of the decoded segment when tiles are cut)
+        uint32_t *mbuf = sm.probe.merge[w];
+        ListDesc &L = sm.probe.list[w];
+        const uint32_t T = min(b.tile_prefix[b.nq], b.max_tiles);
+        const uint32_t H = min(b.tile_prefix[b.nq + 1], T);
+        uint32_t probes = 0, fallbacks = 0, nkeys = 0, merges = 0, done = 0;
+        for (;;) {
+            uint32_t wi = 0;
+            if (lane == 0) wi = atomicAdd(b.tile_counter, 1u);
+            wi = __shfl_sync(0xffffffffu, wi, 0);
+            if (wi >= T) break;
+            const uint4 wr = b.tile_order[wi < H ? wi : b.max_tiles - 1u - (wi - H)];
+            const uint32_t t = wr.x, q = wr.y, ti = wr.z, list0 = wr.w;
+            // the query's sorted terms (lane j holds term j), term count, key base
+            // and the shortest list's descriptor: one round of independent loads
+            const uint32_t tq = b.qterms[(size_t)q * kMaxTerms + lane];
+            const uint32_t k = b.qnterms[q];
+            const uint32_t kbase = b.key_base[q];
+            __syncwarp();
+            if (lane < 5) reinterpret_cast<uint4 *>(&L)[lane] = reinterpret_cast<const uint4 *>(ix.lists + list0)[lane];
+            __syncwarp();
+            // decode the tile's keys: one fixed segment, or 1..255 consecutive
+            // variable segments / one 256-slice of a large segment
+            uint32_t kc = 0, first_elem;
+            keys = sm.probe.keys[w];
+            if (L.log2_block) {
+                // tile ti: part (ti mod 2^s) of segment ti >> s; the whole segment is
+                // decoded (d-gaps need its prefix) and the part's keys probed
+                const uint32_t sp = tile_split_of(L.log2_block, b.tile_split);
+                const uint32_t sg = L.seg_base + (ti >> sp);
+                // fixed blocks: every segment but the last holds 2^log2_block postings
+                const uint32_t cnt = min(1u << L.log2_block, L.n - ((ti >> sp) << L.log2_block));
+                const uint32_t sub = (1u << L.log2_block) >> sp, e0 = (ti & ((1u << sp) - 1u)) * sub;
+                first_elem = ((ti >> sp) << L.log2_block) + e0;
+                warp_decode<KIND>(ix, L, sg, 0, cnt, keys, lane);
+                kc = e0 < cnt ? min(sub, cnt - e0) : 0u;
+                keys += e0;
+            } else {
+                const uint64_t tm = ix.tilemap[L.tile_base + ti];
+                const uint32_t sg0 = L.seg_base + (uint32_t)(tm >> 32);
+                const uint32_t e0 = (uint32_t)(tm >> 8) & kTileMaxE0, ns = (uint32_t)tm & 0xffu;
+                first_elem = ix.seg_rec[sg0].start + e0;
+                for (uint32_t g = 0; g < ns; ++g) {
+                    const uint32_t c = min(kTileKeys - kc, ix.seg_rec[sg0 + g].count - (g ? 0u : e0));
+                    warp_decode<KIND>(ix, L, sg0 + g, g ? 0u : e0, c, keys + kc, lane);
+                    kc += c;
+                }
+            }
+            nkeys += kc;
+            uint32_t alive = kc;
+            for (uint32_t j = 1; j < k && alive; ++j) {
+                const uint32_t lj = __shfl_sync(0xffffffffu, tq, j);
+                __syncwarp();
+                if (lane < 5) reinterpret_cast<uint4 *>(&L)[lane] = reinterpret_cast<const uint4 *>(ix.lists + lj)[lane];
+                __syncwarp();
+                // merge when the keys' range covers few segments: estimated from
+                // the list's density first (no loads), then measured
+                uint32_t span = 0;
+                if (b.merge_segs && alive >= kMergeMinKeys) {
+                    const uint32_t klo = keys[0], khi = keys[alive - 1];
+                    const double dens = (double)L.n / ((double)(L.last_doc - L.first_doc) + 1.0);
+                    if ((double)(khi - klo) * dens < 0.75 * kMergeCap) {
+                        int sl = 0;
+                        if (lane < 2) sl = locate_segment<ALGO>(ix, L, lane ? khi : klo);
+                        const int s0 = max(__shfl_sync(0xffffffffu, sl, 0), 0), s1 = __shfl_sync(0xffffffffu, sl, 1);
+                        if (s1 >= s0 && (uint32_t)(s1 - s0) < b.merge_segs) {
+                            const uint32_t a0 = ix.seg_rec[L.seg_base + s0].start;
+                            const SegRec r1 = ix.seg_rec[L.seg_base + s1];
+                            if (r1.start + r1.count - a0 <= kMergeCap) {
+                                span = r1.start + r1.count - a0;
+                                ++merges;
+                                for (uint32_t sg = L.seg_base + s0; sg <= L.seg_base + (uint32_t)s1; ++sg) {
+                                    const SegRec r = ix.seg_rec[sg];
+                                    for (uint32_t e0 = 0; e0 < r.count; e0 += kTileKeys)
+                                        warp_decode<KIND>(ix, L, sg, e0, min(kTileKeys, r.count - e0),
+                                                          mbuf + (r.start - a0) + e0, lane);
+                                }
+                            }
+                        } else if (s1 < 0) {
+                            alive = 0;  // every key precedes the list: nothing survives
+                            continue;
+                        }
+                    }
+                }
+                uint32_t nout = 0;
+                for (uint32_t base = 0; base < alive; base += 32) {
+                    const uint32_t i = base + lane;
+                    const bool valid = i < alive;
+                    const uint32_t key = valid ? keys[i] : 0u;
+                    bool f;
+                    if (span) {
+                        // first position with mbuf[pos] >= key, in shared memory
+                        uint32_t lo = 0, hi = span;
+                        while (lo < hi) {
+                            const uint32_t mid = (lo + hi) >> 1;
+                            if (mbuf[mid] < key) lo = mid + 1;
+                            else hi = mid;
+                        }
+                        f = valid && lo < span && mbuf[lo] == key;
+                    } else {
+                        f = valid && probe_key<ALGO, KIND>(ix, L, key, fallbacks);
+                    }
+                    probes += valid;
+                    const uint32_t m = __ballot_sync(0xffffffffu, f);
+                    const uint32_t pos = nout + __popc(m & ((1u << lane) - 1u));
+                    __syncwarp();
+                    if (f) keys[pos] = key;
+                    nout += __popc(m);
+                }
+                __syncwarp();
+                alive = nout;
+            }
+            // survivors go to the tile's key-indexed slot (its keys' positions in
+            // the batch's concatenated shortest lists)
+            const uint64_t slot = (uint64_t)kbase + first_elem;
+            if (slot + kc > b.max_keys) {
+                if (lane == 0) atomicOr(b.err, kErrCapacity);
+                alive = 0;
+            }
+            uint32_t *dst = b.scratch + slot;
+            for (uint32_t i = lane; i < alive; i += 32) dst[i] = keys[i];
+            if (lane == 0) {
+                b.tile_count[t] = alive;
+                b.tile_slot[t] = (uint32_t)slot;
+            }
+            ++done;
+            __syncwarp();
         }
-        // nkeys and merges are warp-uniform: lane 0's count is the warp's
+        // this warp's tiles are written: count them in (the scatter phase
+        // starts when the count reaches the batch's tiles)
+        __threadfence();
+        __syncwarp();
         if (lane == 0) {
-            atomicAdd((unsigned long long *)&b.stats[0], (unsigned long long)probes);
-            atomicAdd((unsigned long long *)&b.stats[1], (unsigned long long)fallbacks);
-            atomicAdd((unsigned long long *)&b.stats[2], (unsigned long long)nkeys);
-            atomicAdd((unsigned long long *)&b.stats[3], (unsigned long long)merges);
+            if (done) red_release_add(b.probe_done, done);
+            if (b.stats) atomicMax((unsigned long long *)&b.stats[6], (unsigned long long)global_ns());
         }
+        if (b.stats) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                probes += __shfl_xor_sync(0xffffffffu, probes, o);
+                fallbacks += __shfl_xor_sync(0xffffffffu, fallbacks, o);
+            }
+            // nkeys and merges are warp-uniform: lane 0's count is the warp's
+            if (lane == 0) {
+                atomicAdd((unsigned long long *)&b.stats[0], (unsigned long long)probes);
+                atomicAdd((unsigned long long *)&b.stats[1], (unsigned long long)fallbacks);
+                atomicAdd((unsigned long long *)&b.stats[2], (unsigned long long)nkeys);
+                atomicAdd((unsigned long long *)&b.stats[3], (unsigned long long)merges);
+            }
+        }
+    }
+    __syncthreads();  // the shared union passes to the scatter phase
+
+    // ---- scatter
+    scatter_phase(b, sync, chunk_state, offsets, docids, cap, tag, sm.scatter, spin);
+
+    // the last CTA out resets the counters, hands the batch's error bits to
+    // the host and passes the epoch on; every thread's writes are fenced
+    // before its CTA counts itself out
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0 && atomicAdd(&sync->sdone, 1u) == gridDim.x - 1) {
+        __threadfence();
+        sync->ticket = 0u;
+        sync->done = 0u;
+        sync->sticket = 0u;
+        sync->sdone = 0u;
+        if (b.stats) b.stats[7] = global_ns();
+        hand_over_flags(b);
+        sync->epoch = tag;
+        __threadfence();
     }
 }
 
 // ---------------------------------------------------------------------------
 // Launchers.
 
-template <int ALGO, int WARPS, int MINB, int KIND>
-static void launch_probe_t(const DevIndexView &ix, const BatchView &b, int nsm, cudaStream_t st) {
+template <int ALGO, int MINB, int KIND>
+static cudaError_t launch_batch_t(const BatchLaunch &L, cudaStream_t st) {
     // persistent grid: as many CTAs as fit on the device at once, so every
     // resident warp pulls work items
     static int occ[64] = {};
@@ -319,49 +395,51 @@ static void launch_probe_t(const DevIndexView &ix, const BatchView &b, int nsm, 
     cudaGetDevice(&dev);
     int per_sm = dev >= 0 && dev < 64 ? occ[dev] : 0;
     if (!per_sm) {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_probe<ALGO, WARPS, MINB, KIND>, WARPS * 32, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch<ALGO, MINB, KIND>, kBatchWarps * 32, 0);
         per_sm = per_sm > 0 ? per_sm : 1;
         if (dev >= 0 && dev < 64) occ[dev] = per_sm;
     }
-    const uint32_t grid = (uint32_t)std::max(1, std::min(per_sm, (8 / WARPS) * MINB) * nsm);
-    launch_pdl(k_probe<ALGO, WARPS, MINB, KIND>, dim3(grid), dim3(WARPS * 32), st, ix, b);
+    const uint32_t grid = (uint32_t)std::max(1, std::min(per_sm, MINB) * L.nsm);
+    k_batch<ALGO, MINB, KIND><<<grid, kBatchWarps * 32, 0, st>>>(L.ixv, L.b, L.sync, L.chunk_state, L.lists, L.nlists,
+                                                                  L.terms, L.toff, L.offsets, L.docids, L.cap,
+                                                                  L.spin ? L.spin : kSpin);
+    return cudaGetLastError();
 }
 
-template <int ALGO, int WARPS, int MINB>
-static void launch_probe_k(const DevIndexView &ix, const BatchView &b, int nsm, cudaStream_t st) {
-    switch (codec_kind(ix.codec_mask)) {
-        case kKindResid: launch_probe_t<ALGO, WARPS, MINB, kKindResid>(ix, b, nsm, st); break;
-        case kKindDgap: launch_probe_t<ALGO, WARPS, MINB, kKindDgap>(ix, b, nsm, st); break;
-        default: launch_probe_t<ALGO, WARPS, MINB, kKindAny>(ix, b, nsm, st); break;
+template <int ALGO, int MINB>
+static cudaError_t launch_batch_k(const BatchLaunch &L, cudaStream_t st) {
+    switch (codec_kind(L.ixv.codec_mask)) {
+        case kKindResid: return launch_batch_t<ALGO, MINB, kKindResid>(L, st);
+        case kKindDgap: return launch_batch_t<ALGO, MINB, kKindDgap>(L, st);
+        default: return launch_batch_t<ALGO, MINB, kKindAny>(L, st);
     }
 }
 
-template <int WARPS, int MINB>
-static void launch_probe_a(const DevIndexView &ix, const BatchView &b, int algo, int nsm, cudaStream_t st) {
-    switch (algo) {
-        case EXCL_ALGO_BSEARCH: launch_probe_k<EXCL_ALGO_BSEARCH, WARPS, MINB>(ix, b, nsm, st); break;
-        case EXCL_ALGO_HASHSEG: launch_probe_k<EXCL_ALGO_HASHSEG, WARPS, MINB>(ix, b, nsm, st); break;
-        case EXCL_ALGO_LEARNED: launch_probe_k<EXCL_ALGO_LEARNED, WARPS, MINB>(ix, b, nsm, st); break;
-        default: launch_probe_k<EXCL_ALGO_AUTO, WARPS, MINB>(ix, b, nsm, st); break;
+template <int MINB>
+static cudaError_t launch_batch_a(const BatchLaunch &L, cudaStream_t st) {
+    switch (L.algo) {
+        case EXCL_ALGO_BSEARCH: return launch_batch_k<EXCL_ALGO_BSEARCH, MINB>(L, st);
+        case EXCL_ALGO_HASHSEG: return launch_batch_k<EXCL_ALGO_HASHSEG, MINB>(L, st);
+        case EXCL_ALGO_LEARNED: return launch_batch_k<EXCL_ALGO_LEARNED, MINB>(L, st);
+        case EXCL_ALGO_SEGREG: return launch_batch_k<EXCL_ALGO_SEGREG, MINB>(L, st);
+        default: return launch_batch_k<EXCL_ALGO_AUTO, MINB>(L, st);
     }
 }
 
-template <int WARPS>
-static void launch_probe_w(const DevIndexView &ix, const BatchView &b, int algo, int ctas_per_sm, int nsm,
-                           cudaStream_t st) {
+int launch_batch(const BatchLaunch &L, cudaStream_t st) {
+    if (L.b.nq > kPackMaxQueries) return (int)cudaErrorInvalidValue;
+    if (L.ev) cudaEventRecord(L.ev[0], st);
     // ctas_per_sm is counted in 8-warp CTAs
-    if (ctas_per_sm <= 4) launch_probe_a<WARPS, 4>(ix, b, algo, nsm, st);
-    else if (ctas_per_sm == 5) launch_probe_a<WARPS, 5>(ix, b, algo, nsm, st);
-    else launch_probe_a<WARPS, 6>(ix, b, algo, nsm, st);
-}
-
-int launch_probe(const DevIndexView &ix, const BatchView &b, int algo, int warps, int ctas_per_sm, int nsm,
-                 cudaStream_t st) {
-    switch (warps) {
-        case 4: launch_probe_w<4>(ix, b, algo, ctas_per_sm, nsm, st); break;
-        default: launch_probe_w<8>(ix, b, algo, ctas_per_sm, nsm, st); break;
+    cudaError_t e;
+    if (L.ctas_per_sm <= 4) e = launch_batch_a<4>(L, st);
+    else if (L.ctas_per_sm == 5) e = launch_batch_a<5>(L, st);
+    else e = launch_batch_a<6>(L, st);
+    if (L.ev) {
+        cudaEventRecord(L.ev[1], st);
+        cudaEventRecord(L.ev[2], st);
+        cudaEventRecord(L.ev[3], st);
     }
-    return (int)cudaGetLastError();
+    return (int)e;
 }
 
 }  // namespace excl

@@ -1,4 +1,4 @@
-// Launch wrappers of kernels.cu and the per-batch device view.
+// The per-batch device view and the launchers of kernels.cu / decode.cu.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -14,10 +14,10 @@ struct BatchView {
     const uint32_t *qterms;      // nq * kMaxTerms list ids, ascending length
     const uint32_t *qnterms;     // terms per query
     const uint32_t *tile_prefix; // nq + 1, exclusive prefix of tiles per query
-    uint32_t *tile_q;            // max_tiles, scratch of k_scatter (each tile's output position)
+    uint32_t *tile_q;            // max_tiles, scratch of the scatter phase (each tile's output position)
     uint4 *tile_order;           // max_tiles work records {tile, query, tile within the query, shortest list}:
                                  // heavy tiles from the front, the rest from the back (tile_prefix[nq + 1] = heavy tiles)
-    uint32_t *tile_counter;      // work-queue head (zeroed by k_pack_scan)
+    uint32_t *tile_counter;      // work-queue head (zeroed by the pack phase)
     const uint32_t *key_base;    // nq + 1, exclusive prefix of shortest-list lengths
     uint32_t *tile_count;        // survivors per tile
     uint32_t *tile_slot;         // scratch position of each tile's survivors
@@ -28,40 +28,18 @@ struct BatchView {
     uint64_t max_keys;
     uint32_t *err;               // error flag bits
     uint32_t *err_out;           // or null: device-mapped host word that receives this batch's error bits at its end (the device word is cleared)
-    uint64_t *stats;             // [probes, fallbacks] or null
+    uint32_t *probe_done;        // tiles probed so far (cleared by the pack phase)
+    uint32_t check_polls;        // > 0: one bounded wait on check_flag (which nothing sets) that must give up
+    const uint32_t *check_flag;
+    uint64_t *stats;             // or null: [probes, fallbacks, keys, merges, t_start, t_packed, t_probed, t_end]
+                                 // (times in globaltimer ns)
 };
-
-// Programmatic dependent launch: the batch's kernels are launched with
-// programmatic stream serialization, so a kernel's CTAs may become resident
-// while the previous kernel of the stream still runs. Each kernel lets its
-// successor launch at once (pdl_launch_dependents) and waits, before its
-// first read of the previous kernel's output, until that kernel has finished
-// and its writes are visible (pdl_wait; a no-op when launched without the
-// attribute). This hides the launch and ramp-up gaps between the three
-// launches of a batch.
-__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
-__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
-
-template <typename... KArgs, typename... Args>
-inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t st, Args &&...args) {
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = grid;
-    cfg.blockDim = block;
-    cfg.dynamicSmemBytes = 0;
-    cfg.stream = st;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
-}
 
 // probe kernel: shared-memory merge of a tile's keys against a decoded span
 constexpr uint32_t kMergeCap = 512;      // docIDs of the span (two 256-blocks)
 constexpr uint32_t kMergeMinKeys = 32;   // fewer keys than this: always probe
 
-// pipeline.cu
+// the batch kernel's phases (kernels.cu, batch_phases.cuh)
 constexpr uint32_t kPackThreads = 256;
 constexpr uint32_t kPackMaxCtas = 1024;
 constexpr uint32_t kPackMaxQueries = kPackThreads * kPackMaxCtas;
@@ -71,9 +49,10 @@ constexpr uint32_t kSSChunk = 512;
 // Cross-CTA state of one stream's batches (zeroed once at allocation; the
 // kernels tag what they publish with the batch, so it is never cleared).
 struct PackSync {
-    uint32_t epoch;           // tag of the last batch packed on this state
-    uint32_t ticket, done;    // k_pack_scan: CTA order, CTAs finished
-    uint32_t sticket, sdone;  // k_scatter: chunk order, CTAs finished
+    uint32_t epoch;           // tag of the last batch run on this state
+    uint32_t ticket, done;    // pack phase: chunk tickets, chunks finished
+    uint32_t sticket, sdone;  // scatter phase: chunk tickets; CTAs that left the kernel
+    uint32_t packed;          // tag of the batch whose pack phase is complete
     uint32_t flag[kPackMaxCtas];
     uint32_t agg_t[kPackMaxCtas];
     uint32_t agg_k[kPackMaxCtas];
@@ -93,16 +72,15 @@ struct BatchLaunch {
     uint32_t *docids;       // cap
     uint64_t cap;
     int algo, warps, ctas_per_sm, nsm;
-    cudaEvent_t *ev;  // 4 events around the three kernels, or null
+    uint32_t spin;    // polls before a cross-CTA wait gives up (0: the default)
+    cudaEvent_t *ev;  // 4 events around the batch kernel, or null
 };
 
-// pack -> probe -> scatter on `st`.
+// The batch kernel (pack, probe, scatter in one launch) on `st`.
 int launch_batch(const BatchLaunch &L, cudaStream_t st);
 
 // tk: two zeroed words (work counter, finished CTAs), left zeroed.
 int launch_decode(const DevIndexView &ix, uint32_t l0, uint32_t l1, uint64_t out_base0, uint32_t *out, uint32_t seg0,
                   uint32_t nsegs, int nsm, uint32_t *tk, uint32_t *err, cudaStream_t st);
-int launch_probe(const DevIndexView &ix, const BatchView &b, int algo, int warps, int ctas_per_sm, int nsm,
-                 cudaStream_t st);
 
 }  // namespace excl

@@ -49,7 +49,7 @@ constexpr uint64_t kOffTileSlot = kOffTileCount + up64(kNATiles + 1);
 constexpr uint64_t kOffTileOrder = kOffTileSlot + up64(kNATiles + 1);
 constexpr uint64_t kOffSurvivors = kOffTileOrder + up64(4 * ((uint64_t)kNATiles + 1));  // 16-byte work records
 constexpr uint64_t kOffMisc = kOffSurvivors + up64(kNAKeys);
-constexpr uint64_t kOffStats = kOffMisc + 64;           // 4 x u64 counters (probes, fallbacks, keys, merges)
+constexpr uint64_t kOffStats = kOffMisc + 64;           // 8 x u64: probes, fallbacks, keys, merges, phase times
 constexpr uint64_t kWords = kOffStats + 64;
 static_assert(sizeof(PackSync) <= 4 * (kOffChunkState - kOffSync), "pack state region");
 static_assert(2 * (kNATiles / kSSChunk + 2) <= kOffTilePrefix - kOffChunkState, "chunk state region");
@@ -96,7 +96,7 @@ using namespace excl;
 extern "C" int excl_intersect_device_noalloc(excl_index *ix, const uint32_t *d_terms, const uint32_t *d_term_offsets,
                                              uint32_t nq, uint32_t algo, uint32_t *d_offsets, uint32_t *d_docids,
                                              uint64_t cap, void *stream) {
-    if (!ix || !ix->dev || !d_term_offsets || !d_offsets || (!d_docids && cap) || algo > EXCL_ALGO_LEARNED)
+    if (!ix || !ix->dev || !d_term_offsets || !d_offsets || (!d_docids && cap) || algo > EXCL_ALGO_SEGREG)
         return EXCL_E_INVALID;
     if (nq > kNAQueries) return EXCL_E_CAPACITY;
     int dev = -1;
@@ -124,6 +124,7 @@ extern "C" int excl_intersect_device_noalloc(excl_index *ix, const uint32_t *d_t
     b.merge_segs = 2;
     b.max_keys = kNAKeys;
     b.err = base + kOffMisc;
+    b.probe_done = base + kOffMisc + 2;
     b.stats = reinterpret_cast<uint64_t *>(base + kOffStats);
     BatchLaunch L{};
     L.ixv = ix->dev->view(ix->models ? model_view(ix->models) : ModelView{});

@@ -232,7 +232,7 @@ int ctx_alloc_batch(excl_ctx *ctx) {
     st |= dalloc(ctx, &ctx->d_tile_order, (size_t)ctx->max_tiles + 1, "alloc tile order");
     st |= dalloc(ctx, &ctx->d_scratch, (size_t)c.max_keys, "alloc scratch");
     st |= dalloc(ctx, &ctx->d_misc, 16, "alloc misc");
-    st |= dalloc(ctx, &ctx->d_stats, 4, "alloc stats");
+    st |= dalloc(ctx, &ctx->d_stats, 8, "alloc stats");
     st |= dalloc(ctx, &ctx->d_sync, 1, "alloc pack sync");
     st |= dalloc(ctx, &ctx->d_chunk_state, (size_t)ctx->max_tiles / kSSChunk + 2, "alloc chunk states");
     st |= dalloc(ctx, &ctx->d_offsets, (size_t)c.max_queries + 1, "alloc offsets");
@@ -246,7 +246,7 @@ int ctx_alloc_batch(excl_ctx *ctx) {
     if (st) return EXCL_E_NOMEM;
     for (uint32_t i = kFlagSlots; i-- > 0;) ctx->free_flag_slots.push_back(i);
     cudaMemsetAsync(ctx->d_misc, 0, 16 * 4, ctx->stream);
-    cudaMemsetAsync(ctx->d_stats, 0, 4 * 8, ctx->stream);
+    cudaMemsetAsync(ctx->d_stats, 0, 8 * 8, ctx->stream);
     cudaMemsetAsync(ctx->d_sync, 0, sizeof(PackSync), ctx->stream);
     cudaMemsetAsync(ctx->d_chunk_state, 0, ((size_t)ctx->max_tiles / kSSChunk + 2) * 8, ctx->stream);
     return cuda_status(ctx, cudaStreamSynchronize(ctx->stream), "ctx init");
@@ -263,7 +263,7 @@ int run_pipeline(excl_ctx *ctx, excl_index *ix, const uint32_t *d_terms, const u
         ctx_error(ctx, "batch of %u queries exceeds max_queries %u", nq, ctx->cfg.max_queries);
         return EXCL_E_CAPACITY;
     }
-    if (algo > EXCL_ALGO_LEARNED) {
+    if (algo > EXCL_ALGO_SEGREG) {
         ctx_error(ctx, "unknown algo %u", algo);
         return EXCL_E_INVALID;
     }
@@ -287,6 +287,9 @@ int run_pipeline(excl_ctx *ctx, excl_index *ix, const uint32_t *d_terms, const u
     b.max_keys = ctx->cfg.max_keys;
     b.err = ctx->d_misc + kMiscErr;
     b.err_out = err_out;
+    b.probe_done = ctx->d_misc + kMiscProbeDone;
+    b.check_polls = ctx->wait_check_polls;
+    b.check_flag = ctx->d_misc + kMiscNeverSet;
     b.stats = ctx->collect_stats ? ctx->d_stats : nullptr;
     BatchLaunch L{};
     L.ixv = ix->dev->view(ix->models ? model_view(ix->models) : ModelView{});
@@ -304,6 +307,7 @@ int run_pipeline(excl_ctx *ctx, excl_index *ix, const uint32_t *d_terms, const u
     L.warps = ctx->warps;
     L.ctas_per_sm = ctx->ctas_per_sm;
     L.nsm = ctx->nsm;
+    L.spin = ctx->spin_limit;
     L.ev = ctx->ev;
     ctx->last_was_graph = false;
     if (ctx->use_graphs) {
@@ -317,7 +321,8 @@ int run_pipeline(excl_ctx *ctx, excl_index *ix, const uint32_t *d_terms, const u
                                   (uint64_t)(uintptr_t)d_docids, cap,
                                   (uint64_t)ctx->collect_stats | (uint64_t)ctx->merge_segs << 8 |
                                       (uint64_t)ctx->warps << 16 | (uint64_t)ctx->ctas_per_sm << 32 |
-                                      (uint64_t)ctx->tile_split << 40,
+                                      (uint64_t)ctx->tile_split << 40 | (uint64_t)(ctx->spin_limit != 0) << 48 |
+                                      (uint64_t)(ctx->wait_check_polls != 0) << 49,
                                   (uint64_t)(uintptr_t)err_out};
         const bool same = ctx->gkey_seen && std::memcmp(key, ctx->gkey, sizeof key) == 0;
         if (same || ctx->gexec) {
@@ -730,8 +735,8 @@ extern "C" int excl_autotune(excl_ctx *ctx, excl_index *ix, const uint32_t *term
     float best = rep->default_ms;
     uint32_t ba = EXCL_ALGO_AUTO, bm = 2;
     int bw = 8, bc = 5;
-    const uint32_t algos[3] = {EXCL_ALGO_BSEARCH, EXCL_ALGO_HASHSEG, EXCL_ALGO_LEARNED};
-    const int warps[2] = {4, 8}, ctas[3] = {4, 5, 6};
+    const uint32_t algos[4] = {EXCL_ALGO_BSEARCH, EXCL_ALGO_HASHSEG, EXCL_ALGO_SEGREG, EXCL_ALGO_LEARNED};
+    const int warps[1] = {8}, ctas[3] = {4, 5, 6};
     const uint32_t merges[4] = {0u, 1u, 2u, 4u};
     uint32_t tried = 1;
     for (uint32_t a : algos) {
@@ -819,7 +824,7 @@ extern "C" int excl_submit(excl_ctx *ctx, excl_index *ix, const uint32_t *terms,
 extern "C" int excl_ctx_set_tuning(excl_ctx *ctx, const excl_tune_report *rep) {
     if (!ctx || !rep) return EXCL_E_INVALID;
     std::lock_guard<std::recursive_mutex> g(ctx->op_mu);
-    if (rep->algo > EXCL_ALGO_LEARNED || (rep->warps_per_cta != 4 && rep->warps_per_cta != 8) ||
+    if (rep->algo > EXCL_ALGO_SEGREG || (rep->warps_per_cta != 4 && rep->warps_per_cta != 8) ||
         rep->ctas_per_sm < 4 || rep->ctas_per_sm > 6 || rep->tile_split > 2 ||
         (rep->merge_segs != EXCL_MERGE_OFF && (rep->merge_segs == 0 || rep->merge_segs > 4)))
         return EXCL_E_INVALID;
@@ -828,6 +833,13 @@ extern "C" int excl_ctx_set_tuning(excl_ctx *ctx, const excl_tune_report *rep) {
     ctx->merge_segs = rep->merge_segs == EXCL_MERGE_OFF ? 0u : rep->merge_segs;
     ctx->tuned_algo = rep->algo == EXCL_ALGO_AUTO ? -1 : (int)rep->algo;
     ctx->tile_split = rep->tile_split;
+    return EXCL_OK;
+}
+
+extern "C" int excl_ctx_set_wait_check(excl_ctx *ctx, uint32_t polls) {
+    if (!ctx) return EXCL_E_INVALID;
+    std::lock_guard<std::recursive_mutex> g(ctx->op_mu);
+    ctx->wait_check_polls = polls;
     return EXCL_OK;
 }
 
@@ -989,21 +1001,23 @@ extern "C" int excl_last_stats(excl_ctx *ctx, excl_batch_stats *stt) {
     int s = cuda_status(ctx, cudaStreamSynchronize(ctx->stream), "sync");
     if (s) return s;
     std::memset(stt, 0, sizeof *stt);
-    if (!ctx->last_was_graph) {
-        cudaEventElapsedTime(&stt->pack_ms, ctx->ev[0], ctx->ev[1]);
-        cudaEventElapsedTime(&stt->probe_ms, ctx->ev[1], ctx->ev[2]);
-        cudaEventElapsedTime(&stt->compact_ms, ctx->ev[2], ctx->ev[3]);
-    }
     cudaEventElapsedTime(&stt->total_ms, ctx->ev[0], ctx->ev[3]);
     uint32_t T = 0;
     cudaMemcpy(&T, ctx->d_tile_prefix + ctx->last_nq, 4, cudaMemcpyDeviceToHost);
     stt->tiles = T;
-    uint64_t hs[4] = {0, 0, 0, 0};
-    if (ctx->collect_stats) cudaMemcpy(hs, ctx->d_stats, 32, cudaMemcpyDeviceToHost);
+    uint64_t hs[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    if (ctx->collect_stats) cudaMemcpy(hs, ctx->d_stats, sizeof hs, cudaMemcpyDeviceToHost);
     stt->probes = hs[0];
     stt->fallbacks = hs[1];
     stt->keys = hs[2];
     stt->merges = hs[3];
+    // phases of the batch kernel from its globaltimer stamps: start, pack
+    // phase complete, last warp out of the probe loop, last CTA out
+    if (hs[4] && hs[5] >= hs[4] && hs[6] >= hs[5] && hs[7] >= hs[6]) {
+        stt->pack_ms = (float)((double)(hs[5] - hs[4]) * 1e-6);
+        stt->probe_ms = (float)((double)(hs[6] - hs[5]) * 1e-6);
+        stt->compact_ms = (float)((double)(hs[7] - hs[6]) * 1e-6);
+    }
     return EXCL_OK;
 }
 

@@ -31,7 +31,13 @@ struct DeviceIndex {
 };
 
 // slots of ctx->d_misc
-enum { kMiscErr = 0, kMiscTileCounter = 1, kMiscDecodeTicket = 2 /* and 3: decode work counter, CTAs done */ };
+enum {
+    kMiscErr = 0,
+    kMiscTileCounter = 1,
+    kMiscDecodeTicket = 2,  // and 3: decode work counter, CTAs done
+    kMiscProbeDone = 4,     // tiles probed (batch kernel)
+    kMiscNeverSet = 5,      // stays 0: the flag of the failure-path self-test wait
+};
 // excl_submit_into batches that may be in flight on one context at once
 constexpr uint32_t kFlagSlots = 256;
 
@@ -46,6 +52,8 @@ struct excl_ctx {
     uint32_t tile_split = 0;  // log2 of the tiles each fixed segment of a shortest list is cut into
     int tuned_algo = -1;  // search method the autotuner chose for EXCL_ALGO_AUTO (-1: none)
     bool collect_stats = true;
+    uint32_t spin_limit = 0;  // polls before a cross-CTA wait of the batch kernel gives up (0: the default)
+    uint32_t wait_check_polls = 0;  // excl_ctx_set_wait_check
     // CUDA graph of the last batch launched through excl_intersect_device
     bool use_graphs = false, last_was_graph = false;
     cudaGraphExec_t gexec = nullptr;

@@ -141,9 +141,9 @@ struct Slot {
     cudaEvent_t done = nullptr;
     PackSync *d_sync = nullptr;
     uint64_t *d_chunk = nullptr;
-    uint32_t *d_misc = nullptr;                      // error flag, probe work counter
+    uint32_t *d_misc = nullptr;                      // error flag, probe work counter, tiles probed
     uint32_t *h_terms = nullptr, *h_toff = nullptr;  // pinned, mapped: the pack kernel reads them in place
-    uint32_t *h_err = nullptr;                       // pinned, mapped: the batch's error bits, handed over by k_scatter
+    uint32_t *h_err = nullptr;                       // pinned, mapped: the batch's error bits, handed over by the batch kernel's last CTA
     uint32_t *m_terms = nullptr, *m_toff = nullptr, *m_err = nullptr;  // their device addresses
     uint32_t *h_offsets = nullptr, *h_docids = nullptr;  // mapped pinned results
     uint32_t *m_offsets = nullptr, *m_docids = nullptr;  // their device addresses
@@ -234,9 +234,10 @@ int launch_on_slot(excl_server *s, Slot *sl, uint64_t nterms, uint64_t tiles, ui
     uint8_t *base = s->d_pool + sl->pool_off;
     auto at = [&](uint64_t off) { return reinterpret_cast<uint32_t *>(base + off); };
     cudaStream_t st = sl->stream;
-    // no copies: the pack kernel reads the batch's queries from the slot's
-    // mapped host arrays, k_pack_scan resets the tile counter, and k_scatter
-    // hands the error bits to h_err and clears the device word for the next batch
+    // no copies: the batch kernel reads the batch's queries from the slot's
+    // mapped host arrays, its pack phase resets the tile counters, and its
+    // last CTA hands the error bits to h_err and clears the device word for
+    // the next batch
     BatchView b{};
     b.nq = nq;
     b.qterms = at(L.qterms);
@@ -254,6 +255,7 @@ int launch_on_slot(excl_server *s, Slot *sl, uint64_t nterms, uint64_t tiles, ui
     b.max_keys = keys;
     b.err = sl->d_misc;
     b.err_out = sl->m_err;
+    b.probe_done = sl->d_misc + 2;
     b.stats = nullptr;
     BatchLaunch bl{};
     bl.ixv = s->ix->dev->view(s->ix->models ? model_view(s->ix->models) : ModelView{});
@@ -491,7 +493,7 @@ extern "C" int excl_server_create(int device, excl_index *ix, const excl_server_
     if (c.max_batch_queries == 0 || c.max_batch_queries > kPackMaxQueries) c.max_batch_queries = 4096;
     if (c.max_batch_keys == 0) c.max_batch_keys = 1ull << 22;
     if (c.max_batch_keys > 0xffffffffull / 2) c.max_batch_keys = 0xffffffffull / 2;
-    if (c.algo > EXCL_ALGO_LEARNED) c.algo = EXCL_ALGO_AUTO;
+    if (c.algo > EXCL_ALGO_SEGREG) c.algo = EXCL_ALGO_AUTO;
     s->slot_max_tiles = (uint32_t)(c.max_batch_keys / kMinBlock + c.max_batch_queries + 1);
     const uint64_t per_batch =
         ws_layout(c.max_batch_queries, (uint64_t)c.max_batch_queries * 8, s->slot_max_tiles, c.max_batch_keys).total;

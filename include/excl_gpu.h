@@ -45,12 +45,29 @@ typedef enum {
                                   NewPFor.cpp:52-139); decode as NewPFD_Decompression_kernel.cu:322-488 */
 } excl_codec;
 
-/* Search method for locating a probe in a longer list. */
+/* Search method for locating a probe in a longer list. Every method gives the
+ * same (exact) results; they differ in how a probe reaches its docID:
+ * - BSEARCH and HASHSEG are the plain comparators: no position model. They find
+ *   the segment by binary search over the segment heads or by the top-bits
+ *   bucket directory, then binary-search the block's docIDs (the reference's
+ *   uncompressed mqSearch, cuda_binarySearch_kernel.cu:167-296, and
+ *   cuda_hashSegment_kernel.cu:170-314, on the compressed index);
+ * - SEGREG uses the codec's own linear model: the bucket directory, then the
+ *   segment regression's window (SegLRC_Intersection_kernel.cu:366-371,
+ *   LRCSeg_Intersection_kernel.cu:290-302) on SegLRC, LRCSeg and HS_SegLRC lists;
+ * - LEARNED uses the two-stage learned position model with its exact error
+ *   window on lists that have one, and falls back to HASHSEG elsewhere (and
+ *   where a leaf's window exceeds its threshold);
+ * - AUTO: the autotuner's choice when one was made, else the learned model
+ *   where one exists and SEGREG elsewhere.
+ * d-gap codecs (ParaPFD, HS_ParaPFD, NewPFD) have no random access inside a
+ * block: every method walks the block from its head or median there. */
 typedef enum {
-    EXCL_ALGO_AUTO = 0,     /* learned where a model exists, else hash directory */
-    EXCL_ALGO_BSEARCH = 1,  /* binary search over segment heads (cuda_binarySearch_kernel.cu:167-296) */
-    EXCL_ALGO_HASHSEG = 2,  /* top-bits bucket directory (cuda_hashSegment_kernel.cu:170-314) */
-    EXCL_ALGO_LEARNED = 3   /* two-stage learned position model with exact error window */
+    EXCL_ALGO_AUTO = 0,
+    EXCL_ALGO_BSEARCH = 1,
+    EXCL_ALGO_HASHSEG = 2,
+    EXCL_ALGO_LEARNED = 3,
+    EXCL_ALGO_SEGREG = 4
 } excl_algo;
 
 /* ---------------------------------------------------------------------------
@@ -183,7 +200,7 @@ typedef struct {
     uint32_t max_queries;    /* per batch (reference: 16380-word constant image, ParaPFD_Intersection_kernel.cu:134) */
     uint32_t max_terms;      /* per query, <= 32 (reference MAX_QUERY_LEN 80, of which 8 are used by the workloads) */
     uint64_t max_keys;       /* per batch, sum of shortest-list lengths (reference baseSize) */
-    uint32_t warps_per_cta;  /* probe kernel: 4 or 8 warps per CTA (0 = 8) */
+    uint32_t warps_per_cta;  /* batch kernel CTA width: 8 warps (0 = 8; 4 is accepted and runs as 8) */
     uint32_t ctas_per_sm;    /* probe kernel: 4, 5 or 6 resident 8-warp CTAs per SM, i.e. a register
                                 budget of 64, 48 or 40 per thread (0 = 5) */
     uint32_t use_graphs;     /* 1: excl_intersect_device replays a CUDA graph of the batch's three
@@ -286,7 +303,9 @@ int excl_intersect_device_noalloc(excl_index *ix, const uint32_t *d_terms, const
                                   uint32_t nq, uint32_t algo, uint32_t *d_offsets, uint32_t *d_docids, uint64_t cap,
                                   void *stream);
 
-/* Per-kernel timing of the last excl_intersect_device / excl_wait (ms, CUDA events). */
+/* Timing of the last excl_intersect_device / excl_wait batch: total_ms by CUDA
+ * events around the batch kernel; pack_ms, probe_ms and compact_ms are its
+ * three phases (pack, probe, scatter), from the kernel's own globaltimer stamps. */
 typedef struct {
     float pack_ms, probe_ms, compact_ms, total_ms;
     uint64_t tiles;     /* (query, tile) work items */
@@ -299,8 +318,9 @@ int excl_last_stats(excl_ctx *ctx, excl_batch_stats *st);
 
 /* Autotuner (no counterpart in the reference, which fixes one launch shape per
  * binary). Runs a sample batch (host arrays, as excl_submit) under every
- * candidate setting: search method (bsearch, hash directory, learned where
- * models exist), probe launch shape (warps per CTA x CTAs per SM) and merge
+ * candidate setting: search method (bsearch, hash directory, segment
+ * regression windows, learned where models exist), batch kernel launch shape (8-warp CTAs per SM: 4, 5 or 6, i.e. a
+ * register budget of 64, 48 or 40 per thread) and merge
  * threshold (EXCL_MERGE_OFF, 1, 2, 4 segments); then, for the best of those,
  * tiles of whole segments or of halves / quarters of them. Each candidate is timed with
  * CUDA events (median of 3 after a warm-up); the fastest is kept in the
@@ -316,11 +336,21 @@ typedef struct {
 int excl_autotune(excl_ctx *ctx, excl_index *ix, const uint32_t *terms, const uint32_t *term_offsets, uint32_t nq,
                   excl_tune_report *report);
 /* Applies a setting (a report of an earlier excl_autotune, or one the caller
- * fills: algo, warps_per_cta 4 or 8, ctas_per_sm 4-6, merge_segs 1-4 or
+ * fills: algo, warps_per_cta 8 (4 is accepted), ctas_per_sm 4-6, merge_segs 1-4 or
  * EXCL_MERGE_OFF, tile_split 0-2) to the context without timing anything, so a
  * host can keep its tuning across runs. EXCL_E_INVALID for values outside
  * those ranges. */
 int excl_ctx_set_tuning(excl_ctx *ctx, const excl_tune_report *setting);
+
+/* Self-test of the device failure path (no counterpart in the reference, whose
+ * kernels exit() the process on any error). With polls > 0 every later batch of
+ * the context also runs one bounded device wait on a flag that nothing sets; it
+ * gives up after `polls` polls and raises the same error bit as an expired
+ * cross-CTA wait of the batch kernel, so the batch completes, its results are
+ * still exact, and excl_wait / excl_ctx_check report EXCL_E_DEVICE_FLAG ("scan
+ * wait expired"). The context stays usable; polls = 0 (the default) turns the
+ * check off. Faults nothing and hangs nothing: every device wait is bounded. */
+int excl_ctx_set_wait_check(excl_ctx *ctx, uint32_t polls);
 
 /* ---------------------------------------------------------------------------
  * Serving loop: continuous batching of single queries. No counterpart in the
@@ -341,7 +371,7 @@ typedef struct {
     uint64_t max_batch_keys;    /* shortest-list docIDs per batch, 0 = 2^22; a query above it is rejected */
     uint64_t hbm_budget_bytes;  /* working-set pool shared by the slots, 0 = room for every slot's largest batch */
     uint32_t algo;              /* EXCL_ALGO_* */
-    uint32_t warps_per_cta;     /* probe launch shape, 0 = default */
+    uint32_t warps_per_cta;     /* batch kernel CTA width: 8 warps (0 = default) */
     uint32_t ctas_per_sm;
 } excl_server_config;
 

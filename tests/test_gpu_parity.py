@@ -11,7 +11,7 @@ pytestmark = pytest.mark.gpu
 
 FORMATS = ["parapfd", "lrc", "lrcseg", "seglrc", "hs_seglrc", "hs_parapfd", "newpfd"]
 DGAP = ("parapfd", "newpfd")  # exercised with FRAC 0.1 and 128-entry blocks (exceptions)
-ALGOS = ["bsearch", "hashseg", "auto"]
+ALGOS = ["bsearch", "hashseg", "segreg", "auto"]
 
 
 def _index(w, codec, block=256, frac=0.0, ubits=24):
@@ -211,7 +211,7 @@ def test_autotune_keeps_output_exact(corpus, expected):
     try:
         rep = ctx.autotune(ix, corpus.terms[:int(corpus.term_offsets[500])], corpus.term_offsets[:501])
         assert rep["tried"] > 10
-        assert rep["algo"] in ("bsearch", "hashseg", "learned", "auto")
+        assert rep["algo"] in ("bsearch", "hashseg", "segreg", "learned", "auto")
         assert rep["warps_per_cta"] in (4, 8) and rep["ctas_per_sm"] in (4, 5, 6)
         assert 0 < rep["best_ms"] <= rep["default_ms"]
         assert rep["tile_split"] in (0, 1, 2)

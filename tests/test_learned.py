@@ -104,7 +104,7 @@ def test_learned_windows_are_exact_and_probes_bit_exact(gpu_ctx, long_lists, cod
     terms = np.array([t for l in range(nl) for t in (nl + l, l)], np.uint32)
     toff = np.arange(0, 2 * nl + 1, 2, dtype=np.uint32)
     eo, ed = oracle.answer(all_docs, all_off, terms, toff)
-    for algo in ("learned", "auto", "hashseg"):
+    for algo in ("learned", "auto", "hashseg", "segreg", "bsearch"):
         offs, got = gpu_ctx.intersect(ix2, terms, toff, algo=algo)
         assert np.array_equal(offs.astype(np.uint64), eo) and np.array_equal(got, ed), algo
     ix.close()
