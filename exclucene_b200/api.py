@@ -149,6 +149,16 @@ _qencode = _sig("excl_query_encode", C.c_int, u32p, u32p, C.c_uint32, C.c_void_p
 _autotune = _sig("excl_autotune", C.c_int, C.c_void_p, C.c_void_p, u32p, u32p, C.c_uint32, C.POINTER(TuneReport))
 _set_tuning = _sig("excl_ctx_set_tuning", C.c_int, C.c_void_p, C.POINTER(TuneReport))
 _set_wait_check = _sig("excl_ctx_set_wait_check", C.c_int, C.c_void_p, C.c_uint32)
+
+
+class LayoutCandidate(C.Structure):
+    _fields_ = [("build", BuildParams), ("best_ms", C.c_float), ("tuning", TuneReport),
+                ("device_bytes", C.c_uint64), ("status", C.c_int)]
+
+
+_tune_layout = _sig("excl_autotune_layout", C.c_int, C.c_void_p, C.c_void_p, u64p, C.c_uint32,
+                    C.POINTER(LayoutCandidate), C.c_uint32, u32p, u32p, C.c_uint32, C.POINTER(C.c_uint32),
+                    C.POINTER(C.c_void_p))
 _learn = _sig("excl_learn_models", C.c_int, C.c_void_p, C.c_void_p, C.POINTER(LearnParams), C.POINTER(LearnReport))
 _mexport = _sig("excl_model_export", C.c_int, C.c_void_p, C.c_uint32, C.POINTER(C.c_float), C.POINTER(C.c_float),
                 C.POINTER(C.c_int32), C.POINTER(C.c_uint32))
@@ -162,7 +172,8 @@ EXPORTED = ["excl_learn_models", "excl_model_export", "excl_model_grad", "excl_m
             "excl_ctx_destroy", "excl_last_error", "excl_ctx_stream", "excl_index_upload",
             "excl_decode_lists_device", "excl_decode_lists", "excl_submit", "excl_wait", "excl_batch_free",
             "excl_intersect_device", "excl_ctx_check", "excl_last_stats", "excl_checksum", "excl_submit_into",
-            "excl_host_alloc", "excl_host_free", "excl_ctx_set_tuning", "excl_ctx_set_wait_check"]
+            "excl_host_alloc", "excl_host_free", "excl_ctx_set_tuning", "excl_ctx_set_wait_check",
+            "excl_autotune_layout"]
 
 
 def _p32(a: np.ndarray):
@@ -476,6 +487,34 @@ class Context:
         _check_status(_build_dev(self._h, C.c_void_p(d_docs), loff.ctypes.data_as(u64p), len(loff) - 1, C.byref(p),
                                  C.byref(h)), self, "excl_index_build_device")
         return Index.from_handle(h, len(loff) - 1, np.diff(loff))
+
+    def autotune_layout(self, d_docs: int, list_offsets, candidates, terms, term_offsets):
+        """excl_autotune_layout: builds the corpus (device docID array d_docs,
+        CSR list_offsets) on the GPU under each candidate layout (dicts with
+        build_index's keywords: codec, block, frac, hs_bucket, hs_kbits,
+        hs_ubits), tunes and times the sample batch on each, and keeps the
+        fastest. Returns (index of the chosen layout, uploaded; its position in
+        `candidates`; one dict per candidate with its time, size, tuning and
+        status)."""
+        loff = np.ascontiguousarray(list_offsets, dtype=np.uint64)
+        arr = (LayoutCandidate * len(candidates))()
+        for c, kw in zip(arr, candidates):
+            c.build.codec = CODEC_NAMES[kw.get("codec", "seglrc")]
+            c.build.block = kw.get("block", 256)
+            c.build.frac = kw.get("frac", 0.0)
+            c.build.hs_bucket = kw.get("hs_bucket", 256)
+            c.build.hs_kbits = kw.get("hs_kbits", 0)
+            c.build.hs_ubits = kw.get("hs_ubits", 32)
+        t = _u32(terms) if len(terms) else np.zeros(1, dtype=np.uint32)
+        o = _u32(term_offsets)
+        best = C.c_uint32(0)
+        h = C.c_void_p()
+        _check_status(_tune_layout(self._h, C.c_void_p(d_docs), loff.ctypes.data_as(u64p), len(loff) - 1, arr,
+                                   len(candidates), _p32(t), _p32(o), len(o) - 1, C.byref(best), C.byref(h)),
+                      self, "excl_autotune_layout")
+        report = [dict(kw, best_ms=c.best_ms, device_bytes=int(c.device_bytes), status=int(c.status),
+                       tuning=c.tuning.as_dict() if c.status == OK else None) for c, kw in zip(arr, candidates)]
+        return Index.from_handle(h, len(loff) - 1, np.diff(loff)), int(best.value), report
 
     def set_wait_check(self, polls: int) -> None:
         """excl_ctx_set_wait_check: polls > 0 makes every later batch run one

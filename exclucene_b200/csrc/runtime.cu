@@ -836,6 +836,53 @@ extern "C" int excl_ctx_set_tuning(excl_ctx *ctx, const excl_tune_report *rep) {
     return EXCL_OK;
 }
 
+extern "C" int excl_autotune_layout(excl_ctx *ctx, const uint32_t *d_docs, const uint64_t *list_offsets,
+                                    uint32_t nlists, excl_layout_candidate *cands, uint32_t ncands,
+                                    const uint32_t *terms, const uint32_t *term_offsets, uint32_t nq, uint32_t *best,
+                                    excl_index **out) {
+    if (!ctx || !d_docs || !list_offsets || !cands || !ncands || !term_offsets || !best || !out) return EXCL_E_INVALID;
+    *out = nullptr;
+    std::lock_guard<std::recursive_mutex> g(ctx->op_mu);
+    excl_index *keep = nullptr;
+    uint32_t kb = ncands;
+    for (uint32_t i = 0; i < ncands; ++i) {
+        excl_layout_candidate &c = cands[i];
+        c.best_ms = 0.0f;
+        c.device_bytes = 0;
+        std::memset(&c.tuning, 0, sizeof c.tuning);
+        excl_index *ix = nullptr;
+        c.status = excl_index_build_device(ctx, d_docs, list_offsets, nlists, &c.build, &ix);
+        if (!c.status) c.status = excl_index_upload(ctx, ix);
+        if (!c.status) c.status = excl_autotune(ctx, ix, terms, term_offsets, nq, &c.tuning);
+        if (!c.status) {
+            excl_index_sizes sz{};
+            excl_index_sizes_get(ix, &sz);
+            c.device_bytes = sz.device_bytes;
+            c.best_ms = c.tuning.best_ms;
+        }
+        if (!c.status && (kb == ncands || c.best_ms < cands[kb].best_ms)) {
+            if (keep) excl_index_free(keep);
+            keep = ix;
+            kb = i;
+        } else if (ix) {
+            excl_index_free(ix);
+        }
+    }
+    if (!keep) {
+        ctx_error(ctx, "excl_autotune_layout: no candidate layout could be built and timed");
+        return EXCL_E_INVALID;
+    }
+    // the context keeps the chosen layout's launch setting
+    const int s = excl_ctx_set_tuning(ctx, &cands[kb].tuning);
+    if (s) {
+        excl_index_free(keep);
+        return s;
+    }
+    *best = kb;
+    *out = keep;
+    return EXCL_OK;
+}
+
 extern "C" int excl_ctx_set_wait_check(excl_ctx *ctx, uint32_t polls) {
     if (!ctx) return EXCL_E_INVALID;
     std::lock_guard<std::recursive_mutex> g(ctx->op_mu);

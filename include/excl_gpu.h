@@ -342,6 +342,29 @@ int excl_autotune(excl_ctx *ctx, excl_index *ix, const uint32_t *terms, const ui
  * those ranges. */
 int excl_ctx_set_tuning(excl_ctx *ctx, const excl_tune_report *setting);
 
+/* Index-layout autotuner (no counterpart in the reference, which fixes the
+ * layout per binary: SegmentSize 256 in its encoders, the HS bucket shift
+ * derived from the list length at HS_SegLRC_Generator.cu:554-557). For each
+ * candidate layout (codec, block size, FRAC, HS top-k bits ...) it builds the
+ * corpus on the GPU (excl_index_build_device), uploads it, runs
+ * excl_autotune on the sample batch and records the tuned time; the layout
+ * with the lowest time is kept: *out receives that index (uploaded, owned by
+ * the caller), *best its candidate number, and the context keeps its launch
+ * tuning. The other candidates' indexes are freed. d_docs and list_offsets as
+ * for excl_index_build_device; the sample as for excl_autotune. A candidate
+ * that cannot be built (format limits, NewPFD) records its status and is
+ * skipped; EXCL_E_INVALID if none can. Every layout gives the same results. */
+typedef struct {
+    excl_build_params build;  /* the layout (in) */
+    float best_ms;            /* its tuned device time for the sample (out) */
+    excl_tune_report tuning;  /* the launch setting excl_autotune chose for it (out) */
+    uint64_t device_bytes;    /* its resident size (out) */
+    int status;               /* EXCL_OK, or why it was skipped (out) */
+} excl_layout_candidate;
+int excl_autotune_layout(excl_ctx *ctx, const uint32_t *d_docs, const uint64_t *list_offsets, uint32_t nlists,
+                         excl_layout_candidate *cands, uint32_t ncands, const uint32_t *terms,
+                         const uint32_t *term_offsets, uint32_t nq, uint32_t *best, excl_index **out);
+
 /* Self-test of the device failure path (no counterpart in the reference, whose
  * kernels exit() the process on any error). With polls > 0 every later batch of
  * the context also runs one bounded device wait on a flag that nothing sets; it

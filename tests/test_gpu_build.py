@@ -119,3 +119,33 @@ def test_device_build_rejects_unordered_lists(gpu_ctx):
         assert e.value.status == ex.api.E_INVALID
     with pytest.raises(ex.ExclError):
         gpu_ctx.build_index(d.data_ptr(), np.array([0, 4, 7], np.uint64), codec="newpfd")  # host build only
+
+
+def test_layout_autotuner_keeps_the_fastest_exact_layout(gpu_ctx):
+    """excl_autotune_layout builds each candidate layout on the GPU, tunes and
+    times the sample on it, and hands back the fastest one, uploaded; that
+    index answers as the oracle does, and so would every other candidate."""
+    import torch
+
+    w = synth.skewed(seed=77, nq=300, npool=6, long_min=200_000, long_max=800_000)
+    d_docs = torch.from_numpy(w.docs.view(np.int32)).to("cuda:0")
+    torch.cuda.synchronize()
+    cands = [dict(codec="hs_parapfd", block=128, frac=0.1, hs_kbits=k, hs_ubits=26) for k in (8, 12, 16)]
+    cands += [dict(codec="seglrc", block=256), dict(codec="parapfd", block=128, frac=0.1)]
+    ix, best, rep = gpu_ctx.autotune_layout(d_docs.data_ptr(), w.list_offsets, cands, w.terms, w.term_offsets)
+    assert all(r["status"] == 0 and r["best_ms"] > 0 for r in rep), rep
+    assert rep[best]["best_ms"] == min(r["best_ms"] for r in rep)
+    eo, ed = oracle.answer(w.docs, w.list_offsets, w.terms, w.term_offsets)
+    offs, docs = gpu_ctx.intersect(ix, w.terms, w.term_offsets, algo="auto")
+    assert np.array_equal(offs.astype(np.uint64), eo) and np.array_equal(docs, ed)
+    # the same layout built on the host is the same index
+    host = ex.Index(w.docs, w.list_offsets, **{k: v for k, v in cands[best].items()})
+    _same_index(ix, host)
+    ix.close()
+    host.close()
+    # NewPFD has no device build: recorded as skipped, the others still run
+    ix, best, rep = gpu_ctx.autotune_layout(d_docs.data_ptr(), w.list_offsets,
+                                            [dict(codec="newpfd", block=128), dict(codec="seglrc", block=256)],
+                                            w.terms, w.term_offsets)
+    assert rep[0]["status"] != 0 and rep[1]["status"] == 0 and best == 1
+    ix.close()

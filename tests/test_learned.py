@@ -124,3 +124,43 @@ def test_training_narrows_the_windows(gpu_ctx, long_lists):
     assert trained["final_loss"] < untrained["final_loss"]
     assert trained["mean_window"] < untrained["mean_window"]
     ix.close()
+
+
+@pytest.mark.gpu
+def test_learned_beats_the_plain_methods(gpu_ctx):
+    """What the trained model gains over the method without it: on a fixed
+    batch of probe-key lists ANDed with long SegLRC lists, the learned probe
+    (model window, then a search inside it) takes less device time than both
+    plain comparators (binary search over the heads or the bucket directory,
+    then a binary search over the block), with bit-exact output for all three.
+    Times are medians of 5 batches after a warm-up (CUDA events)."""
+    lens = [3_000_000, 2_000_000, 4_000_000, 1_500_000]
+    t = synth.uniform_lists(lens, ubits=28, seed=21)
+    rng = np.random.default_rng(22)
+    keys = []
+    for q in range(400):
+        l = q % len(lens)
+        lst = t.docs[t.list_offsets[l]:t.list_offsets[l + 1]]
+        k = np.unique(np.concatenate([rng.choice(lst, 6000, replace=False),
+                                      rng.integers(0, 1 << 28, 6000, dtype=np.uint64).astype(np.uint32)]))
+        keys.append(k.astype(np.uint32))
+    docs = np.concatenate([t.docs] + keys)
+    loff = np.concatenate([t.list_offsets, t.list_offsets[-1] + np.cumsum([len(k) for k in keys])]).astype(np.uint64)
+    nl = len(lens)
+    terms = np.array([x for q in range(400) for x in (nl + q, q % nl)], np.uint32)
+    toff = np.arange(0, 801, 2, dtype=np.uint32)
+    ix = ex.Index(docs, loff, codec="seglrc")
+    gpu_ctx.upload(ix)
+    gpu_ctx.learn(ix, min_postings=1_000_000, steps=300, batch=16384)
+    eo, ed = oracle.answer(docs, loff, terms, toff)
+    ms = {}
+    for algo in ("learned", "bsearch", "hashseg"):
+        offs, got = gpu_ctx.intersect(ix, terms, toff, algo=algo)
+        assert np.array_equal(offs.astype(np.uint64), eo) and np.array_equal(got, ed), algo
+        runs = []
+        for _ in range(5):
+            gpu_ctx.intersect(ix, terms, toff, algo=algo)
+            runs.append(gpu_ctx.stats().total_ms)
+        ms[algo] = float(np.median(runs))
+    assert ms["learned"] < min(ms["bsearch"], ms["hashseg"]), ms
+    ix.close()
