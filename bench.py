@@ -65,6 +65,7 @@ def parse():
                    help="lists with at least this many postings get a learned model (default per workload)")
     p.add_argument("--no-learn", action="store_true")
     p.add_argument("--no-serve", action="store_true", help="skip the serving-loop latency measurement")
+    p.add_argument("--no-layout-tune", action="store_true", help="skip the index-layout autotuner")
     return p.parse_args()
 
 
@@ -117,6 +118,14 @@ def make_workload(name: str, scale: float, gen=None, nq_factor: int = 1):
             f"serving corpus: {total:.2e} postings over {nterms} terms (Zipf(1) dfs, 2^28 universe), ParaPFD "
             f"below 1e4 postings else SegLRC; {nq} queries of 2-8 terms ~ df^0.5")
     raise ValueError(name)
+
+
+# Candidate index layouts for the layout autotuner, per workload: the skewed
+# workload's HS top-k bits (8..16), the Zipf corpus's codec and block size.
+LAYOUT_CANDIDATES = {
+    "skewed": lambda p: [dict(p, hs_kbits=k) for k in (8, 10, 12, 14, 16)],
+    "zipf": lambda p: [dict(codec=c, block=b, frac=p["frac"]) for c in ("seglrc", "parapfd") for b in (256, 128)],
+}
 
 
 def query_postings(w) -> int:
@@ -438,12 +447,31 @@ def main():
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
 
-    t_build = time.perf_counter()
-    ix = ex.Index(w.docs, w.list_offsets, **params)
-    host_build_s = time.perf_counter() - t_build
     lens = np.diff(w.list_offsets).astype(np.int64)
     shortest = sum(int(min(lens[w.terms[w.term_offsets[q]:w.term_offsets[q + 1]]], default=0)) for q in range(w.nq))
     ctx = ex.Context(local, max_queries=max(w.nq, 1024), max_keys=max(1 << 20, 2 * shortest))
+    layout = None
+    if not args.no_layout_tune and args.workload in LAYOUT_CANDIDATES and "codecs" not in params:
+        # index-layout autotuner on this batch: candidate layouts built on the
+        # GPU, each tuned and timed; for the skewed workload (HS top-k bits
+        # 8..16 autotuned) the chosen layout is the one measured below, for the
+        # others the named layout is kept and the tuner's result is reported
+        d_all = torch.from_numpy(w.docs.view(np.int32)).to(dev)
+        torch.cuda.synchronize()
+        cands = LAYOUT_CANDIDATES[args.workload](params)
+        t0 = time.perf_counter()
+        lix, lbest, lrep = ctx.autotune_layout(d_all.data_ptr(), w.list_offsets, cands, w.terms, w.term_offsets)
+        lix.close()
+        del d_all
+        layout = {"candidates": [{k: v for k, v in r.items() if k != "tuning"} | {"algo": (r["tuning"] or {}).get("algo")}
+                                 for r in lrep], "chosen": lbest, "wall_s": time.perf_counter() - t0,
+                  "applied": args.workload == "skewed"}
+        if args.workload == "skewed":
+            params.update({k: v for k, v in cands[lbest].items()})
+        ctx.set_tuning(algo="auto", warps_per_cta=8, ctas_per_sm=5, merge_segs=2, tile_split=0)  # back to defaults
+    t_build = time.perf_counter()
+    ix = ex.Index(w.docs, w.list_offsets, **params)
+    host_build_s = time.perf_counter() - t_build
     ctx.upload(ix)
     learn = None
     if not args.no_learn:
@@ -663,6 +691,7 @@ def main():
         if "learned" in per_algo and "segreg" in per_algo else None,
         "learned_models": learn,
         "index_build": index_build,
+        "layout_tune": layout,
         "autotune": tune,
         "per_algo_postings_per_s": {a: job_postings / (min(per_algo[a][0], per_algo_graph[a][0]) / 1e3)
                                     for a in per_algo},
