@@ -471,7 +471,7 @@ class Context:
 
     def build_index(self, d_docs: int, list_offsets, codec="seglrc", block: int = 256, frac: float = 0.0,
                     hs_bucket: int = 256, hs_kbits: int = 0, hs_ubits: int = 32) -> Index:
-        """Build an index (ParaPFD, LRC, LRCSeg, SegLRC, HS_SegLRC or HS_ParaPFD)
+        """Build an index (ParaPFD, NewPFD, LRC, LRCSeg, SegLRC, HS_SegLRC or HS_ParaPFD)
         on this context's GPU from a device docID array (pointer; list l =
         d_docs[list_offsets[l] .. list_offsets[l+1])). Byte-identical to
         Index(docs, list_offsets, ...) with the same parameters; upload it before use."""

@@ -240,9 +240,60 @@ __global__ void __launch_bounds__(kBuildWarps * 32) k_lrc_min(const uint32_t *__
 }
 
 struct Plan {
-    uint32_t lb, eb, hb, en;  // block parameters
+    uint32_t lb, eb, hb, en;  // block parameters (NewPFD: eb = the Simple-16 stream's words, hb unused)
     uint32_t words;           // block size
 };
+
+// Value k of a NewPFD block's exception stream (NewPFor.cpp:91-106): the en
+// position codes (the first position, then gaps minus one), then the en high
+// parts, from the exceptions in element order.
+__device__ __forceinline__ uint32_t newpfd_stream_value(const uint32_t *xp, const uint32_t *xh, uint32_t en,
+                                                        uint32_t k) {
+    if (k >= en) return xh[k - en];
+    return k ? xp[k] - xp[k - 1] - 1u : xp[0];
+}
+
+// Width of value j of Simple-16 layout k.
+__device__ __forceinline__ uint32_t s16_width(uint32_t k, uint32_t j) {
+    const uint32_t c0 = kS16Dev[k][0], c1 = kS16Dev[k][2];
+    return j < c0 ? kS16Dev[k][1] : (j < c0 + c1 ? kS16Dev[k][3] : kS16Dev[k][5]);
+}
+
+// The Simple-16 packing of a NewPFD block's exception stream, warp-parallel
+// over the layouts: for each word, lane k < 16 tests layout k on the next
+// values and the first layout (in table order) that holds them is taken, as
+// the sequential encoder takes it (NewPFor.cpp, Simple16.h). Writes the words
+// to `out` and returns their count, or ~0u when a value needs more than 28
+// bits. Every lane of the warp calls it.
+__device__ uint32_t s16_pack_warp(const uint32_t *xp, const uint32_t *xh, uint32_t en, uint32_t *out, uint32_t lane) {
+    const uint32_t V = 2u * en;
+    uint32_t i = 0, nw = 0;
+    while (i < V) {
+        bool fits = false;
+        uint32_t vol = 0;
+        if (lane < 16u) {
+            const uint32_t total = (uint32_t)kS16Dev[lane][0] + kS16Dev[lane][2] + kS16Dev[lane][4];
+            vol = min(total, V - i);
+            fits = true;
+            for (uint32_t j = 0; j < vol && fits; ++j)
+                fits = newpfd_stream_value(xp, xh, en, i + j) < (1u << s16_width(lane, j));
+        }
+        const uint32_t m = __ballot_sync(0xffffffffu, fits);
+        if (!m) return ~0u;
+        const uint32_t k = (uint32_t)(__ffs(m) - 1);
+        if (lane == k) {
+            uint32_t wv = k << 28, sh = 0;
+            for (uint32_t j = 0; j < vol; ++j) {
+                wv |= newpfd_stream_value(xp, xh, en, i + j) << sh;
+                sh += s16_width(k, j);
+            }
+            out[nw] = wv;
+        }
+        i += __shfl_sync(0xffffffffu, vol, k);
+        ++nw;
+    }
+    return nw;
+}
 
 // One warp per segment of any length. vals (per element) receives the values
 // to pack; ex_pos / ex_high (per element, in the segment's own range) its
@@ -256,7 +307,8 @@ __global__ void __launch_bounds__(kBuildWarps * 32) k_block_plan(const uint32_t 
                                                                  uint32_t *__restrict__ ex_pos,
                                                                  uint32_t *__restrict__ ex_high,
                                                                  uint32_t *__restrict__ head, uint32_t *__restrict__ aux,
-                                                                 Plan *__restrict__ plan, uint32_t *__restrict__ err) {
+                                                                 Plan *__restrict__ plan, uint32_t *__restrict__ s16w,
+                                                                 uint32_t *__restrict__ err) {
     __shared__ uint32_t s_hist[kBuildWarps][33];
     const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
     const uint32_t g = blockIdx.x * kBuildWarps + w;
@@ -356,7 +408,18 @@ __global__ void __launch_bounds__(kBuildWarps * 32) k_block_plan(const uint32_t 
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) orh |= __shfl_xor_sync(0xffffffffu, orh, o);
         p.en = en;
-        if (en) {
+        if (en && codec == EXCL_CODEC_NEWPFD) {
+            // NewPFD: the exceptions go to one Simple-16 stream, packed here
+            // into the segment's scratch slot (2 words per element is enough)
+            __syncwarp();  // the exception lists are written
+            const uint32_t nw = en > 0xffffu ? ~0u : s16_pack_warp(xp, xh, en, s16w + 2 * (lo + s0), lane);
+            if (nw == ~0u) {
+                if (lane == 0) atomicOr(err, kErrBuildFormat);
+                p.en = 0;
+            } else {
+                p.eb = nw;
+            }
+        } else if (en) {
             p.eb = nbits_d(last);
             p.hb = nbits_d(orh);
             // not representable in the descriptor (ParaPFor.cpp:79-88: eb from the last position, hb from the highs, 5-bit fields)
@@ -367,7 +430,9 @@ __global__ void __launch_bounds__(kBuildWarps * 32) k_block_plan(const uint32_t 
         }
     }
     p.words = 1u + (uint32_t)(((uint64_t)n * p.lb + 31u) >> 5);
-    if (p.en) p.words += (uint32_t)(((uint64_t)p.en * p.eb + 31u) >> 5) + (uint32_t)(((uint64_t)p.en * p.hb + 31u) >> 5);
+    if (p.en && codec == EXCL_CODEC_NEWPFD) p.words += p.eb;
+    else if (p.en)
+        p.words += (uint32_t)(((uint64_t)p.en * p.eb + 31u) >> 5) + (uint32_t)(((uint64_t)p.en * p.hb + 31u) >> 5);
     if (lane == 0) plan[g] = p;
 }
 
@@ -392,6 +457,7 @@ __global__ void __launch_bounds__(kBuildWarps * 32) k_block_pack(const uint32_t 
                                                                  const uint32_t *__restrict__ ex_high, SegTab t,
                                                                  uint32_t nsegs, const Plan *__restrict__ plan,
                                                                  const uint64_t *__restrict__ gword,
+                                                                 const uint32_t *__restrict__ s16w, uint32_t codec,
                                                                  uint32_t *__restrict__ words) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t g = blockIdx.x * kBuildWarps + (threadIdx.x >> 5);
@@ -401,12 +467,18 @@ __global__ void __launch_bounds__(kBuildWarps * 32) k_block_pack(const uint32_t 
     const uint64_t e0 = t.list_off[t.seg_list[g]] + t.seg_start[g];
     uint32_t *blk = words + gword[g];
     const uint32_t wl = (uint32_t)(((uint64_t)n * p.lb + 31u) >> 5);
-    if (lane == 0) blk[0] = p.en ? (p.lb << 26) + (p.eb << 21) + (p.hb << 16) + p.en : (p.lb << 26);
+    const bool npfd = codec == EXCL_CODEC_NEWPFD;
+    // descriptors: ParaPFor.cpp:88-91; NewPFD b << 26 | en (NewPFor.cpp:52-139)
+    if (lane == 0) blk[0] = p.en ? (npfd ? (p.lb << 26) + p.en : (p.lb << 26) + (p.eb << 21) + (p.hb << 16) + p.en)
+                                 : (p.lb << 26);
     if (p.lb) {
         const uint32_t mask = (1u << p.lb) - 1u;  // lb <= 31
         for (uint32_t k = lane; k < wl; k += 32) blk[1 + k] = packed_word(vals + e0, n, p.lb, mask, k);
     }
-    if (p.en) {
+    if (p.en && npfd) {
+        const uint32_t *src = s16w + 2 * e0;
+        for (uint32_t k = lane; k < p.eb; k += 32) blk[1 + wl + k] = src[k];
+    } else if (p.en) {
         const uint32_t we = (uint32_t)(((uint64_t)p.en * p.eb + 31u) >> 5);
         const uint32_t wh = (uint32_t)(((uint64_t)p.en * p.hb + 31u) >> 5);
         if (p.eb)
@@ -445,7 +517,7 @@ struct Scratch {
 
 bool device_codec(uint32_t c) {
     return c == EXCL_CODEC_PARAPFD || c == EXCL_CODEC_SEGLRC || c == EXCL_CODEC_LRC || c == EXCL_CODEC_LRCSEG ||
-           c == EXCL_CODEC_HS_SEGLRC || c == EXCL_CODEC_HS_PARAPFD;
+           c == EXCL_CODEC_HS_SEGLRC || c == EXCL_CODEC_HS_PARAPFD || c == EXCL_CODEC_NEWPFD;
 }
 
 }  // namespace
@@ -554,6 +626,8 @@ extern "C" int excl_index_build_device(excl_ctx *ctx, const uint32_t *d_docs, co
         !sc.get(&d_lreg, nlists) || !sc.get(&d_lmin, nlists) || !sc.get(&d_vals, npost) ||
         !sc.get(&d_xpos, npost) || !sc.get(&d_xhigh, npost))
         return EXCL_E_NOMEM;
+    uint32_t *d_s16 = nullptr;  // NewPFD: each segment's Simple-16 exception stream, 2 words per element
+    if (codec == EXCL_CODEC_NEWPFD && !sc.get(&d_s16, 2 * npost)) return EXCL_E_NOMEM;
     const std::vector<int32_t> lmin_init(nlists, INT_MAX);
     e = cudaMemcpyAsync(d_slist, seg_list.data(), (size_t)ns * 4, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(d_sstart, seg_start.data(), (size_t)ns * 4, cudaMemcpyHostToDevice, st);
@@ -649,7 +723,7 @@ extern "C" int excl_index_build_device(excl_ctx *ctx, const uint32_t *d_docs, co
     }
     if (e == cudaSuccess) {
         k_block_plan<<<pgrid, kBuildWarps * 32, 0, st>>>(docs0, t, ns, codec, p->frac, d_reg, d_lreg, d_lmin, d_vals,
-                                                         d_xpos, d_xhigh, d_head, d_aux, d_plan, d_err);
+                                                         d_xpos, d_xhigh, d_head, d_aux, d_plan, d_s16, d_err);
         e = cudaGetLastError();
     }
     // block offsets: a scan of the block sizes (host; 20 bytes per segment)
@@ -665,7 +739,7 @@ extern "C" int excl_index_build_device(excl_ctx *ctx, const uint32_t *d_docs, co
             ctx_error(ctx, "posting lists are not strictly increasing");
             return EXCL_E_INVALID;
         }
-        ctx_error(ctx, "a block is not representable in ParaPFD or a residual spread exceeds 31 bits");
+        ctx_error(ctx, "a block is not representable (ParaPFD or NewPFD limits) or a residual spread exceeds 31 bits");
         return EXCL_E_FORMAT;
     }
     std::vector<uint64_t> gword(ns + 1, 0);
@@ -677,7 +751,8 @@ extern "C" int excl_index_build_device(excl_ctx *ctx, const uint32_t *d_docs, co
     e = cudaMemcpyAsync(d_gword, gword.data(), gword.size() * 8, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(d_words, 0, (gword[ns] + kWordPad) * 4, st);
     if (e == cudaSuccess) {
-        k_block_pack<<<pgrid, kBuildWarps * 32, 0, st>>>(d_vals, d_xpos, d_xhigh, t, ns, d_plan, d_gword, d_words);
+        k_block_pack<<<pgrid, kBuildWarps * 32, 0, st>>>(d_vals, d_xpos, d_xhigh, t, ns, d_plan, d_gword, d_s16, codec,
+                                                         d_words);
         e = cudaGetLastError();
     }
     // the host image

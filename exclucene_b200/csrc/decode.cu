@@ -50,7 +50,8 @@ struct alignas(16) RunMeta {
     uint32_t count, start, aux, head, list;
     float a, b;
     uint32_t codec, r0, r1;  // the list's codec and list-level regression words
-    uint32_t pad[3];
+    uint32_t bw;             // the block's words
+    uint32_t pad[2];
 };
 
 struct DecodeSmem {
@@ -153,6 +154,7 @@ __device__ void plan_run(const DevIndexView &ix, DecodeSmem &sm, uint32_t b, uin
         m.codec = codec;
         m.r0 = r0;
         m.r1 = r1;
+        m.bw = (uint32_t)bw;
     }
     // width classes: a segment of c values takes G = 2^lg lanes, the smallest
     // power of two with c <= 8G, and 32/G segments of one class (same kind,
@@ -208,20 +210,13 @@ constexpr uint32_t kLgRuntime = 8;
 // lanes storing runs of 2, 4 or 8 consecutive values hit distinct banks.
 __device__ __forceinline__ uint32_t sw(uint32_t i) { return i + (i >> 5); }
 
-// Exceptions of a staged block (ParaPFor.cpp:112-123): the G = 2^lg lanes of
-// a group patch the high bits of the listed positions into the group's
-// values, element i at vals[sw(base + i)]. Positions are distinct, so the
-// lanes never write the same word.
-__device__ __forceinline__ void group_patch(const uint32_t *lows, BlkHdr h, uint32_t count, uint32_t codec,
-                                            uint32_t *vals, uint32_t base, uint32_t lg, uint32_t sub) {
+// Exceptions of a staged ParaPFD block (ParaPFor.cpp:112-123): the G = 2^lg
+// lanes of a group patch the high bits of the listed positions into the
+// group's values, element i at vals[sw(base + i)]. Positions are distinct, so
+// the lanes never write the same word.
+__device__ __forceinline__ void group_patch(const uint32_t *lows, BlkHdr h, uint32_t count, uint32_t *vals,
+                                            uint32_t base, uint32_t lg, uint32_t sub) {
     const uint32_t *pb = lows + words_for(count, h.lb);
-    if (codec_is_newpfd(codec)) {
-        // NewPFD: exceptions from the Simple-16 stream, one lane of the group
-        if (sub == 0)
-            newpfd_patch_at(pb, h.en, h.lb, 0, count,
-                            [vals, base](uint32_t i) -> uint32_t & { return vals[sw(base + i)]; });
-        return;
-    }
     const uint32_t *hp = pb + words_for(h.en, h.eb);
     for (uint32_t x = sub; x < h.en; x += 1u << lg) {
         const uint32_t pbit = x * h.eb, hbit = x * h.hb;
@@ -263,7 +258,14 @@ __device__ __forceinline__ void group_dgap(const uint32_t *blk, const RunMeta &m
                 if (q < (int)vpl && el + q < count) vals[sw(base + el + q)] = v[q];
         }
         __syncwarp();
-        if (exc) group_patch(lows, h, count, m.codec, vals, base, lg, sub);
+        // NewPFD blocks: their groups decode the Simple-16 exception stream
+        // together (every lane of the warp takes part in the shuffles)
+        const bool npfd = exc && codec_is_newpfd(m.codec);
+        if (__any_sync(0xffffffffu, npfd))
+            newpfd_patch_group(lows + words_for(count, h.lb), npfd ? m.bw - 1u - words_for(count, h.lb) : 0u,
+                               npfd ? h.en : 0u, h.lb, 0u, count, lg, sub,
+                               [vals, base](uint32_t i) -> uint32_t & { return vals[sw(base + i)]; });
+        if (exc && !npfd) group_patch(lows, h, count, vals, base, lg, sub);
         __syncwarp();
         if (exc) {
 #pragma unroll
@@ -342,7 +344,7 @@ __device__ __forceinline__ void group_resid(const uint32_t *blk, const RunMeta &
                 if (sub + G * q < count) vals[sw(base + sub + G * q)] = v[q];
         }
         __syncwarp();
-        if (exc) group_patch(lows, h, count, m.codec, vals, base, lg, sub);
+        if (exc) group_patch(lows, h, count, vals, base, lg, sub);
         __syncwarp();
         if (exc) {
 #pragma unroll

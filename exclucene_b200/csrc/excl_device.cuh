@@ -247,27 +247,96 @@ __device__ __forceinline__ uint32_t s16_next(S16Cursor &c) {
     return v;
 }
 
-// Adds the high parts of a NewPFD block's exceptions at positions in
-// [e0, e0 + kc) to the buffer word at(pos - e0) (serial: one thread).
-template <class At>
-__device__ __forceinline__ void newpfd_patch_at(const uint32_t *s16, uint32_t en, uint32_t b, uint32_t e0, uint32_t kc,
-                                                At at) {
-    S16Cursor pc, hc;
-    s16_start(pc, s16);
-    s16_start(hc, s16);
-    for (uint32_t i = 0; i < en; ++i) s16_next(hc);
-    uint32_t p = 0;
-    for (uint32_t i = 0; i < en; ++i) {
-        const uint32_t d = s16_next(pc);
-        p = i ? p + d + 1u : d;
-        const uint32_t h = s16_next(hc);
-        if (p >= e0 && p < e0 + kc) at(p - e0) += h << b;
+// Values in a Simple-16 word, and value j of it (its runs of (count, width),
+// low bits first).
+__device__ __forceinline__ uint32_t s16_count(uint32_t word) {
+    const uint32_t k = word >> 28;
+    return (uint32_t)kS16Dev[k][0] + kS16Dev[k][2] + kS16Dev[k][4];
+}
+__device__ __forceinline__ uint32_t s16_value(uint32_t word, uint32_t j) {
+    const uint32_t k = word >> 28;
+    const uint32_t c0 = kS16Dev[k][0], w0 = kS16Dev[k][1], c1 = kS16Dev[k][2], w1 = kS16Dev[k][3],
+                   w2 = kS16Dev[k][5];
+    uint32_t off, wd;
+    if (j < c0) {
+        off = j * w0;
+        wd = w0;
+    } else if (j < c0 + c1) {
+        off = c0 * w0 + (j - c0) * w1;
+        wd = w1;
+    } else {
+        off = c0 * w0 + c1 * w1 + (j - c0 - c1) * w2;
+        wd = w2;
     }
+    return (word >> off) & ((1u << wd) - 1u);  // widths are <= 28
 }
 
-__device__ __forceinline__ void newpfd_patch(const uint32_t *s16, uint32_t en, uint32_t b, uint32_t e0, uint32_t kc,
-                                             uint32_t *buf) {
-    newpfd_patch_at(s16, en, b, e0, kc, [buf](uint32_t i) -> uint32_t & { return buf[i]; });
+// Group-parallel patch of a NewPFD block's exceptions: at(pos - e0) += high
+// << b for every exception at a position in [e0, e0 + kc). The block's
+// Simple-16 stream (NewPFor.cpp:91-106) holds the en position codes (the
+// first absolute, then gaps minus one) and then the en high parts; `nw` words
+// of it may be read. The warp works in groups of G = 2^lg lanes (sub = lane
+// within the group, one block per group); every lane of the warp calls this,
+// and a group with en = 0 only keeps step. Per round of G exceptions: the
+// group scans the value counts of G stream words at a time (each lane one
+// word's selector), so every word's first value index is known, and each lane
+// finds the words holding its exception's position code and high part with a
+// search over the group's word starts (shuffles); a group scan of the codes
+// then gives the positions. The reference decodes this stream with one thread
+// of a block (NewPFD_Decompression_kernel.cu:432-440).
+template <class At>
+__device__ __forceinline__ void newpfd_patch_group(const uint32_t *s16, uint32_t nw, uint32_t en, uint32_t b,
+                                                   uint32_t e0, uint32_t kc, uint32_t lg, uint32_t sub, At at) {
+    const uint32_t G = 1u << lg, full = 0xffffffffu;
+    const uint32_t nwv = min(nw, 2u * en);  // a stream of 2 en values has at most 2 en words
+    // trip counts the whole warp shares (shuffles need every lane)
+    const uint32_t xrounds = __reduce_max_sync(full, (en + G - 1u) >> lg);
+    const uint32_t wrounds = __reduce_max_sync(full, (nwv + G - 1u) >> lg);
+    uint32_t pcarry = 0;  // position of the previous round's last exception
+    for (uint32_t xr = 0; xr < xrounds; ++xr) {
+        const uint32_t x = (xr << lg) + sub;
+        const bool live = x < en;
+        uint32_t code = 0, high = 0, vstart = 0;
+        for (uint32_t wr = 0; wr < wrounds; ++wr) {
+            const uint32_t wi = (wr << lg) + sub;
+            const uint32_t word = wi < nwv ? s16[wi] : 0u;
+            const uint32_t cnt = wi < nwv ? s16_count(word) : 0u;
+            uint32_t inc = cnt;
+            for (uint32_t o = 1; o < G; o <<= 1) {
+                const uint32_t t = __shfl_up_sync(full, inc, o, G);
+                if (sub >= o) inc += t;
+            }
+            const uint32_t st = vstart + inc - cnt;  // value index of this lane's word
+            const uint32_t total = __shfl_sync(full, inc, G - 1u, G);
+#pragma unroll
+            for (int r = 0; r < 2; ++r) {
+                const uint32_t k = r ? en + x : x;
+                // the last lane of the group whose word starts at or before k
+                uint32_t lo = 0;
+                for (uint32_t hb = G >> 1; hb; hb >>= 1) {
+                    const uint32_t sv = __shfl_sync(full, st, lo + hb, G);
+                    if (sv <= k) lo += hb;
+                }
+                const uint32_t wv = __shfl_sync(full, word, lo, G), sv = __shfl_sync(full, st, lo, G);
+                if (live && k >= vstart && k < vstart + total) {
+                    const uint32_t v = s16_value(wv, k - sv);
+                    if (r) high = v;
+                    else code = v;
+                }
+            }
+            vstart += total;
+        }
+        // positions: p(0) = code(0), p(x) = p(x - 1) + code(x) + 1
+        const uint32_t d = live ? code + (x ? 1u : 0u) : 0u;
+        uint32_t inc = d;
+        for (uint32_t o = 1; o < G; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(full, inc, o, G);
+            if (sub >= o) inc += t;
+        }
+        const uint32_t p = pcarry + inc;
+        if (live && p >= e0 && p < e0 + kc) at(p - e0) += high << b;
+        pcarry = __shfl_sync(full, p, G - 1u, G);
+    }
 }
 
 // Warp-cooperative decode of elements [e0, e0 + kc) (kc <= 256) of one
@@ -308,7 +377,11 @@ __device__ __forceinline__ void warp_decode(const DevIndexView &ix, const ListDe
         __syncwarp();
         const uint32_t *pb = blk + 1 + words_for(rec.count, h.lb);
         if (newpfd) {
-            if (lane == 0) newpfd_patch(pb, h.en, h.lb, e0, kc, buf);
+            // the stream ends with the block: its words from the block's extent
+            const uint32_t bw = (uint32_t)(__ldg(ix.seg_gword + sg + 1) - __ldg(ix.seg_gword + sg));
+            const uint32_t nw = bw - 1u - words_for(rec.count, h.lb);
+            newpfd_patch_group(pb, nw, h.en, h.lb, e0, kc, 5u, lane,
+                               [buf](uint32_t i) -> uint32_t & { return buf[i]; });
         } else {
             const uint32_t *hp = pb + words_for(h.en, h.eb);
             for (uint32_t x = lane; x < h.en; x += 32) {

@@ -114,8 +114,8 @@ int excl_index_build(const uint32_t *docs, const uint64_t *list_offsets, uint32_
                      const excl_build_params *params, excl_index **out);
 int excl_index_free(excl_index *ix);
 
-/* The same build on the GPU, for the ParaPFD, LRC, LRCSeg, SegLRC, HS_SegLRC
- * and HS_ParaPFD formats (one codec for all lists, `codecs` = NULL): the hash
+/* The same build on the GPU, for the ParaPFD, NewPFD, LRC, LRCSeg, SegLRC,
+ * HS_SegLRC and HS_ParaPFD formats (one codec for all lists, `codecs` = NULL): the hash
  * partition, regression fits, residuals and minima, d-gaps and medians, and
  * the ParaPFD blocks are computed by kernels on the context's device
  * (HS_SegLRC_Generator.cu:503-594, SegLRC_Generator.cu:94-436,
@@ -125,7 +125,9 @@ int excl_index_free(excl_index *ix);
  * threads, overlapped. d_docs is the CSR docID array in device memory; list l
  * is d_docs[list_offsets[l] .. list_offsets[l+1]) (list_offsets on the host,
  * nlists + 1 entries). The result is byte-identical to excl_index_build's and
- * still has to be uploaded. NewPFD: host build only (EXCL_E_INVALID here).
+ * still has to be uploaded. NewPFD blocks are built too: their Simple-16
+ * exception streams are packed by one warp per block, the 16 layouts tested
+ * in parallel per word (NewPFor.cpp's sequential greedy choice, same bytes).
  * Scratch: about 12 bytes per posting plus 100 bytes per segment, freed on return. */
 struct excl_ctx;
 int excl_index_build_device(struct excl_ctx *ctx, const uint32_t *d_docs, const uint64_t *list_offsets,

@@ -1,5 +1,5 @@
-"""Index build on the GPU: for the ParaPFD, LRC, LRCSeg, SegLRC, HS_SegLRC and
-HS_ParaPFD formats the device build gives the host build's arrays bit for bit
+"""Index build on the GPU: for the ParaPFD, NewPFD, LRC, LRCSeg, SegLRC,
+HS_SegLRC and HS_ParaPFD formats the device build gives the host build's arrays bit for bit
 (hash partition, fits, residual bases, medians, blocks, directories, tile
 maps), rejects unordered lists, and the index it builds answers queries as the
 oracle does."""
@@ -45,7 +45,8 @@ CASES = [("parapfd", 256, 0.0, {}), ("parapfd", 128, 0.12, {}), ("parapfd", 256,
          ("seglrc", 256, 0.0, {}), ("seglrc", 128, 0.1, {}), ("lrc", 256, 0.0, {}), ("lrc", 128, 0.1, {}),
          ("lrcseg", 256, 0.0, {}), ("lrcseg", 128, 0.1, {}),
          ("hs_seglrc", 256, 0.0, HS_BUCKET), ("hs_seglrc", 256, 0.1, HS_BUCKET), ("hs_seglrc", 256, 0.0, HS_TOP),
-         ("hs_parapfd", 128, 0.1, HS_BUCKET), ("hs_parapfd", 256, 0.0, HS_TOP)]
+         ("hs_parapfd", 128, 0.1, HS_BUCKET), ("hs_parapfd", 256, 0.0, HS_TOP),
+         ("newpfd", 128, 0.1, {}), ("newpfd", 256, 0.64, {}), ("newpfd", 32, 0.3, {})]
 
 
 @pytest.mark.parametrize("codec,block,frac,hs", CASES)
@@ -69,7 +70,8 @@ def test_device_build_equals_host_build(gpu_ctx, corpus, codec, block, frac, hs)
         want.close()
 
 
-@pytest.mark.parametrize("codec,hs", [("lrc", {}), ("lrcseg", {}), ("hs_seglrc", HS_BUCKET)])
+@pytest.mark.parametrize("codec,hs", [("lrc", {}), ("lrcseg", {}), ("hs_seglrc", HS_BUCKET),
+                                      ("newpfd", dict(block=128, frac=0.3))])
 def test_device_built_index_answers_queries(gpu_ctx, corpus, codec, hs):
     import torch
 
@@ -113,12 +115,10 @@ def test_device_build_rejects_unordered_lists(gpu_ctx):
     docs = np.array([5, 9, 9, 12, 1, 2, 3], np.uint32)  # list 0 repeats 9
     d = torch.from_numpy(docs.view(np.int32)).cuda()
     torch.cuda.synchronize()
-    for codec in ("parapfd", "seglrc", "lrc", "lrcseg", "hs_seglrc", "hs_parapfd"):
+    for codec in ("parapfd", "seglrc", "lrc", "lrcseg", "hs_seglrc", "hs_parapfd", "newpfd"):
         with pytest.raises(ex.ExclError) as e:
             gpu_ctx.build_index(d.data_ptr(), np.array([0, 4, 7], np.uint64), codec=codec)
         assert e.value.status == ex.api.E_INVALID
-    with pytest.raises(ex.ExclError):
-        gpu_ctx.build_index(d.data_ptr(), np.array([0, 4, 7], np.uint64), codec="newpfd")  # host build only
 
 
 def test_layout_autotuner_keeps_the_fastest_exact_layout(gpu_ctx):
@@ -143,9 +143,11 @@ def test_layout_autotuner_keeps_the_fastest_exact_layout(gpu_ctx):
     _same_index(ix, host)
     ix.close()
     host.close()
-    # NewPFD has no device build: recorded as skipped, the others still run
+    # a layout that cannot be built (blocks of 512 are beyond the tile size) is
+    # recorded as skipped, the others still run
     ix, best, rep = gpu_ctx.autotune_layout(d_docs.data_ptr(), w.list_offsets,
-                                            [dict(codec="newpfd", block=128), dict(codec="seglrc", block=256)],
+                                            [dict(codec="parapfd", block=512), dict(codec="newpfd", block=128,
+                                                                                    frac=0.1)],
                                             w.terms, w.term_offsets)
     assert rep[0]["status"] != 0 and rep[1]["status"] == 0 and best == 1
     ix.close()

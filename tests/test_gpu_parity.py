@@ -286,3 +286,17 @@ def test_reference_file_set_runs_unchanged(gpu_ctx, tmp_path, codec):
         assert np.array_equal(offs.astype(np.uint64), eoffs)
         assert np.array_equal(got, edocs)
     ix.close()
+
+
+@pytest.mark.parametrize("block,frac", [(32, 0.64), (128, 0.64), (256, 0.64), (128, 0.3)])
+def test_newpfd_many_exceptions_decode_and_intersect(gpu_ctx, corpus, expected, block, frac):
+    """NewPFD blocks with up to 64% exceptions: the group-parallel Simple-16
+    exception decode (many rounds of exceptions and of stream words per block)
+    in the whole-list decode and in the probe kernel's tile decode."""
+    ix = _index(corpus, "newpfd", block, frac)
+    gpu_ctx.upload(ix)
+    assert np.array_equal(gpu_ctx.decode_lists(ix), corpus.docs)
+    offs, docs = gpu_ctx.intersect(ix, corpus.terms, corpus.term_offsets, algo="hashseg")
+    eoffs, edocs = expected
+    assert np.array_equal(offs.astype(np.uint64), eoffs) and np.array_equal(docs, edocs)
+    ix.close()
