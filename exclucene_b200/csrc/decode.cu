@@ -297,6 +297,67 @@ __device__ __forceinline__ void group_dgap(const uint32_t *blk, const RunMeta &m
     __syncwarp();
 }
 
+// d-gap codecs, full blocks of 8G values with G = 16 or 32 (ParaPFD blocks of
+// 128 or 256): the same steps as group_dgap with every bound known, so no
+// value needs a bounds test, the G-wide scan is unrolled, and each lane's
+// eight consecutive docIDs leave its registers as two 16-byte stores (the
+// caller checks that the group's output is 16-byte aligned). Every group of
+// the warp holds such a block.
+template <uint32_t LG>
+__device__ __forceinline__ void group_dgap_full(const uint32_t *blk, const RunMeta &m, uint32_t sub, uint32_t *vals,
+                                                uint32_t base, uint32_t *__restrict__ out) {
+    constexpr uint32_t G = 1u << LG, count = 8u * G;
+    const BlkHdr h = blk_hdr(blk[0]);
+    const uint32_t *lows = blk + 1;
+    const uint32_t mask = (1u << h.lb) - 1u;
+    const uint32_t el = sub * 8u;
+    uint32_t v[8];
+    uint32_t bit = el * h.lb;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const uint32_t wi = bit >> 5;
+        v[q] = __funnelshift_r(lows[wi], lows[wi + 1], bit & 31u) & mask;
+        bit += h.lb;
+    }
+    const bool exc = h.en != 0;
+    if (__any_sync(0xffffffffu, exc)) {
+        if (exc) {
+#pragma unroll
+            for (int q = 0; q < 8; ++q) vals[sw(base + el + q)] = v[q];
+        }
+        __syncwarp();
+        const bool npfd = exc && codec_is_newpfd(m.codec);
+        if (__any_sync(0xffffffffu, npfd))
+            newpfd_patch_group(lows + words_for(count, h.lb), npfd ? m.bw - 1u - words_for(count, h.lb) : 0u,
+                               npfd ? h.en : 0u, h.lb, 0u, count, LG, sub,
+                               [vals, base](uint32_t i) -> uint32_t & { return vals[sw(base + i)]; });
+        if (exc && !npfd) group_patch(lows, h, count, vals, base, LG, sub);
+        __syncwarp();
+        if (exc) {
+#pragma unroll
+            for (int q = 0; q < 8; ++q) v[q] = vals[sw(base + el + q)];
+        }
+        __syncwarp();
+    }
+    if (sub == 0) v[0] = m.head;
+    uint32_t run = 0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        run += v[q];
+        v[q] = run;
+    }
+    uint32_t incl = run;
+#pragma unroll
+    for (uint32_t o = 1; o < G; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o, G);
+        if (sub >= o) incl += t;
+    }
+    const uint32_t ex = incl - run;
+    uint4 *o = reinterpret_cast<uint4 *>(out + m.ob + el);
+    o[0] = make_uint4(v[0] + ex, v[1] + ex, v[2] + ex, v[3] + ex);
+    o[1] = make_uint4(v[4] + ex, v[5] + ex, v[6] + ex, v[7] + ex);
+}
+
 // Residual codecs (LRC, LRCSeg, SegLRC, HS_SegLRC), one segment per group of
 // G lanes: no scan; lane `sub` owns values sub, sub+G, ... so the group reads
 // neighbouring words and every value goes from its register straight into a
@@ -492,8 +553,17 @@ __global__ void __launch_bounds__(kDecWarps * 32, kDecCtasPerSm) k_decode_tma(De
         default: EXCL_DEC_CALL(F, 5); break;                \
     }
                     if (c < 6u) {
-                        if (EXCL_DEC_DGAP_FIXED) { EXCL_DEC_SWITCH(group_dgap) }
-                        else EXCL_DEC_CALL(group_dgap, kLgRuntime);
+                        // full blocks of 128 or 256 values in every group, output 16-byte aligned
+                        const bool full = act && (lg == 4u || lg == 5u) && m.count == (8u << lg) &&
+                                          ((reinterpret_cast<uintptr_t>(out + m.ob) & 15u) == 0);
+                        if (__all_sync(0xffffffffu, full)) {
+                            if (lg == 4u) group_dgap_full<4>(blk, m, sub, vals, base, out);
+                            else group_dgap_full<5>(blk, m, sub, vals, base, out);
+                        } else if (EXCL_DEC_DGAP_FIXED) {
+                            EXCL_DEC_SWITCH(group_dgap)
+                        } else {
+                            EXCL_DEC_CALL(group_dgap, kLgRuntime);
+                        }
                     } else {
                         if (EXCL_DEC_RESID_FIXED) { EXCL_DEC_SWITCH(group_resid) }
                         else EXCL_DEC_CALL(group_resid, kLgRuntime);
