@@ -303,18 +303,21 @@ def reference_arm(args, w, desc, params):
                                codecs if codecs is not None else oracle.CODECS[params["codec"]],
                                block=params["block"], frac=params["frac"], bucket=params.get("hs_bucket", 256),
                                kbits=params.get("hs_kbits", 0), ubits=params.get("hs_ubits", 32))
-    vals = []
+    vals, secs = [], []
     n = p = reps = 0
     for i in range(args.warmup + args.steps):
         t, n, p, reps = cpu_run(w, img, max(1.0, args.cpu_sample_s / max(args.steps, 1)), threads)
         if i >= args.warmup:
             vals.append(p / t)
+            secs.append(t)
     v = float(np.median(vals))
     sample = (f"per step {reps} x the first {n} of {w.nq} queries; ParaPFD/regression decode + exact AND on "
               f"the compressed index built by the oracle's encoders (oracle port of the reference CPU path), "
               f"{threads} threads")
     line = {"metric": "postings/s", "value": v, "unit": "postings/s", "impl": "reference", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "steps": args.steps, "warmup": args.warmup,
+            # one step = one bounded CPU sample of the workload (see cpu_baseline.sample)
+            "ms_per_step": float(np.mean(secs)) * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u32", "data": "synthetic",
             "config": bench_config(w, params, desc),
             "cpu_baseline": {"value": v, "unit": "postings/s", "cores": threads, "kind": "port", "sample": sample},
