@@ -7,16 +7,17 @@
 //            tiles, docIDs and heavy tiles; a block scan plus a decoupled
 //            look-back over the chunks give the batch's prefixes; each tile's
 //            16-byte work record goes to its place in the probe order (heavy
-//            tiles from the front, the others from the back). The chunk that
-//            finishes last publishes the batch's "packed" tag.
+//            tiles from the front, the others from the back). Each chunk
+//            publishes a done flag; the probe phase waits for all of them.
 //   probe    kernels.cu: warps take work records from a counter.
-//   scatter  once every taken tile is probed (a count the probe warps add to
-//            once each as they leave the probe loop), CTAs take chunks of 512
-//            tiles: survivor totals, a decoupled look-back for their base,
-//            each tile's output position (replaces cudppScan and ucntResult,
-//            ParaPFD_Intersection.cu:262,301); then every warp copies
-//            survivors to the result array (replaces saCompact, :279) and
-//            every thread writes query offsets.
+//   scatter  once every tile is probed (a count the probe warps add to once
+//            each as they leave the probe loop, which every CTA acquires
+//            before it reads any tile's results), CTAs take chunks of 512
+//            tiles; each chunk owner scans its survivor counts, finds its base
+//            by a decoupled look-back (replaces cudppScan,
+//            ParaPFD_Intersection.cu:262), writes the offsets of the queries
+//            that start in the chunk (ucntResult, :301) and copies its
+//            survivors to the result array (saCompact, :279).
 //
 // Every wait is on work that a running CTA already holds (a ticket it took,
 // tiles it took), so the grid needs no co-residency and batches on other
@@ -87,7 +88,9 @@ struct PackShared {
     uint32_t sc[3][33], pre[3], et[kPackThreads], eh[kPackThreads], h[kPackThreads], l0[kPackThreads];
 };
 struct ScatterShared {
-    uint32_t sa[33], sb[33];
+    uint32_t sa[33];
+    uint32_t ex[kSSChunk];    // exclusive survivor prefix of the chunk's tiles
+    uint32_t slot[kSSChunk];  // their survivor slots
     uint32_t c, base;
 };
 
@@ -174,9 +177,10 @@ __device__ __forceinline__ uint32_t heavy_tiles(uint32_t n, uint32_t nt, uint32_
 }
 
 // Pack chunk `bid` of `npack` (queries bid*256 .. +255) with the CTA's 256
-// threads. The chunk that completes last finishes the phase: batch totals are
-// out (the last chunk wrote them), the probe counter and statistics are
-// cleared, and sync->packed = tag releases the probe phase.
+// threads. Its flag goes to tag << 1 once its aggregates are out (for the
+// look-back of later chunks) and to tag << 1 | 1 once all its writes are
+// visible; the last chunk also writes the batch totals, chunk 0 clears the
+// probe phase's counters and the statistics.
 __device__ __noinline__ void pack_chunk(uint32_t bid, uint32_t npack, uint32_t tag, const ListDesc *__restrict__ lists,
                                            uint32_t nlists, const uint32_t *terms, const uint32_t *toff, uint32_t nq,
                                            const BatchView &b, PackSync *__restrict__ sync, PackShared &sm,
@@ -276,7 +280,7 @@ __device__ __noinline__ void pack_chunk(uint32_t bid, uint32_t npack, uint32_t t
         sync->agg_t[bid] = bt;
         sync->agg_k[bid] = bk;
         sync->agg_h[bid] = tot[2];
-        st_release(&sync->flag[bid], tag);
+        st_release(&sync->flag[bid], tag << 1);  // aggregates out
     }
     if (threadIdx.x < 32) {
         // warp 0: the predecessors' totals. Every predecessor took its ticket
@@ -290,13 +294,13 @@ __device__ __noinline__ void pack_chunk(uint32_t bid, uint32_t npack, uint32_t t
 #pragma unroll
             for (uint32_t j = 0; j < 4; ++j) {
                 const uint32_t p = p0 + lane + 32u * j;
-                f[j] = p < bid ? ld_relaxed(&sync->flag[p]) : tag;
+                f[j] = p < bid ? ld_relaxed(&sync->flag[p]) : tag << 1;
             }
 #pragma unroll
             for (uint32_t j = 0; j < 4; ++j) {
                 const uint32_t p = p0 + lane + 32u * j;
                 uint32_t spins = 0;
-                while (f[j] != tag) {
+                while ((f[j] >> 1) != tag) {  // aggregates out (or the chunk already done)
                     if (++spins > spin) {
                         atomicOr(b.err, kErrScanSpin);
                         break;
@@ -368,21 +372,40 @@ __device__ __noinline__ void pack_chunk(uint32_t bid, uint32_t npack, uint32_t t
         if (i < sm.h[lo]) b.tile_order[hb + i] = wr;
         else b.tile_order[b.max_tiles - 1u - (t - hb - sm.h[lo])] = wr;
     }
-    // this chunk is done once every thread's writes are visible; the chunk
-    // that completes last releases the probe phase
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0 && atomicAdd(&sync->done, 1u) == npack - 1) {
-        __threadfence();  // the other chunks' writes (ordered by their fence before counting) and the totals
+    // chunk 0 also clears the probe phase's counters and the statistics (no
+    // probe starts before every chunk is done, chunk 0 included)
+    if (bid == 0 && threadIdx.x == 0) {
         *b.tile_counter = 0u;
         *b.probe_done = 0u;
         if (b.stats) {
             b.stats[0] = b.stats[1] = b.stats[2] = b.stats[3] = b.stats[6] = 0ull;
-            b.stats[5] = global_ns();
+            b.stats[5] = ~0ull;
         }
-        st_release(&sync->packed, tag);
     }
+    // this chunk is done once every thread's writes are visible: its flag
+    // moves to tag << 1 | 1, which the probe phase waits for on every chunk
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) st_release(&sync->flag[bid], (tag << 1) | 1u);
     __syncthreads();  // sm is reused by the next chunk
+}
+
+// Bounded wait, by one warp, until every pack chunk of the batch is done
+// (flag == tag << 1 | 1); then the CTA may read the batch's records.
+__device__ __forceinline__ void wait_packed(const PackSync *sync, uint32_t npack, uint32_t tag, uint32_t *err,
+                                            uint32_t spin, uint32_t lane) {
+    const uint32_t want = (tag << 1) | 1u;
+    for (uint32_t p = lane; p < npack; p += 32) {
+        uint32_t spins = 0;
+        while (ld_acquire(&sync->flag[p]) != want) {
+            if (++spins > spin) {
+                atomicOr(err, kErrScanSpin);
+                break;
+            }
+            __nanosleep(32);
+        }
+    }
+    __syncwarp();
 }
 
 // The batch's error bits to the host word the batch names (the device word is
@@ -394,52 +417,64 @@ __device__ __forceinline__ void hand_over_flags(const BatchView &b) {
 }
 
 // Scatter phase, run by every CTA once its warps have left the probe loop.
-// Phase A (CTAs holding a chunk ticket): survivor total of the chunk,
-// decoupled look-back for its base, the absolute output position of each of
-// its tiles (into tile_q), then the chunk's inclusive prefix. Phase B (every
-// warp, once all chunk tickets are taken, so every chunk is owned by a running
-// CTA): query offsets, and survivors copied tile by tile, each tile after its
-// chunk's prefix is out.
+// Every CTA first acquires the count of probed tiles (all tiles done: their
+// counts, slots and first-tile marks, written by other CTAs, are read below).
+// Then CTAs take chunks of 512 tiles by ticket, and each chunk owner does all
+// of its chunk's work: the survivor counts' block scan, a decoupled look-back
+// over the chunks for its base (replaces cudppScan, ParaPFD_Intersection.cu:262),
+// the offsets of the queries whose first tile is in the chunk (replaces
+// ucntResult, :301) and the copy of the chunk's survivors to the result array
+// (replaces saCompact, :279), one survivor per thread, so the stores coalesce.
 __device__ __noinline__ void scatter_phase(const BatchView &b, PackSync *__restrict__ sync,
-                                              uint64_t *__restrict__ chunk_state, uint32_t *__restrict__ offsets,
-                                              uint32_t *__restrict__ docids, uint64_t cap, uint32_t tag,
-                                              ScatterShared &sm, uint32_t spin) {
+                                           uint64_t *__restrict__ chunk_state, uint32_t *__restrict__ offsets,
+                                           uint32_t *__restrict__ docids, uint64_t cap, uint32_t tag,
+                                           ScatterShared &sm, uint32_t spin) {
     constexpr uint32_t kPer = kSSChunk / kSSThreads;
     static_assert(kPer == 2, "two tiles per thread");
     const uint32_t nq = b.nq;
     const uint32_t T = min(b.tile_prefix[nq], b.max_tiles);
     const uint32_t nch = (T + kSSChunk - 1) / kSSChunk;
     const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
-    uint32_t *tile_out = b.tile_q;
     if (nch == 0) {  // no tiles in the batch: every offset is 0
         for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q <= nq; q += gridDim.x * blockDim.x) offsets[q] = 0u;
         return;
     }
-    for (;;) {
-        if (threadIdx.x == 0) {
-            sm.c = atomicAdd(&sync->sticket, 1u);
-            // the chunk owners start once every tile of the batch is probed
-            if (sm.c < nch) {
-                uint32_t spins = 0;
-                while (ld_acquire(b.probe_done) != T) {
-                    if (++spins > spin) {
-                        atomicOr(b.err, kErrScanSpin);
-                        break;
-                    }
-                    __nanosleep(64);
-                }
+    if (threadIdx.x == 0) {
+        uint32_t spins = 0;
+        while (ld_acquire(b.probe_done) != T) {
+            if (++spins > spin) {
+                atomicOr(b.err, kErrScanSpin);
+                break;
             }
+            __nanosleep(64);
         }
+    }
+    __syncthreads();
+    for (;;) {
+        if (threadIdx.x == 0) sm.c = atomicAdd(&sync->sticket, 1u);
         __syncthreads();
         const uint32_t c = sm.c;
         if (c >= nch) break;
+        // the chunk's tiles: counts, survivor slots, first-tile marks (query + 1
+        // for a query's first tile, else 0), all loads in flight at once
         const uint32_t t0 = c * kSSChunk;
-        const uint32_t ta = t0 + threadIdx.x * kPer;
+        const uint32_t ja = threadIdx.x * kPer, ta = t0 + ja;
         const uint32_t c0 = ta < T ? b.tile_count[ta] : 0u;
         const uint32_t c1 = ta + 1 < T ? b.tile_count[ta + 1] : 0u;
+        const uint32_t s0 = ta < T ? b.tile_slot[ta] : 0u;
+        const uint32_t s1 = ta + 1 < T ? b.tile_slot[ta + 1] : 0u;
+        const uint32_t f0 = ta < T ? b.tile_q[ta] : 0u;
+        const uint32_t f1 = ta + 1 < T ? b.tile_q[ta + 1] : 0u;
+        // a query before a first tile that has no tiles itself shares its offset
+        const uint32_t pe0 = f0 > 1u ? b.tile_prefix[f0 - 2u] : 0xffffffffu;
+        const uint32_t pe1 = f1 > 1u ? b.tile_prefix[f1 - 2u] : 0xffffffffu;
         uint32_t tot;
         const uint32_t ex = block_scan1(c0 + c1, tot, sm.sa);
         if (threadIdx.x == 0) st_release64(&chunk_state[c], chunk_word(tag, kAggregate, tot));
+        sm.ex[ja] = ex;
+        sm.ex[ja + 1] = ex + c0;
+        sm.slot[ja] = s0;
+        sm.slot[ja + 1] = s1;
         if (w == 0) {
             // look-back: sum the aggregates of the preceding chunks up to the
             // nearest one that has published its inclusive prefix
@@ -449,19 +484,19 @@ __device__ __noinline__ void scatter_phase(const BatchView &b, PackSync *__restr
                 const int64_t idx = p - (int64_t)lane;
                 uint32_t st = kPrefix, v = 0;
                 if (idx >= 0) {
-                    uint64_t s = ld_acquire64(&chunk_state[idx]);
+                    uint64_t sv = ld_acquire64(&chunk_state[idx]);
                     uint32_t spins = 0;
-                    while ((uint32_t)(s >> 34) != tag) {
+                    while ((uint32_t)(sv >> 34) != tag) {
                         if (++spins > spin) {
                             atomicOr(b.err, kErrScanSpin);
-                            s = chunk_word(tag, kPrefix, 0u);
+                            sv = chunk_word(tag, kPrefix, 0u);
                             break;
                         }
                         __nanosleep(32);
-                        s = ld_acquire64(&chunk_state[idx]);
+                        sv = ld_acquire64(&chunk_state[idx]);
                     }
-                    st = (uint32_t)(s >> 32) & 3u;
-                    v = (uint32_t)s;
+                    st = (uint32_t)(sv >> 32) & 3u;
+                    v = (uint32_t)sv;
                 }
                 const uint32_t m = __ballot_sync(0xffffffffu, st == kPrefix);
                 const uint32_t stop = m ? (uint32_t)(__ffs(m) - 1) : 31u;
@@ -472,84 +507,43 @@ __device__ __noinline__ void scatter_phase(const BatchView &b, PackSync *__restr
                 if (m) break;
                 p -= 32;
             }
-            if (lane == 0) sm.base = excl;
+            if (lane == 0) {
+                sm.base = excl;
+                st_release64(&chunk_state[c], chunk_word(tag, kPrefix, excl + tot));
+            }
         }
         __syncthreads();
         const uint32_t base = sm.base;
-        if (ta < T) tile_out[ta] = base + ex;
-        if (ta + 1 < T) tile_out[ta + 1] = base + ex + c0;
         if (c == nch - 1 && threadIdx.x == 0 && (uint64_t)base + tot > cap) atomicOr(b.err, kErrCapacity);
-        __syncthreads();  // tile positions written before the prefix goes out
-        if (threadIdx.x == 0) {
-            __threadfence();
-            st_release64(&chunk_state[c], chunk_word(tag, kPrefix, base + tot));
+        // offsets of the queries that start here (and of empty queries before them)
+        if (f0) {
+            offsets[f0 - 1u] = base + ex;
+            if (pe0 == ta)
+                for (uint32_t q = f0 - 1u; q > 0 && b.tile_prefix[q - 1u] == ta; --q) offsets[q - 1u] = base + ex;
         }
-    }
-    // the query offsets: the output position of each query's first tile, or
-    // for a query with no tile after it, the batch's total (the last chunk's
-    // inclusive prefix); each once its chunk's prefix is out
-    for (uint32_t qq = blockIdx.x * blockDim.x + threadIdx.x; qq <= nq; qq += gridDim.x * blockDim.x) {
-        const uint32_t tp = min(b.tile_prefix[qq], T);
-        const uint32_t c = tp < T ? tp / kSSChunk : nch - 1u;
-        uint64_t s = ld_acquire64(&chunk_state[c]);
-        uint32_t spins = 0;
-        while ((uint32_t)(s >> 34) != tag || ((uint32_t)(s >> 32) & 3u) != kPrefix) {
-            if (++spins > spin) {
-                atomicOr(b.err, kErrScanSpin);
-                break;
-            }
-            __nanosleep(64);
-            s = ld_acquire64(&chunk_state[c]);
+        if (f1) {
+            offsets[f1 - 1u] = base + ex + c0;
+            if (pe1 == ta + 1)
+                for (uint32_t q = f1 - 1u; q > 0 && b.tile_prefix[q - 1u] == ta + 1; --q) offsets[q - 1u] = base + ex + c0;
         }
-        offsets[qq] = tp < T ? ld_acquire(&tile_out[tp]) : (uint32_t)s;
-    }
-    // survivors: warp w takes tiles w, w + nw, w + 2nw, ... (neighbouring
-    // tiles go to different warps, so a query with many survivors spreads over
-    // the grid). Lane j handles the warp's j-th tile of a round of 32: its
-    // survivor count, its chunk's prefix (bounded wait), its output position
-    // and slot, all lanes at once; then the warp copies the non-empty tiles
-    // one after another, eight independent loads per lane.
-    const uint32_t gw = blockIdx.x * (blockDim.x / 32) + w, nw = gridDim.x * (blockDim.x / 32);
-    const uint32_t *__restrict__ scr = b.scratch;
-    for (uint64_t j0 = 0; gw + j0 * nw < T; j0 += 32) {
-        const uint64_t tt = gw + (j0 + lane) * nw;
-        const uint32_t t = tt < T ? (uint32_t)tt : T;
-        const uint32_t n = t < T ? b.tile_count[t] : 0u;
-        uint32_t o = 0, slot = 0;
-        if (n) {
-            const uint32_t c = t / kSSChunk;
-            uint64_t s = ld_acquire64(&chunk_state[c]);
-            uint32_t spins = 0;
-            while ((uint32_t)(s >> 34) != tag || ((uint32_t)(s >> 32) & 3u) != kPrefix) {
-                if (++spins > spin) {
-                    atomicOr(b.err, kErrScanSpin);
-                    break;
-                }
-                __nanosleep(64);
-                s = ld_acquire64(&chunk_state[c]);
-            }
-            o = ld_acquire(&tile_out[t]);
-            slot = b.tile_slot[t];
+        if (c == nch - 1 && threadIdx.x == 0) {
+            // the batch total, and the queries after the last tile (no tiles)
+            offsets[nq] = base + tot;
+            for (uint32_t q = nq; q > 0 && b.tile_prefix[q - 1u] >= T; --q) offsets[q - 1u] = base + tot;
         }
-        uint32_t m = __ballot_sync(0xffffffffu, n != 0u);
-        while (m) {
-            const uint32_t l = (uint32_t)(__ffs(m) - 1);
-            m &= m - 1u;
-            const uint32_t nl = __shfl_sync(0xffffffffu, n, l), ol = __shfl_sync(0xffffffffu, o, l),
-                           sl = __shfl_sync(0xffffffffu, slot, l);
-            const uint32_t *src = scr + sl;
-            uint32_t v[kTileKeys / 32];
-#pragma unroll
-            for (uint32_t i = 0; i < kTileKeys / 32; ++i) {
-                const uint32_t k = lane + 32u * i;
-                if (k < nl) v[i] = src[k];
+        // the chunk's survivors, flattened: element e belongs to the last tile
+        // whose chunk prefix is <= e
+        for (uint32_t e = threadIdx.x; e < tot; e += blockDim.x) {
+            uint32_t lo = 0, hi = kSSChunk - 1;
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi + 1) >> 1;
+                if (sm.ex[mid] <= e) lo = mid;
+                else hi = mid - 1;
             }
-#pragma unroll
-            for (uint32_t i = 0; i < kTileKeys / 32; ++i) {
-                const uint32_t k = lane + 32u * i;
-                if (k < nl && (uint64_t)ol + k < cap) docids[(uint64_t)ol + k] = v[i];
-            }
+            const uint64_t o = (uint64_t)base + e;
+            if (o < cap) docids[o] = b.scratch[sm.slot[lo] + (e - sm.ex[lo])];
         }
+        __syncthreads();  // sm is reused by the next chunk
     }
 }
 

@@ -182,7 +182,12 @@ __global__ void __launch_bounds__(kBatchWarps * 32, MINB) k_batch(DevIndexView i
     const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
     // every CTA reads the same epoch: it changes only when the last CTA of
     // this grid leaves, and that CTA has counted every other one out
-    if (threadIdx.x == 0) s_tag = next_tag(*(volatile uint32_t *)&sync->epoch);
+    // the epoch read and the first pack ticket are in flight together
+    if (threadIdx.x == 0) {
+        const uint32_t e = *(volatile uint32_t *)&sync->epoch;
+        s_ticket = atomicAdd(&sync->ticket, 1u);
+        s_tag = next_tag(e);
+    }
     __syncthreads();
     const uint32_t tag = s_tag;
     // failure-path self-test: a bounded wait on a flag that nothing sets gives
@@ -191,8 +196,8 @@ __global__ void __launch_bounds__(kBatchWarps * 32, MINB) k_batch(DevIndexView i
 
     // ---- pack: chunks of 256 queries by ticket
     const uint32_t npack = max(1u, (b.nq + kPackThreads - 1) / kPackThreads);
-    for (;;) {
-        if (threadIdx.x == 0) s_ticket = atomicAdd(&sync->ticket, 1u);
+    for (bool first = true;; first = false) {
+        if (!first && threadIdx.x == 0) s_ticket = atomicAdd(&sync->ticket, 1u);
         __syncthreads();
         const uint32_t bid = s_ticket;
         __syncthreads();
@@ -200,7 +205,10 @@ __global__ void __launch_bounds__(kBatchWarps * 32, MINB) k_batch(DevIndexView i
         if (bid == 0 && threadIdx.x == 0 && b.stats) b.stats[4] = global_ns();
         pack_chunk(bid, npack, tag, lists, nlists, terms, toff, b.nq, b, sync, sm.pack, spin);
     }
-    if (threadIdx.x == 0) wait_tag(&sync->packed, tag, b.err, spin);
+    if (w == 0) {
+        wait_packed(sync, npack, tag, b.err, spin, lane);
+        if (lane == 0 && b.stats) atomicMin((unsigned long long *)&b.stats[5], (unsigned long long)global_ns());
+    }
     __syncthreads();
 
     // ---- probe. Work order: one record {tile, query, tile within the query,
@@ -344,6 +352,7 @@ __global__ void __launch_bounds__(kBatchWarps * 32, MINB) k_batch(DevIndexView i
             if (lane == 0) {
                 b.tile_count[t] = alive;
                 b.tile_slot[t] = (uint32_t)slot;
+                b.tile_q[t] = ti == 0 ? q + 1u : 0u;  // first-tile mark for the scatter phase's offsets
             }
             ++done;
             __syncwarp();
@@ -384,7 +393,6 @@ __global__ void __launch_bounds__(kBatchWarps * 32, MINB) k_batch(DevIndexView i
     if (threadIdx.x == 0 && atomicAdd(&sync->sdone, 1u) == gridDim.x - 1) {
         __threadfence();
         sync->ticket = 0u;
-        sync->done = 0u;
         sync->sticket = 0u;
         sync->sdone = 0u;
         if (b.stats) b.stats[7] = global_ns();

@@ -14,7 +14,7 @@ struct BatchView {
     const uint32_t *qterms;      // nq * kMaxTerms list ids, ascending length
     const uint32_t *qnterms;     // terms per query
     const uint32_t *tile_prefix; // nq + 1, exclusive prefix of tiles per query
-    uint32_t *tile_q;            // max_tiles, scratch of the scatter phase (each tile's output position)
+    uint32_t *tile_q;            // max_tiles: query + 1 where the tile is its query's first tile, else 0
     uint4 *tile_order;           // max_tiles work records {tile, query, tile within the query, shortest list}:
                                  // heavy tiles from the front, the rest from the back (tile_prefix[nq + 1] = heavy tiles)
     uint32_t *tile_counter;      // work-queue head (zeroed by the pack phase)
@@ -50,10 +50,9 @@ constexpr uint32_t kSSChunk = 512;
 // kernels tag what they publish with the batch, so it is never cleared).
 struct PackSync {
     uint32_t epoch;           // tag of the last batch run on this state
-    uint32_t ticket, done;    // pack phase: chunk tickets, chunks finished
+    uint32_t ticket;          // pack phase: chunk tickets
     uint32_t sticket, sdone;  // scatter phase: chunk tickets; CTAs that left the kernel
-    uint32_t packed;          // tag of the batch whose pack phase is complete
-    uint32_t flag[kPackMaxCtas];
+    uint32_t flag[kPackMaxCtas];  // pack chunk c: tag << 1 (aggregates out), tag << 1 | 1 (done)
     uint32_t agg_t[kPackMaxCtas];
     uint32_t agg_k[kPackMaxCtas];
     uint32_t agg_h[kPackMaxCtas];
