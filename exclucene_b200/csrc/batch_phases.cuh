@@ -187,6 +187,12 @@ __device__ __noinline__ void pack_chunk(uint32_t bid, uint32_t npack, uint32_t t
                                            uint32_t spin) {
     const uint32_t q = bid * kPackThreads + threadIdx.x;
     uint32_t nt = 0, nk = 0, lb0 = 0, l0 = 0;
+    // sorted terms of a query of <= kPackRegTerms terms, written only after
+    // this chunk's aggregates are published (a release waits for its warp's
+    // earlier writes)
+    uint32_t idr[kPackRegTerms];
+    uint32_t kreg = 0;
+    bool regq = false;
     if (q < nq) {
         const uint32_t t0 = toff[q], t1 = toff[q + 1];
         uint32_t k = t1 >= t0 ? t1 - t0 : 0u;
@@ -225,8 +231,9 @@ __device__ __noinline__ void pack_chunk(uint32_t bid, uint32_t npack, uint32_t t
                         x = lbl[j]; lbl[j] = lbl[j - 1]; lbl[j - 1] = x;
                     }
 #pragma unroll
-            for (uint32_t j = 0; j < kPackRegTerms; ++j)
-                if (j < k) dst[j] = id[j];
+            for (uint32_t j = 0; j < kPackRegTerms; ++j) idr[j] = id[j];
+            kreg = k;
+            regq = true;
             nt = k ? ntl[0] : 0u;
             nk = k ? len[0] : 0u;
             lb0 = k ? lbl[0] : 0u;
@@ -265,12 +272,12 @@ __device__ __noinline__ void pack_chunk(uint32_t bid, uint32_t npack, uint32_t t
                 len[j] = cl;
             }
             for (uint32_t i = 0; i < k; ++i) dst[i] = id[i];
+            const_cast<uint32_t *>(b.qnterms)[q] = k;
             lb0 = k ? __ldg(&lists[id[0]].log2_block) : 0u;
             nt = k ? split_tiles(len[0], __ldg(&lists[id[0]].ntiles), lb0, b.tile_split) : 0u;
             nk = k ? len[0] : 0u;
             l0 = k ? id[0] : 0u;
         }
-        const_cast<uint32_t *>(b.qnterms)[q] = k;
     }
     const uint32_t nh = heavy_tiles(nk, nt, lb0, b.tile_split);
     uint32_t ex[3], tot[3];
@@ -282,11 +289,18 @@ __device__ __noinline__ void pack_chunk(uint32_t bid, uint32_t npack, uint32_t t
         sync->agg_h[bid] = tot[2];
         st_release(&sync->flag[bid], tag << 1);  // aggregates out
     }
+    if (regq) {
+        uint32_t *dst = const_cast<uint32_t *>(b.qterms) + (size_t)q * kMaxTerms;
+#pragma unroll
+        for (uint32_t j = 0; j < kPackRegTerms; ++j)
+            if (j < kreg) dst[j] = idr[j];
+        const_cast<uint32_t *>(b.qnterms)[q] = kreg;
+    }
     if (threadIdx.x < 32) {
         // warp 0: the predecessors' totals. Every predecessor took its ticket
         // earlier, so it is running or done. Each lane has the flags of four
-        // predecessors in flight at once; one fence then orders the totals'
-        // loads after the flags that published them.
+        // predecessors in flight at once (acquire loads: the totals' loads
+        // after them see what the flags published).
         const uint32_t lane = threadIdx.x;
         uint32_t pt = 0, pk = 0, ph = 0;
         for (uint32_t p0 = 0; p0 < bid; p0 += 128) {
@@ -294,7 +308,7 @@ __device__ __noinline__ void pack_chunk(uint32_t bid, uint32_t npack, uint32_t t
 #pragma unroll
             for (uint32_t j = 0; j < 4; ++j) {
                 const uint32_t p = p0 + lane + 32u * j;
-                f[j] = p < bid ? ld_relaxed(&sync->flag[p]) : tag << 1;
+                f[j] = p < bid ? ld_acquire(&sync->flag[p]) : tag << 1;
             }
 #pragma unroll
             for (uint32_t j = 0; j < 4; ++j) {
@@ -306,10 +320,9 @@ __device__ __noinline__ void pack_chunk(uint32_t bid, uint32_t npack, uint32_t t
                         break;
                     }
                     __nanosleep(32);
-                    f[j] = ld_relaxed(&sync->flag[p]);
+                    f[j] = ld_acquire(&sync->flag[p]);
                 }
             }
-            __threadfence();
 #pragma unroll
             for (uint32_t j = 0; j < 4; ++j) {
                 const uint32_t p = p0 + lane + 32u * j;
