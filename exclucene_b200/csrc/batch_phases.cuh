@@ -10,10 +10,9 @@
 //            tiles from the front, the others from the back). Each chunk
 //            publishes a done flag; the probe phase waits for all of them.
 //   probe    kernels.cu: warps take work records from a counter.
-//   scatter  once every tile is probed (a count the probe warps add to once
-//            each as they leave the probe loop, which every CTA acquires
-//            before it reads any tile's results), CTAs take chunks of 512
-//            tiles; each chunk owner scans its survivor counts, finds its base
+//   scatter  CTAs take chunks of 512 tiles; a chunk owner waits until every
+//            tile is probed (a count the probe warps add to once each as they
+//            leave the probe loop), then scans its survivor counts, finds its base
 //            by a decoupled look-back (replaces cudppScan,
 //            ParaPFD_Intersection.cu:262), writes the offsets of the queries
 //            that start in the chunk (ucntResult, :301) and copies its
@@ -60,6 +59,14 @@ __device__ __forceinline__ uint64_t global_ns() {
 }
 
 constexpr uint32_t kPackRegTerms = 8;  // queries with up to this many terms are sorted in registers
+
+// Sleep between polls of a cross-CTA word: 64 ns doubling to about 1 us, so a
+// poller that waits long (a CTA done with its work, waiting for the slowest)
+// puts little load on the word's L2 slice, which the working CTAs also use.
+__device__ __forceinline__ void poll_pause(uint32_t &ns) {
+    __nanosleep(ns);
+    ns = ns < 1024u ? ns * 2u : ns;
+}
 
 // Batch tags cycle through 1 .. 2^30 - 1 (0 is the state of fresh memory).
 __device__ __forceinline__ uint32_t next_tag(uint32_t e) { return e >= (1u << 30) - 1u ? 1u : e + 1u; }
@@ -409,13 +416,13 @@ __device__ __forceinline__ void wait_packed(const PackSync *sync, uint32_t npack
                                             uint32_t spin, uint32_t lane) {
     const uint32_t want = (tag << 1) | 1u;
     for (uint32_t p = lane; p < npack; p += 32) {
-        uint32_t spins = 0;
+        uint32_t spins = 0, ns = 64;
         while (ld_acquire(&sync->flag[p]) != want) {
             if (++spins > spin) {
                 atomicOr(err, kErrScanSpin);
                 break;
             }
-            __nanosleep(32);
+            poll_pause(ns);
         }
     }
     __syncwarp();
@@ -430,9 +437,9 @@ __device__ __forceinline__ void hand_over_flags(const BatchView &b) {
 }
 
 // Scatter phase, run by every CTA once its warps have left the probe loop.
-// Every CTA first acquires the count of probed tiles (all tiles done: their
-// counts, slots and first-tile marks, written by other CTAs, are read below).
-// Then CTAs take chunks of 512 tiles by ticket, and each chunk owner does all
+// CTAs take chunks of 512 tiles by ticket; a chunk owner first acquires the
+// count of probed tiles (all tiles done: their counts, slots and first-tile
+// marks, written by other CTAs, are read only by chunk owners), then does all
 // of its chunk's work: the survivor counts' block scan, a decoupled look-back
 // over the chunks for its base (replaces cudppScan, ParaPFD_Intersection.cu:262),
 // the offsets of the queries whose first tile is in the chunk (replaces
@@ -452,19 +459,23 @@ __device__ __noinline__ void scatter_phase(const BatchView &b, PackSync *__restr
         for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q <= nq; q += gridDim.x * blockDim.x) offsets[q] = 0u;
         return;
     }
-    if (threadIdx.x == 0) {
-        uint32_t spins = 0;
-        while (ld_acquire(b.probe_done) != T) {
-            if (++spins > spin) {
-                atomicOr(b.err, kErrScanSpin);
-                break;
-            }
-            __nanosleep(64);
-        }
-    }
-    __syncthreads();
     for (;;) {
-        if (threadIdx.x == 0) sm.c = atomicAdd(&sync->sticket, 1u);
+        // a chunk owner starts once every tile of the batch is probed (the
+        // tiles' counts, slots and marks, written by other CTAs, are read
+        // below); a CTA without a chunk reads nothing and leaves at once
+        if (threadIdx.x == 0) {
+            sm.c = atomicAdd(&sync->sticket, 1u);
+            if (sm.c < nch) {
+                uint32_t spins = 0, ns = 64;
+                while (ld_acquire(b.probe_done) != T) {
+                    if (++spins > spin) {
+                        atomicOr(b.err, kErrScanSpin);
+                        break;
+                    }
+                    poll_pause(ns);
+                }
+            }
+        }
         __syncthreads();
         const uint32_t c = sm.c;
         if (c >= nch) break;

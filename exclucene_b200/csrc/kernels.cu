@@ -223,23 +223,13 @@ __global__ void __launch_bounds__(kBatchWarps * 32, MINB) k_batch(DevIndexView i
         const uint32_t T = min(b.tile_prefix[b.nq], b.max_tiles);
         const uint32_t H = min(b.tile_prefix[b.nq + 1], T);
         uint32_t probes = 0, fallbacks = 0, nkeys = 0, merges = 0, done = 0;
-        // software pipeline over work items: lane 0 takes the next ticket as
-        // an item starts and loads its record once the item's tile is decoded,
-        // so both round trips overlap the item and the next one starts with
-        // its record in hand
-        auto rec_at = [&](uint32_t wi) { return b.tile_order[wi < H ? wi : b.max_tiles - 1u - (wi - H)]; };
-        uint32_t nwi = 0;
-        uint4 nwr = make_uint4(0u, 0u, 0u, 0u);
-        if (lane == 0) {
-            nwi = atomicAdd(b.tile_counter, 1u);
-            if (nwi < T) nwr = rec_at(nwi);
-        }
         for (;;) {
-            const uint32_t wi = __shfl_sync(0xffffffffu, nwi, 0);
+            uint32_t wi = 0;
+            if (lane == 0) wi = atomicAdd(b.tile_counter, 1u);
+            wi = __shfl_sync(0xffffffffu, wi, 0);
             if (wi >= T) break;
-            const uint32_t t = __shfl_sync(0xffffffffu, nwr.x, 0), q = __shfl_sync(0xffffffffu, nwr.y, 0),
-                           ti = __shfl_sync(0xffffffffu, nwr.z, 0), list0 = __shfl_sync(0xffffffffu, nwr.w, 0);
-            if (lane == 0) nwi = atomicAdd(b.tile_counter, 1u);
+            const uint4 wr = b.tile_order[wi < H ? wi : b.max_tiles - 1u - (wi - H)];
+            const uint32_t t = wr.x, q = wr.y, ti = wr.z, list0 = wr.w;
             // the query's sorted terms (lane j holds term j), term count, key base
             // and the shortest list's descriptor: one round of independent loads
             const uint32_t tq = b.qterms[(size_t)q * kMaxTerms + lane];
@@ -276,7 +266,6 @@ __global__ void __launch_bounds__(kBatchWarps * 32, MINB) k_batch(DevIndexView i
                 }
             }
             nkeys += kc;
-            if (lane == 0 && nwi < T) nwr = rec_at(nwi);
             uint32_t alive = kc;
             for (uint32_t j = 1; j < k && alive; ++j) {
                 const uint32_t lj = __shfl_sync(0xffffffffu, tq, j);

@@ -124,7 +124,7 @@ extern "C" int excl_intersect_device_noalloc(excl_index *ix, const uint32_t *d_t
     b.merge_segs = 2;
     b.max_keys = kNAKeys;
     b.err = base + kOffMisc;
-    b.probe_done = base + kOffMisc + 2;
+    b.probe_done = base + kOffMisc + 32;  // its own 128-byte line, apart from the queue head
     b.stats = reinterpret_cast<uint64_t *>(base + kOffStats);
     BatchLaunch L{};
     L.ixv = ix->dev->view(ix->models ? model_view(ix->models) : ModelView{});

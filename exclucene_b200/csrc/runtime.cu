@@ -231,7 +231,7 @@ int ctx_alloc_batch(excl_ctx *ctx) {
     st |= dalloc(ctx, &ctx->d_tile_slot, (size_t)ctx->max_tiles + 1, "alloc tile slot");
     st |= dalloc(ctx, &ctx->d_tile_order, (size_t)ctx->max_tiles + 1, "alloc tile order");
     st |= dalloc(ctx, &ctx->d_scratch, (size_t)c.max_keys, "alloc scratch");
-    st |= dalloc(ctx, &ctx->d_misc, 16, "alloc misc");
+    st |= dalloc(ctx, &ctx->d_misc, kMiscWords, "alloc misc");
     st |= dalloc(ctx, &ctx->d_stats, 8, "alloc stats");
     st |= dalloc(ctx, &ctx->d_sync, 1, "alloc pack sync");
     st |= dalloc(ctx, &ctx->d_chunk_state, (size_t)ctx->max_tiles / kSSChunk + 2, "alloc chunk states");
@@ -245,7 +245,7 @@ int ctx_alloc_batch(excl_ctx *ctx) {
     if (!st) st |= cuda_status(ctx, cudaHostGetDevicePointer((void **)&ctx->m_flags, ctx->h_flags, 0), "mapped flags");
     if (st) return EXCL_E_NOMEM;
     for (uint32_t i = kFlagSlots; i-- > 0;) ctx->free_flag_slots.push_back(i);
-    cudaMemsetAsync(ctx->d_misc, 0, 16 * 4, ctx->stream);
+    cudaMemsetAsync(ctx->d_misc, 0, kMiscWords * 4, ctx->stream);
     cudaMemsetAsync(ctx->d_stats, 0, 8 * 8, ctx->stream);
     cudaMemsetAsync(ctx->d_sync, 0, sizeof(PackSync), ctx->stream);
     cudaMemsetAsync(ctx->d_chunk_state, 0, ((size_t)ctx->max_tiles / kSSChunk + 2) * 8, ctx->stream);

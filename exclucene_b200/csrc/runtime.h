@@ -35,8 +35,9 @@ enum {
     kMiscErr = 0,
     kMiscTileCounter = 1,
     kMiscDecodeTicket = 2,  // and 3: decode work counter, CTAs done
-    kMiscProbeDone = 4,     // tiles probed (batch kernel)
     kMiscNeverSet = 5,      // stays 0: the flag of the failure-path self-test wait
+    kMiscProbeDone = 32,    // tiles probed (batch kernel); its own 128-byte line, apart from the queue head
+    kMiscWords = 64,
 };
 // excl_submit_into batches that may be in flight on one context at once
 constexpr uint32_t kFlagSlots = 256;
