@@ -15,8 +15,9 @@
 //            leave the probe loop), then scans its survivor counts, finds its base
 //            by a decoupled look-back (replaces cudppScan,
 //            ParaPFD_Intersection.cu:262), writes the offsets of the queries
-//            that start in the chunk (ucntResult, :301) and copies its
-//            survivors to the result array (saCompact, :279).
+//            that start in the chunk (ucntResult, :301) and its tiles' output
+//            positions, and counts itself ready; once every chunk is ready,
+//            every warp of the grid copies survivors (saCompact, :279).
 //
 // Every wait is on work that a running CTA already holds (a ticket it took,
 // tiles it took), so the grid needs no co-residency and batches on other
@@ -96,8 +97,6 @@ struct PackShared {
 };
 struct ScatterShared {
     uint32_t sa[33];
-    uint32_t ex[kSSChunk];    // exclusive survivor prefix of the chunk's tiles
-    uint32_t slot[kSSChunk];  // their survivor slots
     uint32_t c, base;
 };
 
@@ -397,6 +396,7 @@ __device__ __noinline__ void pack_chunk(uint32_t bid, uint32_t npack, uint32_t t
     if (bid == 0 && threadIdx.x == 0) {
         *b.tile_counter = 0u;
         *b.probe_done = 0u;
+        *b.scatter_ready = 0u;
         if (b.stats) {
             b.stats[0] = b.stats[1] = b.stats[2] = b.stats[3] = b.stats[6] = 0ull;
             b.stats[5] = ~0ull;
@@ -438,13 +438,13 @@ __device__ __forceinline__ void hand_over_flags(const BatchView &b) {
 
 // Scatter phase, run by every CTA once its warps have left the probe loop.
 // CTAs take chunks of 512 tiles by ticket; a chunk owner first acquires the
-// count of probed tiles (all tiles done: their counts, slots and first-tile
-// marks, written by other CTAs, are read only by chunk owners), then does all
-// of its chunk's work: the survivor counts' block scan, a decoupled look-back
-// over the chunks for its base (replaces cudppScan, ParaPFD_Intersection.cu:262),
-// the offsets of the queries whose first tile is in the chunk (replaces
-// ucntResult, :301) and the copy of the chunk's survivors to the result array
-// (replaces saCompact, :279), one survivor per thread, so the stores coalesce.
+// count of probed tiles (all tiles done: their counts and first-tile marks,
+// written by other CTAs), then scans the chunk's survivor counts, finds its
+// base by a decoupled look-back over the chunks (replaces cudppScan,
+// ParaPFD_Intersection.cu:262), writes the offsets of the queries whose first
+// tile is in the chunk (replaces ucntResult, :301) and each tile's output
+// position, and counts the chunk ready. Every CTA then copies survivors to
+// the result array (replaces saCompact, :279) once all chunks are ready.
 __device__ __noinline__ void scatter_phase(const BatchView &b, PackSync *__restrict__ sync,
                                            uint64_t *__restrict__ chunk_state, uint32_t *__restrict__ offsets,
                                            uint32_t *__restrict__ docids, uint64_t cap, uint32_t tag,
@@ -479,14 +479,12 @@ __device__ __noinline__ void scatter_phase(const BatchView &b, PackSync *__restr
         __syncthreads();
         const uint32_t c = sm.c;
         if (c >= nch) break;
-        // the chunk's tiles: counts, survivor slots, first-tile marks (query + 1
-        // for a query's first tile, else 0), all loads in flight at once
+        // the chunk's tiles: counts and first-tile marks (query + 1 for a
+        // query's first tile, else 0), all loads in flight at once
         const uint32_t t0 = c * kSSChunk;
         const uint32_t ja = threadIdx.x * kPer, ta = t0 + ja;
         const uint32_t c0 = ta < T ? b.tile_count[ta] : 0u;
         const uint32_t c1 = ta + 1 < T ? b.tile_count[ta + 1] : 0u;
-        const uint32_t s0 = ta < T ? b.tile_slot[ta] : 0u;
-        const uint32_t s1 = ta + 1 < T ? b.tile_slot[ta + 1] : 0u;
         const uint32_t f0 = ta < T ? b.tile_q[ta] : 0u;
         const uint32_t f1 = ta + 1 < T ? b.tile_q[ta + 1] : 0u;
         // a query before a first tile that has no tiles itself shares its offset
@@ -495,10 +493,6 @@ __device__ __noinline__ void scatter_phase(const BatchView &b, PackSync *__restr
         uint32_t tot;
         const uint32_t ex = block_scan1(c0 + c1, tot, sm.sa);
         if (threadIdx.x == 0) st_release64(&chunk_state[c], chunk_word(tag, kAggregate, tot));
-        sm.ex[ja] = ex;
-        sm.ex[ja + 1] = ex + c0;
-        sm.slot[ja] = s0;
-        sm.slot[ja + 1] = s1;
         if (w == 0) {
             // look-back: sum the aggregates of the preceding chunks up to the
             // nearest one that has published its inclusive prefix
@@ -555,19 +549,59 @@ __device__ __noinline__ void scatter_phase(const BatchView &b, PackSync *__restr
             offsets[nq] = base + tot;
             for (uint32_t q = nq; q > 0 && b.tile_prefix[q - 1u] >= T; --q) offsets[q - 1u] = base + tot;
         }
-        // the chunk's survivors, flattened: element e belongs to the last tile
-        // whose chunk prefix is <= e
-        for (uint32_t e = threadIdx.x; e < tot; e += blockDim.x) {
-            uint32_t lo = 0, hi = kSSChunk - 1;
-            while (lo < hi) {
-                const uint32_t mid = (lo + hi + 1) >> 1;
-                if (sm.ex[mid] <= e) lo = mid;
-                else hi = mid - 1;
+        // each tile's output position, in place of its first-tile mark (read above)
+        if (ta < T) b.tile_q[ta] = base + ex;
+        if (ta + 1 < T) b.tile_q[ta + 1] = base + ex + c0;
+        // the chunk is ready once every thread's writes are visible
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) red_release_add(b.scatter_ready, 1u);
+    }
+    // Survivors, copied by every warp of the grid once every chunk is ready
+    // (one acquire per CTA; the ready chunks' owners acquired the probed count
+    // before reading the tiles, so the tiles' results are visible too). A
+    // batch's survivors gather in the chunks of its heaviest queries, so the
+    // copy is spread over the whole grid: warp w takes tiles w, w + nw, ...;
+    // lane j fetches the count, slot and output position of the warp's j-th
+    // tile of a round, all lanes at once, and the warp then copies the round's
+    // non-empty tiles with eight independent loads per lane.
+    if (threadIdx.x == 0) {
+        uint32_t spins = 0, ns = 64;
+        while (ld_acquire(b.scatter_ready) != nch) {
+            if (++spins > spin) {
+                atomicOr(b.err, kErrScanSpin);
+                break;
             }
-            const uint64_t o = (uint64_t)base + e;
-            if (o < cap) docids[o] = b.scratch[sm.slot[lo] + (e - sm.ex[lo])];
+            poll_pause(ns);
         }
-        __syncthreads();  // sm is reused by the next chunk
+    }
+    __syncthreads();
+    const uint32_t gw = blockIdx.x * (blockDim.x / 32) + w, nw = gridDim.x * (blockDim.x / 32);
+    const uint32_t *__restrict__ scr = b.scratch;
+    for (uint64_t j0 = 0; gw + j0 * nw < T; j0 += 32) {
+        const uint64_t tt = gw + (j0 + lane) * nw;
+        const uint32_t t = tt < T ? (uint32_t)tt : T;
+        const uint32_t n = t < T ? b.tile_count[t] : 0u;
+        const uint32_t o = n ? b.tile_q[t] : 0u, slot = n ? b.tile_slot[t] : 0u;
+        uint32_t m = __ballot_sync(0xffffffffu, n != 0u);
+        while (m) {
+            const uint32_t l = (uint32_t)(__ffs(m) - 1);
+            m &= m - 1u;
+            const uint32_t nl = __shfl_sync(0xffffffffu, n, l), ol = __shfl_sync(0xffffffffu, o, l),
+                           sl = __shfl_sync(0xffffffffu, slot, l);
+            const uint32_t *src = scr + sl;
+            uint32_t v[kTileKeys / 32];
+#pragma unroll
+            for (uint32_t i = 0; i < kTileKeys / 32; ++i) {
+                const uint32_t k = lane + 32u * i;
+                if (k < nl) v[i] = src[k];
+            }
+#pragma unroll
+            for (uint32_t i = 0; i < kTileKeys / 32; ++i) {
+                const uint32_t k = lane + 32u * i;
+                if (k < nl && (uint64_t)ol + k < cap) docids[(uint64_t)ol + k] = v[i];
+            }
+        }
     }
 }
 

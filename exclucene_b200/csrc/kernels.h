@@ -14,7 +14,8 @@ struct BatchView {
     const uint32_t *qterms;      // nq * kMaxTerms list ids, ascending length
     const uint32_t *qnterms;     // terms per query
     const uint32_t *tile_prefix; // nq + 1, exclusive prefix of tiles per query
-    uint32_t *tile_q;            // max_tiles: query + 1 where the tile is its query's first tile, else 0
+    uint32_t *tile_q;            // max_tiles: query + 1 where the tile is its query's first tile, else 0;
+                                 // then (scatter phase) the tile's output position
     uint4 *tile_order;           // max_tiles work records {tile, query, tile within the query, shortest list}:
                                  // heavy tiles from the front, the rest from the back (tile_prefix[nq + 1] = heavy tiles)
     uint32_t *tile_counter;      // work-queue head (zeroed by the pack phase)
@@ -29,6 +30,7 @@ struct BatchView {
     uint32_t *err;               // error flag bits
     uint32_t *err_out;           // or null: device-mapped host word that receives this batch's error bits at its end (the device word is cleared)
     uint32_t *probe_done;        // tiles probed so far (cleared by the pack phase)
+    uint32_t *scatter_ready;     // scatter chunks whose output positions are out (cleared by the pack phase)
     uint32_t check_polls;        // > 0: one bounded wait on check_flag (which nothing sets) that must give up
     const uint32_t *check_flag;
     uint64_t *stats;             // or null: [probes, fallbacks, keys, merges, t_start, t_packed, t_probed, t_end]

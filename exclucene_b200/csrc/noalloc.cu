@@ -125,6 +125,7 @@ extern "C" int excl_intersect_device_noalloc(excl_index *ix, const uint32_t *d_t
     b.max_keys = kNAKeys;
     b.err = base + kOffMisc;
     b.probe_done = base + kOffMisc + 32;  // its own 128-byte line, apart from the queue head
+    b.scatter_ready = base + kOffMisc + 48;
     b.stats = reinterpret_cast<uint64_t *>(base + kOffStats);
     BatchLaunch L{};
     L.ixv = ix->dev->view(ix->models ? model_view(ix->models) : ModelView{});

@@ -288,6 +288,7 @@ int run_pipeline(excl_ctx *ctx, excl_index *ix, const uint32_t *d_terms, const u
     b.err = ctx->d_misc + kMiscErr;
     b.err_out = err_out;
     b.probe_done = ctx->d_misc + kMiscProbeDone;
+    b.scatter_ready = ctx->d_misc + kMiscScatterReady;
     b.check_polls = ctx->wait_check_polls;
     b.check_flag = ctx->d_misc + kMiscNeverSet;
     b.stats = ctx->collect_stats ? ctx->d_stats : nullptr;

@@ -37,6 +37,7 @@ enum {
     kMiscDecodeTicket = 2,  // and 3: decode work counter, CTAs done
     kMiscNeverSet = 5,      // stays 0: the flag of the failure-path self-test wait
     kMiscProbeDone = 32,    // tiles probed (batch kernel); its own 128-byte line, apart from the queue head
+    kMiscScatterReady = 48, // scatter chunks ready (batch kernel); another line
     kMiscWords = 64,
 };
 // excl_submit_into batches that may be in flight on one context at once

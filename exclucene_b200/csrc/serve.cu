@@ -256,6 +256,7 @@ int launch_on_slot(excl_server *s, Slot *sl, uint64_t nterms, uint64_t tiles, ui
     b.err = sl->d_misc;
     b.err_out = sl->m_err;
     b.probe_done = sl->d_misc + 32;  // its own 128-byte line, apart from the queue head
+    b.scatter_ready = sl->d_misc + 48;
     b.stats = nullptr;
     BatchLaunch bl{};
     bl.ixv = s->ix->dev->view(s->ix->models ? model_view(s->ix->models) : ModelView{});
