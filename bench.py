@@ -286,7 +286,7 @@ def bench_config(w, params, desc) -> dict:
     return {"workload": desc, "codec": params["codec"] if "codecs" not in params else "parapfd+seglrc",
             "block": params["block"], "frac": params["frac"], "queries_per_step": int(w.nq),
             "postings_per_step": int(lens[w.terms.astype(np.int64)].sum()),
-            "l2": "GPU arm: flushed (512 MB read) before each timed step; CPU arm: n/a"}
+            "l2": "GPU arm: flushed (512 MB read on the batch's stream) before each timed step; CPU arm: n/a"}
 
 
 def reference_arm(args, w, desc, params):
@@ -342,9 +342,8 @@ def decode_measure(ctx, ix, w, sizes, arrays, stream, flush, args):
         ctx.decode_lists_device(ix, 0, ix.nlists, out.data_ptr())
     times = []
     for _ in range(args.steps):
-        flush_l2(flush)
-        torch.cuda.synchronize()
         with torch.cuda.stream(stream):
+            flush_l2(flush)  # on the decode's stream, no host sync: the events time the kernel alone
             e0.record(stream)
             ctx.decode_lists_device(ix, 0, ix.nlists, out.data_ptr())
             e1.record(stream)
@@ -531,9 +530,14 @@ def main():
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
+        # the L2 flush runs on the batch's own stream just before it, with no
+        # host sync in between: the host has enqueued the batch while the
+        # flush runs, so the events around the batch time the kernel on the
+        # device, not the host's launch call (e2e below times that)
+        cstream = torch.cuda.ExternalStream(c.stream, device=dev)
         for _ in range(k):
-            flush_l2(flush)
-            torch.cuda.synchronize()
+            with torch.cuda.stream(cstream):
+                flush_l2(flush)
             step(c, algo)
             st = c.stats()
             tot.append(st.total_ms)

@@ -151,7 +151,6 @@ __device__ __forceinline__ int locate_segment(const DevIndexView &ix, const List
 // decodes that span into shared memory once and every key is looked up there;
 // otherwise each key is probed on its own (probe_key).
 
-constexpr int kBatchWarps = 8;
 static_assert(kBatchWarps * 32 == kPackThreads && kBatchWarps * 32 == kSSThreads, "one CTA shape for every phase");
 
 struct ProbeShared {
@@ -407,7 +406,10 @@ static cudaError_t launch_batch_t(const BatchLaunch &L, cudaStream_t st) {
         per_sm = per_sm > 0 ? per_sm : 1;
         if (dev >= 0 && dev < 64) occ[dev] = per_sm;
     }
-    const uint32_t grid = (uint32_t)std::max(1, std::min(per_sm, MINB) * L.nsm);
+    // a small batch (its tile count known on the host) takes one warp per
+    // tile, so the batches of other streams keep the rest of the device
+    uint32_t grid = (uint32_t)std::max(1, std::min(per_sm, MINB) * L.nsm);
+    if (L.max_ctas) grid = std::min(grid, L.max_ctas);
     k_batch<ALGO, MINB, KIND><<<grid, kBatchWarps * 32, 0, st>>>(L.ixv, L.b, L.sync, L.chunk_state, L.lists, L.nlists,
                                                                   L.terms, L.toff, L.offsets, L.docids, L.cap,
                                                                   L.spin ? L.spin : kSpin);

@@ -47,6 +47,7 @@ constexpr uint32_t kPackMaxCtas = 1024;
 constexpr uint32_t kPackMaxQueries = kPackThreads * kPackMaxCtas;
 constexpr uint32_t kSSThreads = 256;
 constexpr uint32_t kSSChunk = 512;
+constexpr uint32_t kBatchWarps = 8;  // warps per CTA of the batch kernel (every phase)
 
 // Cross-CTA state of one stream's batches (zeroed once at allocation; the
 // kernels tag what they publish with the batch, so it is never cleared).
@@ -73,6 +74,8 @@ struct BatchLaunch {
     uint32_t *docids;       // cap
     uint64_t cap;
     int algo, warps, ctas_per_sm, nsm;
+    uint32_t max_ctas;  // > 0: launch at most this many CTAs (a batch whose tile count the host knows needs
+                        // no more than one warp per tile); 0: every CTA that fits on the device
     uint32_t spin;    // polls before a cross-CTA wait gives up (0: the default)
     cudaEvent_t *ev;  // 4 events around the batch kernel, or null
 };

@@ -252,9 +252,25 @@ int ctx_alloc_batch(excl_ctx *ctx) {
     return cuda_status(ctx, cudaStreamSynchronize(ctx->stream), "ctx init");
 }
 
+uint32_t host_batch_tiles(const excl_ctx *ctx, const excl_index *ix, const uint32_t *terms,
+                          const uint32_t *term_offsets, uint32_t nq) {
+    if (nq > kHostTilesMaxQueries || !terms) return 0;
+    uint64_t tiles = 0;
+    for (uint32_t q = 0; q < nq; ++q) {
+        const ListDesc *best = nullptr;
+        for (uint32_t i = term_offsets[q]; i < term_offsets[q + 1]; ++i) {
+            const uint32_t t = terms[i];
+            if (t < ix->nlists && (!best || ix->lists[t].n < best->n)) best = &ix->lists[t];
+        }
+        if (best) tiles += split_tiles(best->n, best->ntiles, best->log2_block, ctx->tile_split);
+    }
+    return (uint32_t)std::min<uint64_t>(std::max<uint64_t>(tiles, 1), 0xffffffffu);
+}
+
 // Runs the whole device pipeline for nq queries whose terms are in device memory.
 int run_pipeline(excl_ctx *ctx, excl_index *ix, const uint32_t *d_terms, const uint32_t *d_toff, uint32_t nq,
-                 uint32_t algo, uint32_t *d_offsets, uint32_t *d_docids, uint64_t cap, uint32_t *err_out) {
+                 uint32_t algo, uint32_t *d_offsets, uint32_t *d_docids, uint64_t cap, uint32_t *err_out,
+                 uint32_t tiles_hint) {
     if (!ix->dev) {
         ctx_error(ctx, "index not uploaded");
         return EXCL_E_INVALID;
@@ -308,6 +324,7 @@ int run_pipeline(excl_ctx *ctx, excl_index *ix, const uint32_t *d_terms, const u
     L.warps = ctx->warps;
     L.ctas_per_sm = ctx->ctas_per_sm;
     L.nsm = ctx->nsm;
+    L.max_ctas = tiles_hint ? std::max<uint32_t>(1, (tiles_hint + kBatchWarps - 1) / kBatchWarps) : 0u;
     L.spin = ctx->spin_limit;
     L.ev = ctx->ev;
     ctx->last_was_graph = false;
@@ -317,14 +334,14 @@ int run_pipeline(excl_ctx *ctx, excl_index *ix, const uint32_t *d_terms, const u
         uint64_t vh = 1469598103934665603ull;
         const unsigned char *vb = reinterpret_cast<const unsigned char *>(&L.ixv);
         for (size_t i = 0; i < sizeof L.ixv; ++i) vh = (vh ^ vb[i]) * 1099511628211ull;
-        const uint64_t key[11] = {(uint64_t)(uintptr_t)ix, vh, (uint64_t)(uintptr_t)d_terms,
+        const uint64_t key[12] = {(uint64_t)(uintptr_t)ix, vh, (uint64_t)(uintptr_t)d_terms,
                                   (uint64_t)(uintptr_t)d_toff, nq, algo, (uint64_t)(uintptr_t)d_offsets,
                                   (uint64_t)(uintptr_t)d_docids, cap,
                                   (uint64_t)ctx->collect_stats | (uint64_t)ctx->merge_segs << 8 |
                                       (uint64_t)ctx->warps << 16 | (uint64_t)ctx->ctas_per_sm << 32 |
                                       (uint64_t)ctx->tile_split << 40 | (uint64_t)(ctx->spin_limit != 0) << 48 |
                                       (uint64_t)(ctx->wait_check_polls != 0) << 49,
-                                  (uint64_t)(uintptr_t)err_out};
+                                  (uint64_t)(uintptr_t)err_out, L.max_ctas};
         const bool same = ctx->gkey_seen && std::memcmp(key, ctx->gkey, sizeof key) == 0;
         if (same || ctx->gexec) {
             if (!same || !ctx->gexec) {
@@ -807,7 +824,7 @@ extern "C" int excl_submit(excl_ctx *ctx, excl_index *ix, const uint32_t *terms,
     const int32_t slot = take_slot(ctx);
     if (slot < 0) return EXCL_E_CAPACITY;
     s = run_pipeline(ctx, ix, ctx->d_terms, ctx->d_toff, nq, algo, ctx->d_offsets, ctx->d_docids, ctx->docids_cap,
-                     ctx->m_flags + slot);
+                     ctx->m_flags + slot, host_batch_tiles(ctx, ix, terms, term_offsets, nq));
     if (!s)
         s = cuda_status(ctx, cudaMemcpyAsync(ctx->h_offsets, ctx->d_offsets, ((size_t)nq + 1) * 4,
                                              cudaMemcpyDeviceToHost, st),
@@ -951,7 +968,8 @@ extern "C" int excl_submit_into(excl_ctx *ctx, excl_index *ix, const uint32_t *t
     if (s) return s;
     const int32_t slot = take_slot(ctx);
     if (slot < 0) return EXCL_E_CAPACITY;
-    s = run_pipeline(ctx, ix, q_terms, q_toff, nq, algo, mapped[0], mapped[1], cap, ctx->m_flags + slot);
+    s = run_pipeline(ctx, ix, q_terms, q_toff, nq, algo, mapped[0], mapped[1], cap, ctx->m_flags + slot,
+                     host_batch_tiles(ctx, ix, terms, term_offsets, nq));
     if (s) {
         cudaStreamSynchronize(st);
         ctx->free_flag_slots.push_back((uint32_t)slot);

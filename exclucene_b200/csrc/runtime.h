@@ -59,7 +59,7 @@ struct excl_ctx {
     // CUDA graph of the last batch launched through excl_intersect_device
     bool use_graphs = false, last_was_graph = false;
     cudaGraphExec_t gexec = nullptr;
-    uint64_t gkey[11] = {};
+    uint64_t gkey[12] = {};
     bool gkey_seen = false;  // the key ran once uncaptured (first sighting)
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -95,8 +95,16 @@ void ctx_error(excl_ctx *ctx, const char *fmt, ...);
 int cuda_status(excl_ctx *ctx, cudaError_t e, const char *what);
 int read_device_flags(excl_ctx *ctx);
 int flags_status(excl_ctx *ctx, uint32_t f);
+// tiles_hint > 0: the batch's tile count, known on the host, caps the grid at one warp per tile
 int run_pipeline(excl_ctx *ctx, excl_index *ix, const uint32_t *d_terms, const uint32_t *d_toff, uint32_t nq,
-                 uint32_t algo, uint32_t *d_offsets, uint32_t *d_docids, uint64_t cap, uint32_t *err_out = nullptr);
+                 uint32_t algo, uint32_t *d_offsets, uint32_t *d_docids, uint64_t cap, uint32_t *err_out = nullptr,
+                 uint32_t tiles_hint = 0);
+// Tiles of a batch of at most kHostTilesMaxQueries queries whose terms are in
+// host memory (the shortest list's tiles per query, as the pack phase counts
+// them); 0 for larger batches, which take the whole device anyway.
+constexpr uint32_t kHostTilesMaxQueries = 512;
+uint32_t host_batch_tiles(const excl_ctx *ctx, const excl_index *ix, const uint32_t *terms,
+                          const uint32_t *term_offsets, uint32_t nq);
 
 // learned.cu
 ModelView model_view(const ModelSet *m);

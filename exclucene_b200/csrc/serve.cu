@@ -274,6 +274,9 @@ int launch_on_slot(excl_server *s, Slot *sl, uint64_t nterms, uint64_t tiles, ui
     bl.warps = s->cfg.warps_per_cta ? (int)s->cfg.warps_per_cta : 8;
     bl.ctas_per_sm = s->cfg.ctas_per_sm ? (int)s->cfg.ctas_per_sm : 5;
     bl.nsm = s->nsm;
+    // one warp per tile: a batch of a few queries leaves the rest of the
+    // device to the batches of the other slots
+    bl.max_ctas = (uint32_t)std::max<uint64_t>(1, (tiles + kBatchWarps - 1) / kBatchWarps);
     bl.ev = nullptr;
     if (launch_batch(bl, st)) return EXCL_E_CUDA;
     return cudaEventRecord(sl->done, st) == cudaSuccess ? EXCL_OK : EXCL_E_CUDA;
