@@ -61,13 +61,10 @@ __device__ __forceinline__ uint64_t global_ns() {
 
 constexpr uint32_t kPackRegTerms = 8;  // queries with up to this many terms are sorted in registers
 
-// Sleep between polls of a cross-CTA word: 64 ns doubling to about 1 us, so a
-// poller that waits long (a CTA done with its work, waiting for the slowest)
-// puts little load on the word's L2 slice, which the working CTAs also use.
-__device__ __forceinline__ void poll_pause(uint32_t &ns) {
-    __nanosleep(ns);
-    ns = ns < 1024u ? ns * 2u : ns;
-}
+// Polls of a cross-CTA word sleep between reads, doubling from 32 ns up to a
+// cap, so a poller that waits long (a CTA done with its work, waiting for the
+// slowest) puts little load on the word's L2 slice, which the working CTAs
+// also use.
 
 // Batch tags cycle through 1 .. 2^30 - 1 (0 is the state of fresh memory).
 __device__ __forceinline__ uint32_t next_tag(uint32_t e) { return e >= (1u << 30) - 1u ? 1u : e + 1u; }
@@ -78,17 +75,32 @@ __device__ __forceinline__ uint64_t chunk_word(uint32_t tag, uint32_t status, ui
     return ((uint64_t)tag << 34) | ((uint64_t)status << 32) | v;
 }
 
-// Bounded wait until *p == tag (acquire); false (and kErrScanSpin) if it gave up.
-__device__ __forceinline__ bool wait_tag(const uint32_t *p, uint32_t tag, uint32_t *err, uint32_t spin) {
-    uint32_t spins = 0;
-    while (ld_acquire(p) != tag) {
-        if (++spins > spin) {
-            atomicOr(err, kErrScanSpin);
-            return false;
+// Bounded wait until *p == want, polled with relaxed loads (a poll touches
+// only the word's L2 line; an acquire load per poll would also order, and so
+// hold up, the poller's later loads each time); once the value is seen, one
+// acquire load makes the writes published before it visible. false (and
+// kErrScanSpin in *err) if it gave up.
+// `cap_ns` bounds the sleep between polls: short where few CTAs poll, longer
+// where the whole grid polls one word.
+__device__ __forceinline__ bool wait_eq(const uint32_t *p, uint32_t want, uint32_t *err, uint32_t spin,
+                                        uint32_t cap_ns = 1024u) {
+    uint32_t spins = 0, ns = 32;
+    for (;;) {
+        while (ld_relaxed(p) != want) {
+            if (++spins > spin) {
+                atomicOr(err, kErrScanSpin);
+                return false;
+            }
+            __nanosleep(ns);
+            ns = ns < cap_ns ? ns * 2u : cap_ns;
         }
-        __nanosleep(64);
+        if (ld_acquire(p) == want) return true;
     }
-    return true;
+}
+
+// Bounded wait until *p == tag (the failure-path self-test's flag).
+__device__ __forceinline__ bool wait_tag(const uint32_t *p, uint32_t tag, uint32_t *err, uint32_t spin) {
+    return wait_eq(p, tag, err, spin);
 }
 
 // Shared memory of the pack and scatter phases (a union with the probe's).
@@ -182,16 +194,17 @@ __device__ __forceinline__ uint32_t heavy_tiles(uint32_t n, uint32_t nt, uint32_
     return min(nt, n / S + (2u * (n % S) >= S ? 1u : 0u));
 }
 
-// Pack chunk `bid` of `npack` (queries bid*256 .. +255) with the CTA's 256
-// threads. Its flag goes to tag << 1 once its aggregates are out (for the
-// look-back of later chunks) and to tag << 1 | 1 once all its writes are
-// visible; the last chunk also writes the batch totals, chunk 0 clears the
-// probe phase's counters and the statistics.
-__device__ __noinline__ void pack_chunk(uint32_t bid, uint32_t npack, uint32_t tag, const ListDesc *__restrict__ lists,
-                                           uint32_t nlists, const uint32_t *terms, const uint32_t *toff, uint32_t nq,
-                                           const BatchView &b, PackSync *__restrict__ sync, PackShared &sm,
-                                           uint32_t spin) {
-    const uint32_t q = bid * kPackThreads + threadIdx.x;
+// Pack chunk `bid` of `npack` (queries bid*qpc .. +qpc-1, one per thread of
+// the first qpc threads; the CTA's other threads take part in its scans and
+// record writes). Its flag goes to tag << 1 once its aggregates are out (for
+// the look-back of later chunks), and it counts itself in sync->packed once
+// all its writes are visible; the last chunk also writes the batch totals,
+// chunk 0 clears the probe phase's counters and the statistics.
+__device__ __noinline__ void pack_chunk(uint32_t bid, uint32_t npack, uint32_t qpc, uint32_t tag,
+                                           const ListDesc *__restrict__ lists, uint32_t nlists, const uint32_t *terms,
+                                           const uint32_t *toff, uint32_t nq, const BatchView &b,
+                                           PackSync *__restrict__ sync, PackShared &sm, uint32_t spin) {
+    const uint32_t q = threadIdx.x < qpc ? bid * qpc + threadIdx.x : nq;
     uint32_t nt = 0, nk = 0, lb0 = 0, l0 = 0;
     // sorted terms of a query of <= kPackRegTerms terms, written only after
     // this chunk's aggregates are published (a release waits for its warp's
@@ -217,9 +230,11 @@ __device__ __noinline__ void pack_chunk(uint32_t bid, uint32_t npack, uint32_t t
             for (uint32_t j = 0; j < kPackRegTerms; ++j) {
                 const bool v = j < k && id[j] < nlists;
                 bad |= j < k && id[j] >= nlists;
-                len[j] = v ? __ldg(&lists[id[j]].n) : 0xffffffffu;  // absent terms sort last
-                lbl[j] = v ? __ldg(&lists[id[j]].log2_block) : 0u;
-                ntl[j] = v ? split_tiles(len[j], __ldg(&lists[id[j]].ntiles), lbl[j], b.tile_split) : 0u;
+                // n, ntiles and log2_block: the descriptor's first 16 bytes
+                const uint4 m = v ? __ldg(reinterpret_cast<const uint4 *>(lists + id[j])) : make_uint4(0, 0, 0, 0);
+                len[j] = v ? m.x : 0xffffffffu;  // absent terms sort last
+                lbl[j] = m.z;
+                ntl[j] = v ? split_tiles(m.x, m.y, m.z, b.tile_split) : 0u;
             }
             if (bad) {
                 atomicOr(b.err, kErrTermId);
@@ -302,42 +317,24 @@ __device__ __noinline__ void pack_chunk(uint32_t bid, uint32_t npack, uint32_t t
             if (j < kreg) dst[j] = idr[j];
         const_cast<uint32_t *>(b.qnterms)[q] = kreg;
     }
-    if (threadIdx.x < 32) {
-        // warp 0: the predecessors' totals. Every predecessor took its ticket
-        // earlier, so it is running or done. Each lane has the flags of four
-        // predecessors in flight at once (acquire loads: the totals' loads
-        // after them see what the flags published).
-        const uint32_t lane = threadIdx.x;
+    {
+        // the predecessors' totals, one predecessor per thread (all acquire
+        // loads in flight at once), then a block reduction. Every predecessor
+        // took its ticket earlier, so it is running or done.
         uint32_t pt = 0, pk = 0, ph = 0;
-        for (uint32_t p0 = 0; p0 < bid; p0 += 128) {
-            uint32_t f[4];
-#pragma unroll
-            for (uint32_t j = 0; j < 4; ++j) {
-                const uint32_t p = p0 + lane + 32u * j;
-                f[j] = p < bid ? ld_acquire(&sync->flag[p]) : tag << 1;
-            }
-#pragma unroll
-            for (uint32_t j = 0; j < 4; ++j) {
-                const uint32_t p = p0 + lane + 32u * j;
-                uint32_t spins = 0;
-                while ((f[j] >> 1) != tag) {  // aggregates out (or the chunk already done)
-                    if (++spins > spin) {
-                        atomicOr(b.err, kErrScanSpin);
-                        break;
-                    }
-                    __nanosleep(32);
-                    f[j] = ld_acquire(&sync->flag[p]);
+        for (uint32_t p = threadIdx.x; p < bid; p += blockDim.x) {
+            uint32_t f = ld_acquire(&sync->flag[p]), spins = 0;
+            while ((f >> 1) != tag) {  // aggregates not out yet
+                if (++spins > spin) {
+                    atomicOr(b.err, kErrScanSpin);
+                    break;
                 }
+                __nanosleep(32);
+                f = ld_acquire(&sync->flag[p]);
             }
-#pragma unroll
-            for (uint32_t j = 0; j < 4; ++j) {
-                const uint32_t p = p0 + lane + 32u * j;
-                if (p < bid) {
-                    pt += ld_relaxed(&sync->agg_t[p]);
-                    pk += ld_relaxed(&sync->agg_k[p]);
-                    ph += ld_relaxed(&sync->agg_h[p]);
-                }
-            }
+            pt += ld_relaxed(&sync->agg_t[p]);
+            pk += ld_relaxed(&sync->agg_k[p]);
+            ph += ld_relaxed(&sync->agg_h[p]);
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
@@ -345,10 +342,17 @@ __device__ __noinline__ void pack_chunk(uint32_t bid, uint32_t npack, uint32_t t
             pk += __shfl_xor_sync(0xffffffffu, pk, o);
             ph += __shfl_xor_sync(0xffffffffu, ph, o);
         }
+        const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
         if (lane == 0) {
-            sm.pre[0] = pt;
-            sm.pre[1] = pk;
-            sm.pre[2] = ph;
+            sm.sc[0][w] = pt;
+            sm.sc[1][w] = pk;
+            sm.sc[2][w] = ph;
+        }
+        __syncthreads();
+        if (threadIdx.x < 3) {
+            uint32_t v = 0;
+            for (uint32_t i = 0; i < (blockDim.x >> 5); ++i) v += sm.sc[threadIdx.x][i];
+            sm.pre[threadIdx.x] = v;
         }
     }
     sm.et[threadIdx.x] = et;
@@ -387,7 +391,7 @@ __device__ __noinline__ void pack_chunk(uint32_t bid, uint32_t npack, uint32_t t
             }
         }
         const uint32_t t = pt + tl, i = tl - sm.et[lo], hb = ph + sm.eh[lo];
-        const uint4 wr = make_uint4(t, bid * blockDim.x + lo, i, sm.l0[lo]);
+        const uint4 wr = make_uint4(t, bid * qpc + lo, i, sm.l0[lo]);
         if (i < sm.h[lo]) b.tile_order[hb + i] = wr;
         else b.tile_order[b.max_tiles - 1u - (t - hb - sm.h[lo])] = wr;
     }
@@ -402,30 +406,18 @@ __device__ __noinline__ void pack_chunk(uint32_t bid, uint32_t npack, uint32_t t
             b.stats[5] = ~0ull;
         }
     }
-    // this chunk is done once every thread's writes are visible: its flag
-    // moves to tag << 1 | 1, which the probe phase waits for on every chunk
+    // this chunk is done once every thread's writes are visible: it counts
+    // itself in sync->packed, which the probe phase waits for
     __threadfence();
     __syncthreads();
-    if (threadIdx.x == 0) st_release(&sync->flag[bid], (tag << 1) | 1u);
+    if (threadIdx.x == 0) red_release_add(&sync->packed, 1u);
     __syncthreads();  // sm is reused by the next chunk
 }
 
-// Bounded wait, by one warp, until every pack chunk of the batch is done
-// (flag == tag << 1 | 1); then the CTA may read the batch's records.
-__device__ __forceinline__ void wait_packed(const PackSync *sync, uint32_t npack, uint32_t tag, uint32_t *err,
-                                            uint32_t spin, uint32_t lane) {
-    const uint32_t want = (tag << 1) | 1u;
-    for (uint32_t p = lane; p < npack; p += 32) {
-        uint32_t spins = 0, ns = 64;
-        while (ld_acquire(&sync->flag[p]) != want) {
-            if (++spins > spin) {
-                atomicOr(err, kErrScanSpin);
-                break;
-            }
-            poll_pause(ns);
-        }
-    }
-    __syncwarp();
+// Bounded wait, by one thread, until every pack chunk of the batch is done;
+// then the CTA may read the batch's records.
+__device__ __forceinline__ void wait_packed(const PackSync *sync, uint32_t npack, uint32_t *err, uint32_t spin) {
+    wait_eq(&sync->packed, npack, err, spin, 512u);
 }
 
 // The batch's error bits to the host word the batch names (the device word is
@@ -465,16 +457,7 @@ __device__ __noinline__ void scatter_phase(const BatchView &b, PackSync *__restr
         // below); a CTA without a chunk reads nothing and leaves at once
         if (threadIdx.x == 0) {
             sm.c = atomicAdd(&sync->sticket, 1u);
-            if (sm.c < nch) {
-                uint32_t spins = 0, ns = 64;
-                while (ld_acquire(b.probe_done) != T) {
-                    if (++spins > spin) {
-                        atomicOr(b.err, kErrScanSpin);
-                        break;
-                    }
-                    poll_pause(ns);
-                }
-            }
+            if (sm.c < nch) wait_eq(b.probe_done, T, b.err, spin, 128u);  // chunk owners only: few pollers
         }
         __syncthreads();
         const uint32_t c = sm.c;
@@ -565,16 +548,7 @@ __device__ __noinline__ void scatter_phase(const BatchView &b, PackSync *__restr
     // lane j fetches the count, slot and output position of the warp's j-th
     // tile of a round, all lanes at once, and the warp then copies the round's
     // non-empty tiles with eight independent loads per lane.
-    if (threadIdx.x == 0) {
-        uint32_t spins = 0, ns = 64;
-        while (ld_acquire(b.scatter_ready) != nch) {
-            if (++spins > spin) {
-                atomicOr(b.err, kErrScanSpin);
-                break;
-            }
-            poll_pause(ns);
-        }
-    }
+    if (threadIdx.x == 0) wait_eq(b.scatter_ready, nch, b.err, spin, 512u);
     __syncthreads();
     const uint32_t gw = blockIdx.x * (blockDim.x / 32) + w, nw = gridDim.x * (blockDim.x / 32);
     const uint32_t *__restrict__ scr = b.scratch;

@@ -25,14 +25,17 @@ inline constexpr uint64_t tile_pack(uint32_t seg, uint32_t e0, uint32_t nseg) {
 }
 
 // Device-resident description of one posting list (80 bytes, 16-byte aligned
-// so a warp reads it with 128-bit loads).
+// so a warp reads it with 128-bit loads). The first 16 bytes hold what the
+// batch kernel's pack phase reads per query term (length, tiles, block size),
+// so that costs one vector load.
 struct alignas(16) ListDesc {
-    uint64_t word_base;   // first word of the list's blocks in the words[] array
     uint32_t n;           // postings
+    uint32_t ntiles;      // tiles when this list is the shortest of a query
+    uint32_t log2_block;  // fixed block size = 1 << log2_block; 0 = variable (HS)
     uint32_t seg_base;    // first segment of the list in the per-segment arrays
+    uint64_t word_base;   // first word of the list's blocks in the words[] array
     uint32_t nseg;        // segments (fixed blocks, or non-empty HS blocks)
     uint32_t codec;       // excl_codec
-    uint32_t log2_block;  // fixed block size = 1 << log2_block; 0 = variable (HS)
     uint32_t first_doc;
     uint32_t last_doc;
     uint32_t reg[4];      // list-level regression raw bits (LRC: slope, icpt, range, 0; others a, b, L, R)
@@ -40,11 +43,12 @@ struct alignas(16) ListDesc {
     uint32_t dir_base;    // first directory entry (ndir + 1 entries)
     uint32_t ndir;        // buckets
     uint32_t tile_base;   // variable lists: first tilemap entry
-    uint32_t ntiles;      // tiles when this list is the shortest of a query
     uint32_t model;       // learned model slot or kNoModel
     uint32_t pad;
 };
 static_assert(sizeof(ListDesc) == 80, "ListDesc layout");
+static_assert(offsetof(ListDesc, n) == 0 && offsetof(ListDesc, ntiles) == 4 && offsetof(ListDesc, log2_block) == 8,
+              "the pack phase reads n, ntiles and log2_block as one 16-byte vector");
 
 // Per-segment record: start element, word offset within the list, aux
 // (ParaPFD: docID at the segment middle = segMedian; residual codecs: base).

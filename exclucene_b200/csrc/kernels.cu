@@ -159,7 +159,8 @@ struct ProbeShared {
     ListDesc list[kBatchWarps];
 };
 
-// Spin limit of every cross-CTA wait (x >= 64 ns of sleep per poll: > 0.25 s).
+// Spin limit of every cross-CTA wait: 2^22 polls, 32 ns to ~1 us of sleep
+// each, so a wait that gives up has waited between 0.13 s and about 4 s.
 constexpr uint32_t kSpin = 1u << 22;
 
 // MINB: resident 8-warp CTAs per SM the register budget is cut for (4: 64
@@ -167,7 +168,7 @@ constexpr uint32_t kSpin = 1u << 22;
 // shape is an autotuner choice. KIND: the codec family the instance handles
 // (kKindAny for mixed indexes); a one-family instance needs fewer registers.
 template <int ALGO, int MINB, int KIND>
-__global__ void __launch_bounds__(kBatchWarps * 32, MINB) k_batch(DevIndexView ix, BatchView b, PackSync *sync,
+__global__ void __launch_bounds__(kBatchWarps * 32, MINB) k_batch(const __grid_constant__ DevIndexView ix, const __grid_constant__ BatchView b, PackSync *sync,
                                                                   uint64_t *chunk_state, const ListDesc *lists,
                                                                   uint32_t nlists, const uint32_t *terms,
                                                                   const uint32_t *toff, uint32_t *offsets,
@@ -193,8 +194,9 @@ __global__ void __launch_bounds__(kBatchWarps * 32, MINB) k_batch(DevIndexView i
     // up and raises the expired-wait bit; the batch itself is unaffected
     if (b.check_polls && blockIdx.x == 0 && threadIdx.x == 0) wait_tag(b.check_flag, tag, b.err, b.check_polls);
 
-    // ---- pack: chunks of 256 queries by ticket
-    const uint32_t npack = max(1u, (b.nq + kPackThreads - 1) / kPackThreads);
+    // ---- pack: chunks of qpc queries by ticket
+    const uint32_t qpc = pack_chunk_queries(b.nq);
+    const uint32_t npack = max(1u, (b.nq + qpc - 1) / qpc);
     for (bool first = true;; first = false) {
         if (!first && threadIdx.x == 0) s_ticket = atomicAdd(&sync->ticket, 1u);
         __syncthreads();
@@ -202,11 +204,11 @@ __global__ void __launch_bounds__(kBatchWarps * 32, MINB) k_batch(DevIndexView i
         __syncthreads();
         if (bid >= npack) break;
         if (bid == 0 && threadIdx.x == 0 && b.stats) b.stats[4] = global_ns();
-        pack_chunk(bid, npack, tag, lists, nlists, terms, toff, b.nq, b, sync, sm.pack, spin);
+        pack_chunk(bid, npack, qpc, tag, lists, nlists, terms, toff, b.nq, b, sync, sm.pack, spin);
     }
-    if (w == 0) {
-        wait_packed(sync, npack, tag, b.err, spin, lane);
-        if (lane == 0 && b.stats) atomicMin((unsigned long long *)&b.stats[5], (unsigned long long)global_ns());
+    if (threadIdx.x == 0) {
+        wait_packed(sync, npack, b.err, spin);
+        if (b.stats) atomicMin((unsigned long long *)&b.stats[5], (unsigned long long)global_ns());
     }
     __syncthreads();
 
@@ -383,6 +385,7 @@ __global__ void __launch_bounds__(kBatchWarps * 32, MINB) k_batch(DevIndexView i
         sync->ticket = 0u;
         sync->sticket = 0u;
         sync->sdone = 0u;
+        sync->packed = 0u;
         if (b.stats) b.stats[7] = global_ns();
         hand_over_flags(b);
         sync->epoch = tag;

@@ -55,11 +55,22 @@ struct PackSync {
     uint32_t epoch;           // tag of the last batch run on this state
     uint32_t ticket;          // pack phase: chunk tickets
     uint32_t sticket, sdone;  // scatter phase: chunk tickets; CTAs that left the kernel
-    uint32_t flag[kPackMaxCtas];  // pack chunk c: tag << 1 (aggregates out), tag << 1 | 1 (done)
+    uint32_t flag[kPackMaxCtas];  // pack chunk c: tag << 1 once its aggregates are out
     uint32_t agg_t[kPackMaxCtas];
     uint32_t agg_k[kPackMaxCtas];
     uint32_t agg_h[kPackMaxCtas];
+    // pack chunks whose writes are all visible (the probe phase starts when it
+    // reaches the batch's chunks; reset by the last CTA out). Every CTA polls
+    // it, so it has a cache line of its own.
+    alignas(128) uint32_t packed;
 };
+
+// Queries per pack chunk: small chunks spread the pack's gathers (terms,
+// list descriptors) over many SMs; larger ones keep big batches within the
+// kPackMaxCtas chunk slots.
+__host__ __device__ inline uint32_t pack_chunk_queries(uint32_t nq) {
+    return nq <= 64u * kPackMaxCtas ? 64u : (nq <= 128u * kPackMaxCtas ? 128u : 256u);
+}
 
 // Everything one batch launch needs.
 struct BatchLaunch {
