@@ -244,17 +244,24 @@ __global__ void __launch_bounds__(kBatchWarps * 32, MINB) k_batch(const __grid_c
             uint32_t kc = 0, first_elem;
             keys = sm.probe.keys[w];
             if (L.log2_block) {
-                // tile ti: part (ti mod 2^s) of segment ti >> s; the whole segment is
-                // decoded (d-gaps need its prefix) and the part's keys probed
+                // tile ti: part (ti mod 2^s) of segment ti >> s. Residual codecs
+                // decode any element on its own, so only the part is decoded;
+                // d-gap codecs decode the whole segment (the part needs its
+                // prefix) and probe the part's keys
                 const uint32_t sp = tile_split_of(L.log2_block, b.tile_split);
                 const uint32_t sg = L.seg_base + (ti >> sp);
                 // fixed blocks: every segment but the last holds 2^log2_block postings
                 const uint32_t cnt = min(1u << L.log2_block, L.n - ((ti >> sp) << L.log2_block));
                 const uint32_t sub = (1u << L.log2_block) >> sp, e0 = (ti & ((1u << sp) - 1u)) * sub;
                 first_elem = ((ti >> sp) << L.log2_block) + e0;
-                warp_decode<KIND>(ix, L, sg, 0, cnt, keys, lane);
                 kc = e0 < cnt ? min(sub, cnt - e0) : 0u;
-                keys += e0;
+                const bool resid = KIND == kKindResid || (KIND == kKindAny && !codec_is_dgap(L.codec));
+                if (sp && resid) {
+                    if (kc) warp_decode<KIND>(ix, L, sg, e0, kc, keys, lane);
+                } else {
+                    warp_decode<KIND>(ix, L, sg, 0, cnt, keys, lane);
+                    keys += e0;
+                }
             } else {
                 const uint64_t tm = ix.tilemap[L.tile_base + ti];
                 const uint32_t sg0 = L.seg_base + (uint32_t)(tm >> 32);
