@@ -45,8 +45,8 @@ MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 
 # dram__bytes_read.sum + dram__bytes_write.sum of one k_batch launch on the full-size workload,
-# from one ncu capture of this bench command (profiles/); None until captured for this build
-NCU_BATCH_TRAFFIC: dict = {}
+# from one ncu capture (profiles/k_batch_zipf_seglrc.md: 45.47 MB read + 0.30 MB written)
+NCU_BATCH_TRAFFIC: dict = {"zipf": 45_472_768 + 302_080}
 
 
 def parse():
@@ -66,6 +66,8 @@ def parse():
     p.add_argument("--no-learn", action="store_true")
     p.add_argument("--no-serve", action="store_true", help="skip the serving-loop latency measurement")
     p.add_argument("--no-layout-tune", action="store_true", help="skip the index-layout autotuner")
+    p.add_argument("--ctas-per-sm", type=int, default=0,
+                   help="with --algo: batch kernel CTAs per SM (4, 5 or 6) instead of the default launch shape")
     return p.parse_args()
 
 
@@ -517,6 +519,9 @@ def main():
 
     # a second context on the same resident index replays each batch as a CUDA graph
     gctx = ex.Context(local, max_queries=max(w.nq, 1024), max_keys=max(1 << 20, 2 * shortest), use_graphs=True)
+    if args.algo and args.ctas_per_sm:
+        for c in (ctx, gctx):
+            c.set_tuning(algo=args.algo, warps_per_cta=8, ctas_per_sm=args.ctas_per_sm, merge_segs=2, tile_split=0)
 
     def step(c, algo):
         c.intersect_device(ix, d_terms.data_ptr(), d_toff.data_ptr(), w.nq, algo, d_offs.data_ptr(),
