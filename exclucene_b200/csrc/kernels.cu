@@ -24,10 +24,6 @@ __device__ __forceinline__ int64_t imax64(int64_t a, int64_t b) { return a > b ?
 __device__ __forceinline__ int64_t imin64(int64_t a, int64_t b) { return a < b ? a : b; }
 
 template <int ALGO, int KIND>
-__device__ __forceinline__ bool probe_in_segment(const DevIndexView &ix, const ListDesc &L, const ProbeRec *pr, int s,
-                                                 uint32_t key, bool learned, int64_t plo, int64_t phi);
-
-template <int ALGO, int KIND>
 __device__ __forceinline__ bool probe_key(const DevIndexView &ix, const ListDesc &L, uint32_t key, uint32_t &fallback) {
     if (key < L.first_doc || key > L.last_doc) return false;
     uint32_t lo, hi;
@@ -69,15 +65,6 @@ __device__ __forceinline__ bool probe_key(const DevIndexView &ix, const ListDesc
         s = last_head_le_rec(pr, lo, hi, key);
     }
     if (s < (int)lo) return false;
-    return probe_in_segment<ALGO, KIND>(ix, L, pr, s, key, learned, plo, phi);
-}
-
-// The search for `key` inside segment s of L (its head <= key): the segment's
-// record, then the d-gap walk or the residual window search; a learned rank
-// window [plo, phi] bounds the residual search when `learned`.
-template <int ALGO, int KIND>
-__device__ __forceinline__ bool probe_in_segment(const DevIndexView &ix, const ListDesc &L, const ProbeRec *pr, int s,
-                                                 uint32_t key, bool learned, int64_t plo, int64_t phi) {
     // the segment's record: head, block offset, count, base/median, block
     // descriptor and segment regression
     const uint4 q0 = __ldg(reinterpret_cast<const uint4 *>(pr + s));
@@ -152,56 +139,6 @@ __device__ __forceinline__ int locate_segment(const DevIndexView &ix, const List
         hi = d1;
     }
     return last_head_le(ix.seg_head + L.seg_base, lo, hi, key);
-}
-
-// Segments of a tile's keys in one longer list by the directory, found in
-// passes over all the keys instead of one chain of loads per key: pass 1
-// issues the directory words of kStageKeys keys per lane, pass 2 their first
-// two candidate heads (the directory's usual range; a wider range is searched
-// for that key alone), all loads of a pass in flight together. st[i] receives
-// key i's segment within the list, or ~0 when the key cannot be in the list
-// (the same segment probe_key finds with the directory).
-constexpr int kStageKeys = 4;
-__device__ __forceinline__ void stage_segments(const DevIndexView &ix, const ListDesc &L, const uint32_t *keys,
-                                               uint32_t n, uint32_t *st, uint32_t lane) {
-    const ProbeRec *pr = ix.seg_probe + L.seg_base;
-    const bool hs = codec_is_hs(L.codec);
-    for (uint32_t i0 = 0; i0 < n; i0 += 32u * kStageKeys) {
-        uint32_t lo[kStageKeys], hi[kStageKeys], h0[kStageKeys], h1[kStageKeys];
-#pragma unroll
-        for (int r = 0; r < kStageKeys; ++r) {
-            const uint32_t i = i0 + lane + 32u * r;
-            const uint32_t key = i < n ? keys[i] : 0u;
-            const bool in = i < n && key >= L.first_doc && key <= L.last_doc;
-            const uint32_t b = (uint32_t)((uint64_t)key >> L.dir_shift);
-            lo[r] = in ? ldg(ix.dir + L.dir_base + b) : 0u;
-            hi[r] = in ? ldg(ix.dir + L.dir_base + b + 1) : 0u;
-        }
-#pragma unroll
-        for (int r = 0; r < kStageKeys; ++r) {
-            if (!hs) lo[r] = lo[r] ? lo[r] - 1u : 0u;
-            h0[r] = lo[r] < hi[r] ? __ldg(&pr[lo[r]].head) : 0u;
-            h1[r] = lo[r] + 1u < hi[r] ? __ldg(&pr[lo[r] + 1u].head) : 0u;
-        }
-#pragma unroll
-        for (int r = 0; r < kStageKeys; ++r) {
-            const uint32_t i = i0 + lane + 32u * r;
-            if (i < n) {
-                const uint32_t key = keys[i];
-                int sg = (int)lo[r] - 1;
-                if (hi[r] > lo[r]) {
-                    if (hi[r] - lo[r] <= 2u) {
-                        if (h0[r] <= key) sg = (int)lo[r];
-                        if (lo[r] + 1u < hi[r] && h1[r] <= key) sg = (int)lo[r] + 1;
-                    } else {
-                        sg = last_head_le_rec(pr, lo[r], hi[r], key);
-                    }
-                }
-                st[i] = sg >= (int)lo[r] ? (uint32_t)sg : 0xffffffffu;
-            }
-        }
-    }
-    __syncwarp();
 }
 
 // ---------------------------------------------------------------------------
@@ -372,23 +309,13 @@ __global__ void __launch_bounds__(kBatchWarps * 32, MINB) k_batch(const __grid_c
                         }
                     }
                 }
-                // directory methods: the keys' segments in passes over all keys
-                // (the merge buffer holds them), when there is more than one round
-                const bool staged = !span && alive > 32u &&
-                                    (ALGO == EXCL_ALGO_HASHSEG || ALGO == EXCL_ALGO_SEGREG ||
-                                     (ALGO == EXCL_ALGO_AUTO && L.model == kNoModel));
-                if (staged) stage_segments(ix, L, keys, alive, mbuf, lane);
                 uint32_t nout = 0;
                 for (uint32_t base = 0; base < alive; base += 32) {
                     const uint32_t i = base + lane;
                     const bool valid = i < alive;
                     const uint32_t key = valid ? keys[i] : 0u;
                     bool f;
-                    if (staged) {
-                        const uint32_t sg = valid ? mbuf[i] : 0xffffffffu;
-                        f = sg != 0xffffffffu && probe_in_segment<ALGO, KIND>(ix, L, ix.seg_probe + L.seg_base, (int)sg,
-                                                                             key, false, 0, -1);
-                    } else if (span) {
+                    if (span) {
                         // first position with mbuf[pos] >= key, in shared memory
                         uint32_t lo = 0, hi = span;
                         while (lo < hi) {
