@@ -415,7 +415,7 @@ class Context:
     def submit_into(self, ix: Index, terms: np.ndarray, term_offsets: np.ndarray, offsets: np.ndarray,
                     docids: np.ndarray, algo="auto") -> "Batch":
         """Zero-copy batch (excl_submit_into): offsets[nq+1] and docids are pinned_empty
-        arrays the last kernel writes into; terms and term_offsets are read from host
+        arrays the batch kernel writes into; terms and term_offsets are read from host
         memory (pinned_empty ones asynchronously). Keep all four alive and unchanged
         until wait() returns the number of docIDs written."""
         for a in (terms, term_offsets, offsets, docids):

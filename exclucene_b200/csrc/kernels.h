@@ -37,7 +37,7 @@ struct BatchView {
                                  // (times in globaltimer ns)
 };
 
-// probe kernel: shared-memory merge of a tile's keys against a decoded span
+// probe phase: shared-memory merge of a tile's keys against a decoded span
 constexpr uint32_t kMergeCap = 512;      // docIDs of the span (two 256-blocks)
 constexpr uint32_t kMergeMinKeys = 32;   // fewer keys than this: always probe
 

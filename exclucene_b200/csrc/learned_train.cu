@@ -9,7 +9,7 @@
 //   leaf  out * L routes the key to one of L linear fits rank ~ a*x + b,
 //         solved from per-leaf sums over all keys;
 //   error per leaf, the min and max of rank - floor(a*x + b) over the leaf's
-//         keys, computed with the same inference code the probe kernel runs,
+//         keys, computed with the same inference code the probe phase runs,
 //         so a present key's rank always lies in [pred + elo, pred + ehi].
 #include <cuda_runtime.h>
 

@@ -661,7 +661,7 @@ static int32_t take_slot(excl_ctx *ctx) {
 }
 
 // Ends a batch whose pipeline ran with err_out = the slot's mapped word (the
-// scatter kernel hands the batch's error bits to it and clears the device
+// batch kernel's last CTA hands the batch's error bits to it and clears the device
 // word, so batches in flight together each see their own flags): records the
 // slot's event and hands the batch out. On failure the slot is returned.
 static int finish_batch(excl_ctx *ctx, uint32_t nq, int32_t slot, const uint32_t *into_offsets, excl_batch **ticket) {

@@ -16,7 +16,7 @@
 //
 // A slot is a stream with its own cross-CTA pipeline state, error flag and
 // pinned host buffers, so batches of different slots overlap on the GPU while
-// new queries keep arriving. The scatter kernel writes each batch's offsets
+// new queries keep arriving. The batch kernel writes each batch's offsets
 // and docIDs straight into the slot's mapped pinned host buffers, so a result
 // needs no copy back after the batch event.
 #include <cuda_runtime.h>
@@ -142,7 +142,7 @@ struct Slot {
     PackSync *d_sync = nullptr;
     uint64_t *d_chunk = nullptr;
     uint32_t *d_misc = nullptr;                      // error flag, probe work counter, tiles probed
-    uint32_t *h_terms = nullptr, *h_toff = nullptr;  // pinned, mapped: the pack kernel reads them in place
+    uint32_t *h_terms = nullptr, *h_toff = nullptr;  // pinned, mapped: the pack phase reads them in place
     uint32_t *h_err = nullptr;                       // pinned, mapped: the batch's error bits, handed over by the batch kernel's last CTA
     uint32_t *m_terms = nullptr, *m_toff = nullptr, *m_err = nullptr;  // their device addresses
     uint32_t *h_offsets = nullptr, *h_docids = nullptr;  // mapped pinned results

@@ -203,12 +203,12 @@ typedef struct {
     uint32_t max_terms;      /* per query, <= 32 (reference MAX_QUERY_LEN 80, of which 8 are used by the workloads) */
     uint64_t max_keys;       /* per batch, sum of shortest-list lengths (reference baseSize) */
     uint32_t warps_per_cta;  /* batch kernel CTA width: 8 warps (0 = 8; 4 is accepted and runs as 8) */
-    uint32_t ctas_per_sm;    /* probe kernel: 4, 5 or 6 resident 8-warp CTAs per SM, i.e. a register
+    uint32_t ctas_per_sm;    /* batch kernel: 4, 5 or 6 resident 8-warp CTAs per SM, i.e. a register
                                 budget of 64, 48 or 40 per thread (0 = 5) */
-    uint32_t use_graphs;     /* 1: excl_intersect_device replays a CUDA graph of the batch's three
-                                kernels when called again with the same arguments (per-kernel
-                                times in excl_last_stats are then 0; total_ms stays) */
-    uint32_t merge_segs;     /* probe kernel: a tile whose keys span at most this many segments of a
+    uint32_t use_graphs;     /* 1: excl_intersect_device replays a CUDA graph of the batch kernel
+                                when called again with the same arguments (excl_last_stats then
+                                times the graph launch) */
+    uint32_t merge_segs;     /* probe phase: a tile whose keys span at most this many segments of a
                                 longer list decodes that span into shared memory and merges instead
                                 of probing key by key (0 = default 2, EXCL_MERGE_OFF = never; max 4) */
 } excl_ctx_config;
@@ -255,7 +255,7 @@ int excl_wait(excl_batch *ticket, uint32_t *offsets, uint32_t *docids, size_t ca
 int excl_batch_free(excl_batch *ticket);
 
 /* Zero-copy variant of excl_submit, same results. The inputs are read from
- * host memory (asynchronously when page-locked) and the last kernel writes
+ * host memory (asynchronously when page-locked) and the batch kernel writes
  * offsets[nq+1] and up to cap docIDs straight into the caller's arrays, which
  * must be page-locked, device-mapped host memory (excl_host_alloc, or
  * cudaHostAlloc / cudaHostRegister with the mapped flag). Query q's terms are

@@ -103,7 +103,7 @@ def test_invalid_batches_raise(gpu_ctx, corpus):
 
 def test_tile_overflow_reports_capacity(corpus):
     """A batch with more tiles (and shortest-list docIDs) than a small context
-    holds fails with EXCL_E_CAPACITY: the pack kernel's work order then covers
+    holds fails with EXCL_E_CAPACITY: the pack phase's work order then covers
     only the tiles that fit, and nothing runs past the buffers. The context
     answers the next batch exactly."""
     ix = _index(corpus, "seglrc")
@@ -292,7 +292,7 @@ def test_reference_file_set_runs_unchanged(gpu_ctx, tmp_path, codec):
 def test_newpfd_many_exceptions_decode_and_intersect(gpu_ctx, corpus, expected, block, frac):
     """NewPFD blocks with up to 64% exceptions: the group-parallel Simple-16
     exception decode (many rounds of exceptions and of stream words per block)
-    in the whole-list decode and in the probe kernel's tile decode."""
+    in the whole-list decode and in the probe phase's tile decode."""
     ix = _index(corpus, "newpfd", block, frac)
     gpu_ctx.upload(ix)
     assert np.array_equal(gpu_ctx.decode_lists(ix), corpus.docs)
