@@ -22,10 +22,11 @@ _API_NAMES = set(__all__)
 def __getattr__(name):
     # the binding is loaded on first use, so the build module imports (and can
     # rebuild) even when the library is missing or older than the binding
-    if name in _API_NAMES:
+    if name in _API_NAMES or name == "api":
         if not _os.path.exists(_LIB):
             raise ImportError(f"{_LIB} is not built; run `python -m exclucene_b200.build`")
-        from . import api
+        import importlib
 
-        return getattr(api, name)
+        api = importlib.import_module(__name__ + ".api")
+        return api if name == "api" else getattr(api, name)
     raise AttributeError(name)
