@@ -312,12 +312,22 @@ __device__ __forceinline__ void group_dgap_full(const uint32_t *blk, const RunMe
     const uint32_t mask = (1u << h.lb) - 1u;
     const uint32_t el = sub * 8u;
     uint32_t v[8];
-    uint32_t bit = el * h.lb;
+    // a 64-bit window slides over the lane's words: each word is read from
+    // shared memory once (two words, then one more whenever the bit position
+    // crosses a word) instead of twice per value
+    const uint32_t bit0 = el * h.lb;
+    uint32_t wi = bit0 >> 5, sh = bit0 & 31u;
+    uint32_t lo = lows[wi], hi = lows[wi + 1];
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
-        const uint32_t wi = bit >> 5;
-        v[q] = __funnelshift_r(lows[wi], lows[wi + 1], bit & 31u) & mask;
-        bit += h.lb;
+        v[q] = __funnelshift_r(lo, hi, sh) & mask;
+        sh += h.lb;
+        if (q < 7 && sh >= 32u) {
+            sh -= 32u;
+            lo = hi;
+            ++wi;
+            hi = lows[wi + 1];
+        }
     }
     const bool exc = h.en != 0;
     if (__any_sync(0xffffffffu, exc)) {
