@@ -244,11 +244,24 @@ __device__ __forceinline__ void group_dgap(const uint32_t *blk, const RunMeta &m
     const uint32_t el = sub * vpl;
     const uint32_t mask = (1u << h.lb) - 1u;
     uint32_t v[8];
+    {
+        // a 64-bit window slides over the lane's words (as group_dgap_full),
+        // moving on only while the lane has another value to extract
+        const uint32_t nv = el < count ? min(vpl, count - el) : 0u;
+        const uint32_t bit0 = el * h.lb;
+        uint32_t wi = bit0 >> 5, sh = bit0 & 31u;
+        uint32_t lo = nv ? lows[wi] : 0u, hi = nv ? lows[wi + 1] : 0u;
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
-        const uint32_t bit = (el + q) * h.lb;
-        const uint32_t wi = bit >> 5;
-        v[q] = (q < (int)vpl && el + q < count) ? (__funnelshift_r(lows[wi], lows[wi + 1], bit & 31u) & mask) : 0u;
+        for (int q = 0; q < 8; ++q) {
+            v[q] = q < (int)nv ? (__funnelshift_r(lo, hi, sh) & mask) : 0u;
+            sh += h.lb;
+            if (q + 1 < (int)nv && sh >= 32u) {
+                sh -= 32u;
+                lo = hi;
+                ++wi;
+                hi = lows[wi + 1];
+            }
+        }
     }
     const bool exc = count && h.en;
     if (__any_sync(0xffffffffu, exc)) {
