@@ -133,7 +133,8 @@ def test_learned_beats_the_plain_methods(gpu_ctx):
     (model window, then a search inside it) takes less device time than both
     plain comparators (binary search over the heads or the bucket directory,
     then a binary search over the block), with bit-exact output for all three.
-    Times are medians of 5 batches after a warm-up (CUDA events)."""
+    Times are the fastest of 7 batches after a warm-up (CUDA events), which is
+    the least sensitive to other work on a shared GPU."""
     lens = [3_000_000, 2_000_000, 4_000_000, 1_500_000]
     t = synth.uniform_lists(lens, ubits=28, seed=21)
     rng = np.random.default_rng(22)
@@ -158,9 +159,9 @@ def test_learned_beats_the_plain_methods(gpu_ctx):
         offs, got = gpu_ctx.intersect(ix, terms, toff, algo=algo)
         assert np.array_equal(offs.astype(np.uint64), eo) and np.array_equal(got, ed), algo
         runs = []
-        for _ in range(5):
+        for _ in range(7):
             gpu_ctx.intersect(ix, terms, toff, algo=algo)
             runs.append(gpu_ctx.stats().total_ms)
-        ms[algo] = float(np.median(runs))
+        ms[algo] = float(min(runs))
     assert ms["learned"] < min(ms["bsearch"], ms["hashseg"]), ms
     ix.close()
