@@ -313,9 +313,9 @@ __device__ __forceinline__ void group_dgap(const uint32_t *blk, const RunMeta &m
 // d-gap codecs, full blocks of 8G values with G = 16 or 32 (ParaPFD blocks of
 // 128 or 256): the same steps as group_dgap with every bound known, so no
 // value needs a bounds test, the G-wide scan is unrolled, and each lane's
-// eight consecutive docIDs leave its registers as two 16-byte stores (the
-// caller checks that the group's output is 16-byte aligned). Every group of
-// the warp holds such a block.
+// eight consecutive docIDs leave its registers as two 16-byte stores when the
+// group's output is 16-byte aligned. Every group of the warp holds such a
+// block.
 template <uint32_t LG>
 __device__ __forceinline__ void group_dgap_full(const uint32_t *blk, const RunMeta &m, uint32_t sub, uint32_t *vals,
                                                 uint32_t base, uint32_t *__restrict__ out) {
@@ -376,9 +376,31 @@ __device__ __forceinline__ void group_dgap_full(const uint32_t *blk, const RunMe
         if (sub >= o) incl += t;
     }
     const uint32_t ex = incl - run;
-    uint4 *o = reinterpret_cast<uint4 *>(out + m.ob + el);
-    o[0] = make_uint4(v[0] + ex, v[1] + ex, v[2] + ex, v[3] + ex);
-    o[1] = make_uint4(v[4] + ex, v[5] + ex, v[6] + ex, v[7] + ex);
+    // a group whose output starts on a 16-byte boundary stores its lanes'
+    // eight docIDs as two 16-byte vectors; another (a hash bucket's block
+    // starts anywhere) goes through the warp's buffer and stores G-wide
+    uint32_t *ob = out + m.ob;
+    const bool al = (reinterpret_cast<uintptr_t>(ob) & 15u) == 0;
+    if (__all_sync(0xffffffffu, al)) {
+        uint4 *o = reinterpret_cast<uint4 *>(ob + el);
+        o[0] = make_uint4(v[0] + ex, v[1] + ex, v[2] + ex, v[3] + ex);
+        o[1] = make_uint4(v[4] + ex, v[5] + ex, v[6] + ex, v[7] + ex);
+        return;
+    }
+    if (!al) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) vals[sw(base + el + q)] = v[q] + ex;
+    }
+    __syncwarp();
+    if (al) {
+        uint4 *o = reinterpret_cast<uint4 *>(ob + el);
+        o[0] = make_uint4(v[0] + ex, v[1] + ex, v[2] + ex, v[3] + ex);
+        o[1] = make_uint4(v[4] + ex, v[5] + ex, v[6] + ex, v[7] + ex);
+    } else {
+#pragma unroll
+        for (uint32_t j = 0; j < 8; ++j) ob[sub + G * j] = vals[sw(base + sub + G * j)];
+    }
+    __syncwarp();
 }
 
 // Residual codecs (LRC, LRCSeg, SegLRC, HS_SegLRC), one segment per group of
@@ -576,9 +598,8 @@ __global__ void __launch_bounds__(kDecWarps * 32, kDecCtasPerSm) k_decode_tma(De
         default: EXCL_DEC_CALL(F, 5); break;                \
     }
                     if (c < 6u) {
-                        // full blocks of 128 or 256 values in every group, output 16-byte aligned
-                        const bool full = act && (lg == 4u || lg == 5u) && m.count == (8u << lg) &&
-                                          ((reinterpret_cast<uintptr_t>(out + m.ob) & 15u) == 0);
+                        // full blocks of 128 or 256 values in every group
+                        const bool full = act && (lg == 4u || lg == 5u) && m.count == (8u << lg);
                         if (__all_sync(0xffffffffu, full)) {
                             if (lg == 4u) group_dgap_full<4>(blk, m, sub, vals, base, out);
                             else group_dgap_full<5>(blk, m, sub, vals, base, out);
